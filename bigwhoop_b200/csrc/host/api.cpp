@@ -1,0 +1,673 @@
+// bwc_compress / bwc_decompress: the device pipeline behind the libbwc API.
+//
+// Compression of one tile (libbwc.c:3145-3438), per parameter, all on the codec's CUDA stream:
+//   upload -> fill + min/max -> normalise -> forward 9/7 DWT -> tier-1 encode (warp per
+//   codeblock); then one download of the per-codeblock tier-1 summary (K, Z, truncation
+//   lengths, log slopes), host tier-2 (rate control, packet headers, layout), and one device
+//   gather that assembles header bytes and coded-byte slices into the codestream, which is
+//   copied to stream->out.
+// Decompression (libbwc.c:3485-3710): host parsing of headers and packets, upload of the
+// codestream, device gather of each codeblock's bytes, tier-1 decode + dequantise, inverse DWT,
+// denormalise + dtype conversion, copy to stream->out.
+//
+// There is no CPU fallback: a missing or failing GPU makes the calls fail (0 / 1 returns and a
+// diagnostic on stderr, the reference's error convention).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <vector>
+
+#include "../kernels/kernels.hpp"
+#include "bwc_b200.h"
+#include "common.hpp"
+
+namespace bwcb {
+
+void launch_t1_encode_ex(const bwc_float *work, const FieldDims &dims, const CbDev *cbs,
+                         uint32_t ncb, const SbDev *sbs, uchar erres, const T1EncOut &out,
+                         uint32_t state_cap, uint16_t *gstate, uint32_t *work_counter, int grid,
+                         cudaStream_t s);
+
+namespace {
+
+bool cuda_ok(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return true;
+  fprintf(stderr,
+          "o##########################################################o\n"
+          "| ERROR: CUDA failure in %-34s|\n"
+          "|        %-50s|\n"
+          "o##########################################################o\n",
+          what, cudaGetErrorString(e));
+  return false;
+}
+
+// Process-wide cache of device allocations: codecs are short-lived (one per field in the
+// libbwc usage pattern), so their buffers are recycled instead of cudaMalloc'd per call.
+class Pool {
+ public:
+  static Pool &get() {
+    static Pool p;
+    return p;
+  }
+  void *acquire(size_t bytes, size_t *got) {
+    std::lock_guard<std::mutex> l(m_);
+    auto it = free_.lower_bound(bytes);
+    if (it != free_.end() && it->first <= bytes * 2 + (1 << 20)) {
+      void *p = it->second;
+      *got = it->first;
+      free_.erase(it);
+      return p;
+    }
+    void *p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+      // give cached blocks back and retry once
+      for (auto &kv : free_) cudaFree(kv.second);
+      free_.clear();
+      cudaGetLastError();
+      if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+      }
+    }
+    *got = bytes;
+    return p;
+  }
+  void release(void *p, size_t bytes) {
+    if (!p) return;
+    std::lock_guard<std::mutex> l(m_);
+    free_.emplace(bytes, p);
+  }
+
+ private:
+  std::mutex m_;
+  std::multimap<size_t, void *> free_;
+};
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  template <typename T>
+  T *as() const { return reinterpret_cast<T *>(p); }
+  bool ensure(size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (cap >= bytes) return true;
+    Pool::get().release(p, cap);
+    p = Pool::get().acquire(bytes, &cap);
+    if (!p) {
+      cap = 0;
+      fprintf(stderr, "%s", kMemError);
+      return false;
+    }
+    return true;
+  }
+  void drop() {
+    Pool::get().release(p, cap);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+uint8_t sig_class(uint8_t hb) {
+  // context table by subband orientation (tier1.c:2416-2446)
+  switch (hb) {
+    case 1: case 5: case 9: case 13: return 1;
+    case 3: case 7: case 11: case 15: return 2;
+    default: return 0;
+  }
+}
+
+}  // namespace
+
+struct DeviceState {
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[8] = {};
+  DevBuf in, work, keys, stats, cbtab, sbtab, bytes, scratch, snaps, dmse, K, Z, L, S, flags,
+      slopes, counter, cs, blob, pieces, outbuf, mags, lmax;
+  bool dump_set = false, ddump_set = false;
+  bwc_b200_stage_dump dump{};
+  bwc_b200_decode_dump ddump{};
+  double timings[8] = {};
+
+  ~DeviceState() {
+    DevBuf *all[] = {&in, &work, &keys, &stats, &cbtab, &sbtab, &bytes, &scratch, &snaps, &dmse,
+                     &K, &Z, &L, &S, &flags, &slopes, &counter, &cs, &blob, &pieces, &outbuf,
+                     &mags, &lmax};
+    if (stream) cudaStreamSynchronize(stream);
+    for (DevBuf *b : all) b->drop();
+    for (auto &e : ev)
+      if (e) cudaEventDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+static DeviceState *device_state(bwc_codec *codec) {
+  bwc_b200_engine *eng = codec->tile;
+  if (!eng) return nullptr;
+  if (!eng->dev) {
+    DeviceState *d = new (std::nothrow) DeviceState();
+    if (!d) return nullptr;
+    if (!cuda_ok(cudaGetDevice(&d->device), "cudaGetDevice") ||
+        !cuda_ok(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking), "stream")) {
+      delete d;
+      return nullptr;
+    }
+    for (auto &e : d->ev) cudaEventCreate(&e);
+    eng->dev = d;
+  }
+  return eng->dev;
+}
+
+void free_engine(bwc_codec *codec) {
+  if (!codec || !codec->tile) return;
+  delete codec->tile->dev;
+  delete codec->tile;
+  codec->tile = nullptr;
+}
+
+static bool is_device_pointer(const void *p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+static DwtPlan make_plan(const bwc_gl_ctrl &c, const Parameter &par) {
+  DwtPlan plan{};
+  plan.levels = c.nDecomp;
+  const uint8_t dec[4] = {c.decompX, c.decompY, c.decompZ, c.decompTS};
+  for (int l = 0; l < c.nDecomp; ++l) {
+    const Box &b = par.res[c.nDecomp - l].box;
+    const uint64_t e[4] = {b.X1 - b.X0, b.Y1 - b.Y0, b.Z1 - b.Z0, b.TS1 - b.TS0};
+    for (int a = 0; a < 4; ++a) {
+      plan.ext[l][a] = e[a];
+      if (l < dec[a] && e[a] > 1) plan.axis_on[l] |= (uint8_t)(1 << a);
+    }
+  }
+  return plan;
+}
+
+static void build_tables(const Parameter &par, bool compress, std::vector<CbDev> &cbs,
+                         std::vector<SbDev> &sbs, uint64_t *bytes_total, uint64_t *scratch_total,
+                         uint32_t *max_cols) {
+  sbs.clear();
+  for (const Subband &s : par.subbands) {
+    SbDev d;
+    double g = (double)s.dwt_gain;
+    g *= (double)(bwc_float)(s.qt_step * s.qt_step);
+    d.gain_step2 = g;
+    d.qt_eff = s.qt_eff;
+    d.Kmax = s.Kmax;
+    d.cls = sig_class(s.highband);
+    sbs.push_back(d);
+  }
+  cbs.clear();
+  uint64_t off = 0, soff = 0;
+  uint32_t mc = 0;
+  for (const Codeblock &cb : par.codeblocks) {
+    CbDev d;
+    d.x0 = (uint32_t)cb.box.X0;
+    d.y0 = (uint32_t)cb.box.Y0;
+    d.z0 = (uint32_t)cb.box.Z0;
+    d.t0 = (uint32_t)cb.box.TS0;
+    d.w = (uint32_t)(cb.box.X1 - cb.box.X0);
+    d.h = (uint32_t)(cb.box.Y1 - cb.box.Y0);
+    d.d = (uint32_t)(cb.box.Z1 - cb.box.Z0);
+    d.nt = (uint32_t)(cb.box.TS1 - cb.box.TS0);
+    d.sb = cb.subband;
+    const uint64_t nsamp = (uint64_t)d.w * d.h * d.d * d.nt;
+    const uint32_t ncols = d.w * ((d.h + 3) / 4) * d.d * d.nt;
+    mc = std::max(mc, ncols);
+    if (compress) {
+      const uint64_t cap = nsamp * (kPrecByte + 1) + 64;
+      d.out_off = off;
+      d.out_cap = (uint32_t)std::min<uint64_t>(cap, 0xFFFFFFF0u);
+      off += (cap + 15) & ~15ull;
+      d.scratch_off = soff;
+      soff += (((uint64_t)ncols * (2 + kPrecBit + 1)) + 15) & ~15ull;
+    } else {
+      d.out_off = 0;   // filled by the caller
+      d.out_cap = 0;
+      d.scratch_off = soff;   // elements of the magnitude scratch
+      soff += (uint64_t)ncols * 4;
+    }
+    cbs.push_back(d);
+  }
+  *bytes_total = off;
+  *scratch_total = soff;
+  *max_cols = mc;
+}
+
+static int t1_grid(const void *kernel_unused, size_t smem_per_block) {
+  (void)kernel_unused;
+  int dev = 0, sms = 148, smem_max = 227 * 1024;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  int per_sm = (int)std::max<size_t>(1, std::min<size_t>(16, smem_max / (smem_per_block + 1024)));
+  return sms * per_sm;
+}
+
+// ---------------------------------------------------------------------------------------------
+static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
+  bwc_b200_engine *eng = codec->tile;
+  if (!eng || eng->tiles.empty()) {
+    warn("o##########################################################o\n"
+         "| ERROR: bwc_create_compression has not been called        |\n"
+         "o##########################################################o\n");
+    return 0;
+  }
+  DeviceState *dv = device_state(codec);
+  if (!dv) return 0;
+  cudaStream_t s = dv->stream;
+  bwc_gl_ctrl &c = codec->control;
+  bwc_gl_inf &info = codec->info;
+  Tile &tile = eng->tiles[0];
+  const uint64_t n = tile.box.size();
+  const size_t dsz = (info.data_prec == bwc_precision_double) ? 8 : 4;
+  const uint64_t in_bytes = info.nX * info.nY * info.nZ * info.nTS * (uint64_t)info.nPar * dsz;
+  const FieldDims dims{tile.box.nx(), tile.box.ny(), tile.box.nz(), tile.box.nt()};
+
+  cudaEventRecord(dv->ev[0], s);
+  const uint8_t *src = (const uint8_t *)stream->inp;
+  if (!is_device_pointer(stream->inp)) {
+    if (!dv->in.ensure(in_bytes)) return 0;
+    if (!cuda_ok(cudaMemcpyAsync(dv->in.p, stream->inp, in_bytes, cudaMemcpyHostToDevice, s), "upload"))
+      return 0;
+    src = dv->in.as<uint8_t>();
+  }
+  cudaEventRecord(dv->ev[1], s);
+
+  // tables and output regions of every parameter
+  std::vector<std::vector<CbDev>> cbs(info.nPar);
+  std::vector<std::vector<SbDev>> sbs(info.nPar);
+  std::vector<uint64_t> cb_base(info.nPar + 1, 0), byte_base(info.nPar + 1, 0),
+      scr_base(info.nPar + 1, 0), sb_base(info.nPar + 1, 0);
+  uint32_t max_cols = 0;
+  for (int p = 0; p < info.nPar; ++p) {
+    uint64_t bt, st;
+    uint32_t mc;
+    build_tables(tile.params[p], true, cbs[p], sbs[p], &bt, &st, &mc);
+    max_cols = std::max(max_cols, mc);
+    cb_base[p + 1] = cb_base[p] + cbs[p].size();
+    byte_base[p + 1] = byte_base[p] + bt;
+    scr_base[p + 1] = scr_base[p] + st;
+    sb_base[p + 1] = sb_base[p] + sbs[p].size();
+    for (CbDev &d : cbs[p]) {
+      d.out_off += byte_base[p];
+      d.scratch_off += scr_base[p];
+      d.sb += (uint32_t)sb_base[p];
+    }
+  }
+  const uint64_t ncb = cb_base[info.nPar];
+  std::vector<CbDev> allcb;
+  std::vector<SbDev> allsb;
+  for (int p = 0; p < info.nPar; ++p) {
+    allcb.insert(allcb.end(), cbs[p].begin(), cbs[p].end());
+    allsb.insert(allsb.end(), sbs[p].begin(), sbs[p].end());
+  }
+  if (!dv->work.ensure(n * sizeof(bwc_float)) || !dv->keys.ensure(16 * info.nPar) ||
+      !dv->stats.ensure(4 * sizeof(bwc_float) * info.nPar) ||
+      !dv->cbtab.ensure(sizeof(CbDev) * ncb) || !dv->sbtab.ensure(sizeof(SbDev) * allsb.size()) ||
+      !dv->bytes.ensure(byte_base[info.nPar]) || !dv->scratch.ensure(scr_base[info.nPar]) ||
+      !dv->snaps.ensure(ncb * kMaxPasses * 16) || !dv->dmse.ensure(ncb * kMaxPasses * 8) ||
+      !dv->K.ensure(ncb) || !dv->Z.ensure(ncb) || !dv->L.ensure(ncb * kMaxPasses * 4) ||
+      !dv->S.ensure(ncb * (kMaxPasses + 1) * 2) || !dv->flags.ensure(ncb * 4) ||
+      !dv->slopes.ensure(8) || !dv->counter.ensure(4 * info.nPar))
+    return 0;
+  cudaMemcpyAsync(dv->cbtab.p, allcb.data(), sizeof(CbDev) * ncb, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(dv->sbtab.p, allsb.data(), sizeof(SbDev) * allsb.size(), cudaMemcpyHostToDevice, s);
+  {
+    const uint32_t init[2] = {0xFFFF, 0};
+    cudaMemcpyAsync(dv->slopes.p, init, 8, cudaMemcpyHostToDevice, s);
+  }
+  cudaMemsetAsync(dv->flags.p, 0, ncb * 4, s);
+  cudaMemsetAsync(dv->counter.p, 0, 4 * info.nPar, s);
+  cudaMemsetAsync(dv->keys.p, 0, 16 * info.nPar, s);
+  for (int p = 0; p < info.nPar; ++p) cudaMemsetAsync(dv->keys.as<uint64_t>() + 2 * p, 0xFF, 8, s);
+
+  const uint32_t state_cap = std::min<uint32_t>(max_cols, 6144);
+  const size_t smem = (32 * 2 + 32 * 12) * 4 + (size_t)state_cap * 2 * 4;
+  const int grid = t1_grid(nullptr, smem);
+  float t_norm = 0, t_dwt = 0, t_t1 = 0;
+  for (int p = 0; p < info.nPar; ++p) {
+    cudaEvent_t a, b2, c2, d2;
+    cudaEventCreate(&a); cudaEventCreate(&b2); cudaEventCreate(&c2); cudaEventCreate(&d2);
+    cudaEventRecord(a, s);
+    launch_fill_minmax(src + (uint64_t)p * n * dsz, dsz == 8, n, dv->work.as<bwc_float>(),
+                       dv->keys.as<uint64_t>() + 2 * p, s);
+    launch_normalize(dv->work.as<bwc_float>(), n, dv->keys.as<uint64_t>() + 2 * p, c.Qm,
+                     dv->stats.as<bwc_float>() + 4 * p, s);
+    if (p == 0 && dv->dump_set && dv->dump.normalized)
+      cudaMemcpyAsync(dv->dump.normalized, dv->work.p, n * sizeof(bwc_float), cudaMemcpyDeviceToHost, s);
+    cudaEventRecord(b2, s);
+    launch_dwt_forward(dv->work.as<bwc_float>(), dims, make_plan(c, tile.params[p]), s);
+    if (p == 0 && dv->dump_set && dv->dump.transformed)
+      cudaMemcpyAsync(dv->dump.transformed, dv->work.p, n * sizeof(bwc_float), cudaMemcpyDeviceToHost, s);
+    cudaEventRecord(c2, s);
+    T1EncOut o;
+    o.bytes = dv->bytes.as<uint8_t>();
+    o.K = dv->K.as<uint8_t>() + cb_base[p];
+    o.Z = dv->Z.as<uint8_t>() + cb_base[p];
+    o.L = dv->L.as<uint32_t>() + cb_base[p] * kMaxPasses;
+    o.S = dv->S.as<uint16_t>() + cb_base[p] * (kMaxPasses + 1);
+    o.slopes = dv->slopes.as<uint32_t>();
+    o.flags = dv->flags.as<uint32_t>() + cb_base[p];
+    o.planes = dv->scratch.as<uint8_t>();
+    o.snaps = dv->snaps.as<uint64_t>() + cb_base[p] * kMaxPasses * 2;
+    o.dmse = dv->dmse.as<int64_t>() + cb_base[p] * kMaxPasses;
+    launch_t1_encode_ex(dv->work.as<bwc_float>(), dims, dv->cbtab.as<CbDev>() + cb_base[p],
+                        (uint32_t)cbs[p].size(), dv->sbtab.as<SbDev>(), c.error_resilience, o,
+                        state_cap, dv->scratch.as<uint16_t>(), dv->counter.as<uint32_t>() + p,
+                        grid, s);
+    cudaEventRecord(d2, s);
+    if (!cuda_ok(cudaStreamSynchronize(s), "compression kernels")) return 0;
+    float x;
+    cudaEventElapsedTime(&x, a, b2); t_norm += x;
+    cudaEventElapsedTime(&x, b2, c2); t_dwt += x;
+    cudaEventElapsedTime(&x, c2, d2); t_t1 += x;
+    cudaEventDestroy(a); cudaEventDestroy(b2); cudaEventDestroy(c2); cudaEventDestroy(d2);
+  }
+
+  // tier-1 summary to the host
+  cudaEventRecord(dv->ev[2], s);
+  std::vector<uint8_t> hK(ncb), hZ(ncb);
+  std::vector<uint32_t> hL(ncb * kMaxPasses), hflags(ncb), hslopes(2);
+  std::vector<uint16_t> hS(ncb * (kMaxPasses + 1));
+  std::vector<bwc_float> hstats(4 * info.nPar);
+  cudaMemcpyAsync(hK.data(), dv->K.p, ncb, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hZ.data(), dv->Z.p, ncb, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hL.data(), dv->L.p, ncb * kMaxPasses * 4, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hS.data(), dv->S.p, ncb * (kMaxPasses + 1) * 2, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hflags.data(), dv->flags.p, ncb * 4, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hslopes.data(), dv->slopes.p, 8, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hstats.data(), dv->stats.p, 4 * sizeof(bwc_float) * info.nPar,
+                  cudaMemcpyDeviceToHost, s);
+  cudaEventRecord(dv->ev[3], s);
+  if (!cuda_ok(cudaStreamSynchronize(s), "tier-1 download")) return 0;
+
+  for (uint64_t i = 0; i < ncb; ++i) {
+    if (hflags[i] & 1u) {
+      warn("o##########################################################o\n"
+           "| ERROR: tier-1 output exceeded its codeblock buffer       |\n"
+           "o##########################################################o\n");
+      return 0;
+    }
+  }
+  if (dv->dump_set) {
+    const bwc_b200_stage_dump &d = dv->dump;
+    const uint64_t n0 = cbs[0].size();
+    if (d.K) std::memcpy(d.K, hK.data(), n0);
+    if (d.Z) std::memcpy(d.Z, hZ.data(), n0);
+    if (d.L) std::memcpy(d.L, hL.data(), n0 * kMaxPasses * 4);
+    if (d.S) std::memcpy(d.S, hS.data(), n0 * (kMaxPasses + 1) * 2);
+    if (d.flags) std::memcpy(d.flags, hflags.data(), n0 * 4);
+    if (d.stats) std::memcpy(d.stats, hstats.data(), 4 * sizeof(bwc_float));
+    if (d.bytes && d.byte_offsets) {
+      uint64_t pos = 0;
+      for (uint64_t i = 0; i < n0; ++i) {
+        const uint64_t len = hZ[i] ? hL[i * kMaxPasses + hZ[i] - 1] : 0;
+        d.byte_offsets[i] = pos;
+        if (pos + len <= d.bytes_cap && len)
+          cudaMemcpy(d.bytes + pos, dv->bytes.as<uint8_t>() + cbs[0][i].out_off, len,
+                     cudaMemcpyDeviceToHost);
+        pos += len;
+      }
+    }
+  }
+  for (int p = 0; p < info.nPar; ++p) {
+    Parameter &par = tile.params[p];
+    par.pmin = hstats[4 * p + 0];
+    par.pmax = hstats[4 * p + 1];
+    par.alpha = hstats[4 * p + 2];
+    par.beta = hstats[4 * p + 3];
+    for (uint64_t i = 0; i < cbs[p].size(); ++i) {
+      const uint64_t g = cb_base[p] + i;
+      Codeblock &cb = par.codeblocks[i];
+      CodedBlock &e = cb.enc;
+      e.K = hK[g];
+      e.Z = hZ[g];
+      e.Kmsbs = e.K ? (uint8_t)(par.subbands[cb.subband].Kmax - e.K) : 0;
+      for (int j = 0; j < e.Z; ++j) e.L[j] = hL[g * kMaxPasses + j];
+      for (int j = 0; j <= e.Z; ++j) e.S[j] = hS[g * (kMaxPasses + 1) + j];
+      cb.data_off = cbs[p][i].out_off;
+      cb.data_cap = cbs[p][i].out_cap;
+    }
+  }
+  tile.slope_min = (uint16_t)hslopes[0];
+  tile.slope_max = (uint16_t)hslopes[1];
+
+  // tier 2 on the host
+  cudaEvent_t t2a;
+  cudaEventCreate(&t2a);
+  const auto h0 = std::chrono::steady_clock::now();
+  if (t2_encode(codec, tile)) return 0;
+  std::vector<uint8_t> blob;
+  std::vector<GatherPiece> pieces;
+  const uint64_t total = layout_codestream(codec, stream, blob, pieces);
+  const auto h1 = std::chrono::steady_clock::now();
+  if (!total) return 0;
+
+  // codestream assembly on the device
+  cudaEventRecord(dv->ev[4], s);
+  if (!dv->blob.ensure(blob.size()) || !dv->pieces.ensure(pieces.size() * sizeof(GatherPiece)))
+    return 0;
+  cudaMemcpyAsync(dv->blob.p, blob.data(), blob.size(), cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(dv->pieces.p, pieces.data(), pieces.size() * sizeof(GatherPiece),
+                  cudaMemcpyHostToDevice, s);
+  const bool out_dev = is_device_pointer(stream->out);
+  uint8_t *csdst;
+  if (out_dev) {
+    csdst = (uint8_t *)stream->out;
+  } else {
+    if (!dv->cs.ensure(total)) return 0;
+    csdst = dv->cs.as<uint8_t>();
+  }
+  launch_gather(csdst, dv->blob.as<uint8_t>(), dv->bytes.as<uint8_t>(),
+                dv->pieces.as<GatherPiece>(), pieces.size(), s);
+  if (!out_dev) cudaMemcpyAsync(stream->out, csdst, total, cudaMemcpyDeviceToHost, s);
+  cudaEventRecord(dv->ev[5], s);
+  if (!cuda_ok(cudaStreamSynchronize(s), "codestream assembly")) return 0;
+  cudaEventDestroy(t2a);
+
+  float up = 0, dl = 0, as = 0;
+  cudaEventElapsedTime(&up, dv->ev[0], dv->ev[1]);
+  cudaEventElapsedTime(&dl, dv->ev[2], dv->ev[3]);
+  cudaEventElapsedTime(&as, dv->ev[4], dv->ev[5]);
+  dv->timings[0] = up;
+  dv->timings[1] = t_norm;
+  dv->timings[2] = t_dwt;
+  dv->timings[3] = t_t1;
+  dv->timings[4] = dl;
+  dv->timings[5] = std::chrono::duration<double, std::milli>(h1 - h0).count();
+  dv->timings[6] = as;
+  dv->timings[7] = up + t_norm + t_dwt + t_t1 + dl + dv->timings[5] + as;
+  dv->dump_set = false;
+  return total;
+}
+
+// ---------------------------------------------------------------------------------------------
+static uchar decompress_impl(bwc_codec *codec, bwc_stream *stream) {
+  bwc_b200_engine *eng = codec->tile;
+  if (!eng || eng->tiles.empty()) {
+    warn(kCsError);
+    return 1;
+  }
+  DeviceState *dv = device_state(codec);
+  if (!dv) return 1;
+  cudaStream_t s = dv->stream;
+  bwc_gl_ctrl &c = codec->control;
+  bwc_gl_inf &info = codec->info;
+  Tile &tile = eng->tiles[0];
+  const uint64_t n = tile.box.size();
+  const size_t dsz = (info.data_prec == bwc_precision_double) ? 8 : 4;
+  const uint64_t out_bytes = info.nX * info.nY * info.nZ * info.nTS * (uint64_t)info.nPar * dsz;
+  const FieldDims dims{tile.box.nx(), tile.box.ny(), tile.box.nz(), tile.box.nt()};
+  const uint64_t cs_len = c.codestreamSize;
+
+  cudaEventRecord(dv->ev[0], s);
+  const uint8_t *dcs = (const uint8_t *)stream->inp;
+  if (!is_device_pointer(stream->inp)) {
+    if (!dv->cs.ensure(cs_len)) return 1;
+    cudaMemcpyAsync(dv->cs.p, stream->inp, cs_len, cudaMemcpyHostToDevice, s);
+    dcs = dv->cs.as<uint8_t>();
+  }
+  const bool out_dev = is_device_pointer(stream->out);
+  uint8_t *dout = (uint8_t *)stream->out;
+  if (!out_dev) {
+    if (!dv->outbuf.ensure(out_bytes)) return 1;
+    dout = dv->outbuf.as<uint8_t>();
+  }
+  cudaEventRecord(dv->ev[1], s);
+  float t_t1 = 0, t_dwt = 0, t_norm = 0;
+  for (int p = 0; p < info.nPar; ++p) {
+    Parameter &par = tile.params[p];
+    std::vector<CbDev> cbs;
+    std::vector<SbDev> sbs;
+    uint64_t bt, st;
+    uint32_t mc;
+    build_tables(par, false, cbs, sbs, &bt, &st, &mc);
+    const uint64_t ncb = cbs.size();
+    std::vector<uint8_t> hK(ncb), hZ(ncb);
+    std::vector<uint32_t> hLmax(ncb);
+    std::vector<GatherPiece> pieces;
+    uint64_t off = 0;
+    for (uint64_t i = 0; i < ncb; ++i) {
+      Codeblock &cb = par.codeblocks[i];
+      const Subband &sb = par.subbands[cb.subband];
+      hK[i] = (uint8_t)(sb.Kmax - cb.enc.Kmsbs);
+      hZ[i] = cb.enc.Z;
+      hLmax[i] = cb.enc.Z ? (uint32_t)cb.enc.L[cb.enc.Z - 1] : 0;
+      cbs[i].out_off = off;
+      uint64_t pos = off;
+      for (auto &ch : cb.chunks) {
+        if (ch.second) pieces.push_back({ch.first, pos, ch.second, 1});
+        pos += ch.second;
+      }
+      off += ((std::max<uint64_t>(pos - off, hLmax[i]) + 16) + 15) & ~15ull;
+    }
+    const uint32_t state_cap = std::min<uint32_t>(mc, 6144);
+    const size_t smem = 32 * 4 + (size_t)state_cap * 2 * 4;
+    const bool big = mc > state_cap;
+    uint64_t gstate_bytes = 0;
+    if (big)
+      for (uint64_t i = 0; i < ncb; ++i) gstate_bytes = std::max<uint64_t>(gstate_bytes, cbs[i].scratch_off);
+    if (!dv->work.ensure(n * sizeof(bwc_float)) || !dv->cbtab.ensure(sizeof(CbDev) * ncb) ||
+        !dv->sbtab.ensure(sizeof(SbDev) * sbs.size()) || !dv->bytes.ensure(off + 64) ||
+        !dv->mags.ensure(st * sizeof(bwc_raw)) || !dv->K.ensure(ncb) || !dv->Z.ensure(ncb) ||
+        !dv->lmax.ensure(ncb * 4) || !dv->flags.ensure(ncb * 4) || !dv->counter.ensure(4) ||
+        !dv->pieces.ensure(pieces.size() * sizeof(GatherPiece) + 16) ||
+        (big && !dv->scratch.ensure(st * 2 + 64)))
+      return 1;
+    cudaMemcpyAsync(dv->cbtab.p, cbs.data(), sizeof(CbDev) * ncb, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dv->sbtab.p, sbs.data(), sizeof(SbDev) * sbs.size(), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dv->K.p, hK.data(), ncb, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dv->Z.p, hZ.data(), ncb, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dv->lmax.p, hLmax.data(), ncb * 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dv->pieces.p, pieces.data(), pieces.size() * sizeof(GatherPiece),
+                    cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(dv->bytes.p, 0, off + 64, s);
+    cudaMemsetAsync(dv->flags.p, 0, ncb * 4, s);
+    cudaMemsetAsync(dv->counter.p, 0, 4, s);
+    launch_gather(dv->bytes.as<uint8_t>(), dcs, nullptr, dv->pieces.as<GatherPiece>(),
+                  pieces.size(), s);
+    cudaEvent_t a, b2, c2, d2;
+    cudaEventCreate(&a); cudaEventCreate(&b2); cudaEventCreate(&c2); cudaEventCreate(&d2);
+    cudaEventRecord(a, s);
+    cudaMemsetAsync(dv->work.p, 0, n * sizeof(bwc_float), s);
+    const int grid = t1_grid(nullptr, smem);
+    launch_t1_decode_ex(dv->work.as<bwc_float>(), dims, dv->cbtab.as<CbDev>(), (uint32_t)ncb,
+                        dv->sbtab.as<SbDev>(), dv->bytes.as<uint8_t>(), dv->K.as<uint8_t>(),
+                        dv->Z.as<uint8_t>(), dv->lmax.as<uint32_t>(), c.error_resilience,
+                        dv->mags.as<bwc_raw>(), dv->flags.as<uint32_t>(), state_cap,
+                        big ? dv->scratch.as<uint16_t>() : nullptr, dv->counter.as<uint32_t>(),
+                        grid, s);
+    if (p == 0 && dv->ddump_set && dv->ddump.dequantized)
+      cudaMemcpyAsync(dv->ddump.dequantized, dv->work.p, n * sizeof(bwc_float), cudaMemcpyDeviceToHost, s);
+    cudaEventRecord(b2, s);
+    launch_dwt_inverse(dv->work.as<bwc_float>(), dims, make_plan(c, par), s);
+    if (p == 0 && dv->ddump_set && dv->ddump.reconstructed)
+      cudaMemcpyAsync(dv->ddump.reconstructed, dv->work.p, n * sizeof(bwc_float), cudaMemcpyDeviceToHost, s);
+    cudaEventRecord(c2, s);
+    launch_denormalize(dv->work.as<bwc_float>(), n, par.pmin, par.pmax, c.Qm,
+                       dout + (uint64_t)p * n * dsz, dsz == 8, s);
+    cudaEventRecord(d2, s);
+    if (!cuda_ok(cudaStreamSynchronize(s), "decompression kernels")) return 1;
+    float x;
+    cudaEventElapsedTime(&x, a, b2); t_t1 += x;
+    cudaEventElapsedTime(&x, b2, c2); t_dwt += x;
+    cudaEventElapsedTime(&x, c2, d2); t_norm += x;
+    cudaEventDestroy(a); cudaEventDestroy(b2); cudaEventDestroy(c2); cudaEventDestroy(d2);
+  }
+  cudaEventRecord(dv->ev[2], s);
+  if (!out_dev) cudaMemcpyAsync(stream->out, dout, out_bytes, cudaMemcpyDeviceToHost, s);
+  cudaEventRecord(dv->ev[3], s);
+  if (!cuda_ok(cudaStreamSynchronize(s), "decompression download")) return 1;
+  float up = 0, dl = 0;
+  cudaEventElapsedTime(&up, dv->ev[0], dv->ev[1]);
+  cudaEventElapsedTime(&dl, dv->ev[2], dv->ev[3]);
+  dv->timings[0] = up;
+  dv->timings[1] = t_norm;
+  dv->timings[2] = t_dwt;
+  dv->timings[3] = t_t1;
+  dv->timings[4] = 0;
+  dv->timings[5] = 0;
+  dv->timings[6] = dl;
+  dv->timings[7] = up + t_norm + t_dwt + t_t1 + dl;
+  dv->ddump_set = false;
+  return 0;
+}
+
+}  // namespace bwcb
+
+using namespace bwcb;
+
+extern "C" size_t bwc_compress(bwc_codec *const codec, bwc_stream *const data) {
+  if (!codec || !data) return 0;
+  return compress_impl(codec, data);
+}
+
+extern "C" uchar bwc_decompress(bwc_codec *const codec, bwc_stream *const stream) {
+  if (!codec || !stream) return 1;
+  return decompress_impl(codec, stream);
+}
+
+extern "C" int bwc_b200_precision_bits(void) { return kPrecBit; }
+
+extern "C" void bwc_b200_reset_gain_state(void) { reset_gain_lut(); }
+
+extern "C" void bwc_b200_get_gain_state(double *out30) { copy_gain_lut(out30); }
+
+extern "C" uint64 bwc_b200_num_codeblocks(bwc_codec *const codec, uint8 const param) {
+  if (!codec || !codec->tile || codec->tile->tiles.empty()) return 0;
+  if (param >= codec->tile->tiles[0].params.size()) return 0;
+  return codec->tile->tiles[0].params[param].codeblocks.size();
+}
+
+extern "C" void bwc_b200_set_stage_dump(bwc_codec *const codec, bwc_b200_stage_dump const *dump) {
+  DeviceState *d = device_state(codec);
+  if (!d) return;
+  d->dump_set = dump != nullptr;
+  if (dump) d->dump = *dump;
+}
+
+extern "C" void bwc_b200_set_decode_dump(bwc_codec *const codec, bwc_b200_decode_dump const *dump) {
+  DeviceState *d = device_state(codec);
+  if (!d) return;
+  d->ddump_set = dump != nullptr;
+  if (dump) d->ddump = *dump;
+}
+
+extern "C" int bwc_b200_last_timings(bwc_codec *const codec, double *out_ms, int n) {
+  if (!codec || !codec->tile || !codec->tile->dev) return 0;
+  const int k = std::min(n, 8);
+  for (int i = 0; i < k; ++i) out_ms[i] = codec->tile->dev->timings[i];
+  return k;
+}

@@ -1,0 +1,89 @@
+// Host-only inspection entry points (declared in bwc_b200.h).
+//
+// They expose the codec geometry, the parsed state of a decompression codec, and the tier-2 +
+// codestream stage on caller-supplied tier-1 results.  None of them codes samples: the
+// compression and decompression paths proper run on the GPU only.
+#include <cstring>
+
+#include "bwc_b200.h"
+#include "common.hpp"
+
+using namespace bwcb;
+
+static Parameter *param_of(bwc_codec *codec, uint8 p) {
+  if (!codec || !codec->tile || codec->tile->tiles.empty()) return nullptr;
+  Tile &t = codec->tile->tiles[0];
+  return p < t.params.size() ? &t.params[p] : nullptr;
+}
+
+extern "C" int bwc_b200_codeblock_geometry(bwc_codec *const codec, uint8 const param,
+                                           uint64 const c, uint64 *geom10) {
+  Parameter *par = param_of(codec, param);
+  if (!par || c >= par->codeblocks.size()) return 1;
+  const Codeblock &cb = par->codeblocks[c];
+  const Subband &sb = par->subbands[cb.subband];
+  const uint64 g[10] = {cb.box.X0, cb.box.Y0, cb.box.Z0, cb.box.TS0, cb.box.X1,
+                        cb.box.Y1, cb.box.Z1, cb.box.TS1, sb.highband, sb.Kmax};
+  std::memcpy(geom10, g, sizeof(g));
+  return 0;
+}
+
+extern "C" int bwc_b200_subband_steps(bwc_codec *const codec, uint8 const param, uint64 const c,
+                                      double *out3) {
+  Parameter *par = param_of(codec, param);
+  if (!par || c >= par->codeblocks.size()) return 1;
+  const Subband &sb = par->subbands[par->codeblocks[c].subband];
+  out3[0] = sb.qt_eff;
+  out3[1] = sb.qt_step;
+  out3[2] = sb.dwt_gain;
+  return 0;
+}
+
+extern "C" int bwc_b200_parsed_codeblock(bwc_codec *const codec, uint8 const param,
+                                         uint64 const c, int64 *meta3, uint64 *L) {
+  Parameter *par = param_of(codec, param);
+  if (!par || c >= par->codeblocks.size()) return 1;
+  const Codeblock &cb = par->codeblocks[c];
+  meta3[0] = par->subbands[cb.subband].Kmax - cb.enc.Kmsbs;
+  meta3[1] = cb.enc.Kmsbs;
+  meta3[2] = cb.enc.Z;
+  if (L) std::memcpy(L, cb.enc.L, sizeof(cb.enc.L));
+  return 0;
+}
+
+extern "C" size_t bwc_b200_assemble_from_tier1(bwc_codec *const codec, bwc_stream *const stream,
+                                               uint8 const *K, uint8 const *Z, uint64 const *L,
+                                               uint16 const *S, uint8 const *bytes,
+                                               uint64 const *byte_offsets,
+                                               bwc_float const *minmax, uint16 const slope_min,
+                                               uint16 const slope_max) {
+  if (!codec || !codec->tile || codec->tile->tiles.empty()) return 0;
+  Tile &tile = codec->tile->tiles[0];
+  uint64_t g = 0;
+  for (size_t p = 0; p < tile.params.size(); ++p) {
+    Parameter &par = tile.params[p];
+    par.pmin = minmax[2 * p];
+    par.pmax = minmax[2 * p + 1];
+    for (Codeblock &cb : par.codeblocks) {
+      CodedBlock &e = cb.enc;
+      e.K = K[g];
+      e.Z = Z[g];
+      e.Kmsbs = e.K ? (uint8_t)(par.subbands[cb.subband].Kmax - e.K) : 0;
+      for (int j = 0; j < e.Z; ++j) e.L[j] = L[g * kMaxPasses + j];
+      for (int j = 0; j <= e.Z; ++j) e.S[j] = S[g * (kMaxPasses + 1) + j];
+      cb.data_off = byte_offsets[g];
+      ++g;
+    }
+  }
+  tile.slope_min = slope_min;
+  tile.slope_max = slope_max;
+  if (t2_encode(codec, tile)) return 0;
+  std::vector<uint8_t> blob;
+  std::vector<GatherPiece> pieces;
+  const uint64_t total = layout_codestream(codec, stream, blob, pieces);
+  if (!total) return 0;
+  uint8_t *out = (uint8_t *)stream->out;
+  for (const GatherPiece &pc : pieces)
+    std::memcpy(out + pc.dst, (pc.from_blob ? blob.data() : bytes) + pc.src, pc.size);
+  return total;
+}

@@ -1,0 +1,362 @@
+// Tier-2: PCRD rate control, packet headers and packet parsing.
+//
+// Rate control is the reference's per-layer bisection over 16-bit log slopes
+// (tier2.c:1115-1254): every probe truncates each codeblock at its last pass whose slope is at
+// or above the threshold, sums the body bytes and estimates every packet header
+// (tier2.c:896-1079, :434-711).  The probe results feed a trajectory-dependent search (exact
+// exits on equality, the `tmp` fallback), so the same arithmetic -- including its quirks, such
+// as adding L[0] for a codeblock whose previous layer stopped after one pass -- is kept here.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+
+#include "common.hpp"
+
+namespace bwcb {
+
+// (uint16)log2(x) of the reference for positive integers; x == 0 gives 0 (log2(0) = -inf,
+// which x86-64 converts to the integer-indefinite value whose low 16 bits are 0)
+static inline uint16_t ilog2_u16(uint64_t x) {
+  if (!x) return 0;
+  return (uint16_t)(63 - __builtin_clzll(x));
+}
+
+static void encode_delta_z(BitWriter &bw, int dz) {
+  if (dz == 1) {
+    bw.emit(0);
+  } else if (dz == 2) {
+    bw.emit(1); bw.emit(0);
+  } else if (dz < 6) {
+    dz -= 3;
+    bw.emit(1); bw.emit(1);
+    bw.emit(dz & 2); bw.emit(dz & 1);
+  } else if (dz < 37) {
+    dz -= 6;
+    for (int i = 0; i < 4; ++i) bw.emit(1);
+    for (int b = 4; b >= 0; --b) bw.emit(dz & (1 << b));
+  } else if (dz < 293) {
+    dz -= 37;
+    for (int i = 0; i < 9; ++i) bw.emit(1);
+    for (int b = 7; b >= 0; --b) bw.emit(dz & (1 << b));
+  }
+}
+
+static int decode_delta_z(BitReader &br) {
+  if (!br.get_bit()) return 1;
+  if (!br.get_bit()) return 2;
+  int dz = br.get_bit() << 1;
+  dz |= br.get_bit();
+  if (dz < 3) return dz + 3;
+  dz = 0;
+  for (int b = 4; b >= 0; --b) dz |= br.get_bit() << b;
+  if (dz < 31) return dz + 6;
+  dz = 0;
+  for (int b = 7; b >= 0; --b) dz |= br.get_bit() << b;
+  return dz + 37;
+}
+
+static void encode_length(BitWriter &bw, Codeblock &cb, int q, uchar estimate) {
+  int16_t *cp = cb.cp();
+  const int16_t z_curr = cp[q] - 1, z_prev = cp[q - 1] - 1;
+  uint16_t beta = (!estimate) ? cb.beta : cb.beta_est;
+  uint16_t max_beta = beta;
+  const uint32_t L = (uint32_t)(cb.enc.L[z_curr] - ((z_prev >= 0) ? cb.enc.L[z_prev] : 0));
+  const uint16_t cp_bits = ilog2_u16((uint64_t)(z_curr - z_prev));
+  int32_t L_bits = (int32_t)ilog2_u16(L) + 1 - cp_bits;
+  max_beta = (max_beta < L_bits) ? (uint16_t)L_bits : max_beta;
+  while (beta < max_beta) {
+    bw.emit(1);
+    beta++;
+  }
+  bw.emit(0);
+  const int sh = beta + cp_bits - 1;
+  int64_t bitv = (sh >= 0 && sh < 31) ? ((int64_t)1 << sh) : 0;
+  while (bitv > 0) {
+    bw.emit(L & (uint32_t)bitv);
+    bitv >>= 1;
+  }
+  if (estimate == 0) {
+    cb.beta = beta;
+    cb.beta_est = beta;
+  } else if (estimate == 1) {
+    cb.beta_est = beta;
+  }
+}
+
+// create_packet (tier2.c:434-711).  est: 0 final, 1 final-size estimate, 2 probe.
+static int64_t create_packet(Parameter &par, Resolution &res, uint32_t p, int q, uchar est) {
+  Packet &pk = res.packets[(uint64_t)q * res.nprec + p];
+  if (pk.e) {
+    BitWriter hdr;
+    hdr.mem.reserve(64);
+    if (!est) pk.pieces.clear();
+    hdr.emit(1);
+    for (uint8_t m = 0; m < res.nsub; ++m) {
+      const Subband &sb = par.subbands[res.first_subband + m];
+      Precinct &pr = par.precincts[sb.first_precinct + p];
+      for (uint64_t k = 0; k < pr.ncb; ++k) {
+        Codeblock &cb = par.codeblocks[pr.first_cb + k];
+        int16_t *cp = cb.cp();
+        const int dz = cp[q] - cp[q - 1];
+        if (cp[q - 1] == 0) {
+          tagtree_encode(pr.incl, hdr, (uint32_t)(q + 1), k, est);
+          if (cp[q])
+            for (uint32_t kk = 1; kk <= cb.enc.Kmsbs + 1u; ++kk)
+              tagtree_encode(pr.msbs, hdr, kk, k, est);
+        } else {
+          hdr.emit(dz);
+        }
+        if (dz) {
+          encode_delta_z(hdr, dz);
+          encode_length(hdr, cb, q, est);
+          if (est <= 1) {
+            const uint32_t start = (cp[q - 1] == 0) ? 0 : (uint32_t)cb.enc.L[cp[q - 1] - 1];
+            const uint32_t end = (cp[q] == 0) ? 0 : (uint32_t)cb.enc.L[cp[q] - 1];
+            if (est == 1)
+              pk.body_size += (uint32_t)(end - start);
+            else
+              pk.pieces.emplace_back(cb.data_off + start, (uint32_t)(end - start));
+          }
+        }
+      }
+    }
+    hdr.flush();
+    if (est) {
+      if (est == 2) pk.e = 0;
+      return (int64_t)hdr.mem.size();
+    }
+    pk.header = std::move(hdr.mem);
+    pk.size = pk.body_size + pk.header.size();
+    return (int64_t)pk.header.size();
+  }
+  if (est) {
+    if (est == 2) pk.e = 0;
+    return 1;
+  }
+  pk.size = 1;
+  pk.header.assign(1, 0);
+  return 1;
+}
+
+// create_quality_layer (tier2.c:896-1079)
+static int64_t create_quality_layer(bwc_codec *codec, Tile &tile, uint16_t threshold, int q,
+                                    uchar est) {
+  const bwc_gl_ctrl &c = codec->control;
+  int64_t size = 0;
+  for (Parameter &par : tile.params) {
+    for (Resolution &res : par.res) {
+      for (uint8_t m = 0; m < res.nsub; ++m) {
+        const Subband &sb = par.subbands[res.first_subband + m];
+        for (uint64_t p = 0; p < res.nprec; ++p) {
+          Precinct &pr = par.precincts[sb.first_precinct + p];
+          for (uint64_t k = 0; k < pr.ncb; ++k) {
+            Codeblock &cb = par.codeblocks[pr.first_cb + k];
+            int16_t *cp = cb.cp();
+            int16_t z;
+            for (z = cb.enc.Z; z >= 0 && cb.enc.S[z] < threshold; --z) {
+            }
+            if (z < cp[q - 1]) {
+              cp[q] = cp[q - 1];
+              if (cp[q] == 1) size += (int64_t)cb.enc.L[0];
+            } else {
+              cp[q] = z;
+              if (z > 0) {
+                size += (int64_t)cb.enc.L[z - 1];
+                if (z > 1 && (cp[q - 1] > 0)) size -= (int64_t)cb.enc.L[cp[q - 1] - 1];
+              }
+            }
+            if (cp[q] > cp[q - 1]) res.packets[(uint64_t)q * res.nprec + p].e = 1;
+            if (!est) {
+              if (q == 0) tagtree_set(pr.msbs, k, cb.enc.Kmsbs);
+              if (q + 1 == c.nLayers) {
+                uint8_t l;
+                for (l = 0; (l < c.nLayers) && (cb.cp()[l] == 0); ++l) {
+                }
+                tagtree_set(pr.incl, k, l);
+              }
+            }
+          }
+        }
+      }
+      for (uint64_t p = 0; p < res.nprec; ++p) {
+        const int64_t ph = create_packet(par, res, (uint32_t)p, q, est + 1);
+        if (ph < 0) return -1;
+        size += ph;
+      }
+    }
+  }
+  return size;
+}
+
+// create_quality_layers (tier2.c:1115-1254)
+static uchar create_quality_layers(bwc_codec *codec, Tile &tile) {
+  const bwc_gl_ctrl &c = codec->control;
+  const bwc_gl_inf &info = codec->info;
+  int64_t est_tile = 0, target = 0, est = 0;
+  const uint32_t main_header = (uint32_t)c.headerSize;
+  const uint64_t tile_size = tile.box.size() * (uint64_t)info.nPar;
+  const uint64_t header_size =
+      (uint64_t)ceilf((float)(main_header + tile.header_size) / (float)c.nLayers);
+  for (uint8_t l = 0; l < c.nLayers; ++l) {
+    uint16_t slope;
+    target = (int64_t)ceilf(c.bitrate[l] * (float)tile_size / 8.0f);
+    if ((float)target > 0.0f) {
+      uint16_t smin = tile.slope_min, smax = tile.slope_max;
+      uint16_t tmp = smin;
+      slope = smin;
+      while (smin < smax) {
+        slope = (uint16_t)((smax + smin) >> 1);
+        est = create_quality_layer(codec, tile, slope, l, 1);
+        if (est >= 0)
+          est += est_tile + (int64_t)header_size;
+        else
+          return 1;
+        if (est > target) {
+          if (smin == slope) smax = slope;
+          smin = slope;
+        } else if (est < target) {
+          if (smax == slope) smin = slope;
+          smax = slope;
+          tmp = slope;
+        } else {
+          smax = slope;
+          smin = slope;
+        }
+      }
+      if (est > target) slope = std::max(tmp, tile.slope_min);
+    } else {
+      slope = 0;
+    }
+    est = create_quality_layer(codec, tile, slope, l, 0);
+    if (est >= 0)
+      est_tile += est + (int64_t)header_size;
+    else
+      return 1;
+  }
+  return 0;
+}
+
+// create_packets (tier2.c:751-849): final headers for every packet, then the per-codeblock
+// coding state is cleared as in the reference.
+static uchar create_packets(bwc_codec *codec, Tile &tile) {
+  const bwc_gl_ctrl &c = codec->control;
+  for (Parameter &par : tile.params) {
+    for (Resolution &res : par.res) {
+      for (uint64_t p = 0; p < res.nprec; ++p) {
+        for (uint8_t l = 0; l < c.nLayers; ++l)
+          if (create_packet(par, res, (uint32_t)p, l, 0) < 0) return 1;
+        // the reference clears each codeblock's coding state once its packets exist
+        for (uint8_t m = 0; m < res.nsub; ++m) {
+          const Subband &sb = par.subbands[res.first_subband + m];
+          const Precinct &pr = par.precincts[sb.first_precinct + p];
+          for (uint64_t k = 0; k < pr.ncb; ++k) {
+            Codeblock &cb = par.codeblocks[pr.first_cb + k];
+            cb.enc = CodedBlock();
+            for (int l = 0; l < c.nLayers; ++l) cb.cp()[l] = 0;
+          }
+        }
+      }
+    }
+  }
+  return 0;
+}
+
+uchar t2_encode(bwc_codec *codec, Tile &tile) {
+  if (create_quality_layers(codec, tile)) return 1;
+  if (create_packets(codec, tile)) return 1;
+  return 0;
+}
+
+static void decode_length(BitReader &br, Codeblock &cb, int q) {
+  while (br.get_bit()) cb.beta++;
+  int16_t *cp = cb.cp();
+  const int16_t z_curr = cp[q] - 1, z_prev = cp[q - 1] - 1;
+  uint16_t L_bits = (uint16_t)(cb.beta + ilog2_u16((uint64_t)(z_curr - z_prev)));
+  uint32_t i = 0;
+  for (; L_bits > 0; --L_bits) {
+    i <<= 1;
+    i |= br.get_bit();
+  }
+  cb.enc.L[z_curr] = ((z_prev >= 0) ? cb.enc.L[z_prev] : 0) + i;
+}
+
+// parse_packet (tier2.c:1364-1684).  `pos` is the packet's first byte in the codestream,
+// `body_size` the tile body bytes still unread.  The body is taken to start where the bit
+// reader stopped (its byte index, not bytes_used), as in the reference.
+uchar parse_packet(bwc_codec *codec, Tile &tile, Packet &pk, const uint8_t *cs, uint64_t cs_len,
+                   uint64_t pos, uint64_t body_size) {
+  Parameter &par = tile.params[pk.c];
+  Resolution &res = par.res[pk.r];
+  const int q = pk.l;
+  BitReader br;
+  br.mem = cs + pos;
+  br.Lmax = (uint32_t)body_size;
+  if (pos + br.Lmax > cs_len) br.Lmax = cs_len - pos;
+  pk.e = br.get_bit();
+  for (uint8_t m = 0; m < res.nsub; ++m) {
+    const Subband &sb = par.subbands[res.first_subband + m];
+    Precinct &pr = par.precincts[sb.first_precinct + pk.p];
+    for (uint64_t k = 0; k < pr.ncb; ++k) {
+      Codeblock &cb = par.codeblocks[pr.first_cb + k];
+      int16_t *cp = cb.cp();
+      if (pk.e) {
+        int dz = 0;
+        if (cp[q - 1] == 0) {
+          tagtree_decode(pr.incl, br, (uint32_t)(q + 1), k);
+          if (pr.incl.nodes[k].value <= q) {
+            dz = 1;
+            uint32_t kk = 1;
+            while (tagtree_decode(pr.msbs, br, kk++, k)) {
+            }
+            cb.enc.Kmsbs = (uint8_t)pr.msbs.nodes[k].value;
+          }
+        } else {
+          dz = br.get_bit();
+        }
+        cp[q] = cp[q - 1];
+        if (dz) {
+          dz = decode_delta_z(br);
+          cp[q] += dz;
+          cb.enc.Z = (uint8_t)cp[q];
+          decode_length(br, cb, q);
+        }
+      } else {
+        cp[q] = cp[q - 1];
+      }
+    }
+  }
+  if (!pk.header_len) pk.header_len = br.bytes_used();
+  pk.header_pos = pos;
+  uint64_t body = pos + br.L;
+  if (codec->control.error_resilience) {
+    if (body + 2 > cs_len || cs[body] != 0xFF || cs[body + 1] != 0x92) return 1;
+    body += 2;
+    pk.header_len += 2;
+  }
+  pk.body_pos = body;
+  pk.body_size = 0;
+  if (pk.e) {
+    uint64_t at = body;
+    for (uint8_t m = 0; m < res.nsub; ++m) {
+      const Subband &sb = par.subbands[res.first_subband + m];
+      Precinct &pr = par.precincts[sb.first_precinct + pk.p];
+      for (uint64_t k = 0; k < pr.ncb; ++k) {
+        Codeblock &cb = par.codeblocks[pr.first_cb + k];
+        int16_t *cp = cb.cp();
+        if (cp[q] > cp[q - 1]) {
+          const uint32_t start = (cp[q - 1] == 0) ? 0 : (uint32_t)cb.enc.L[cp[q - 1] - 1];
+          const uint32_t end = (cp[q] == 0) ? 0 : (uint32_t)cb.enc.L[cp[q] - 1];
+          const uint32_t size = end - start;
+          if (at + size > cs_len) return 1;
+          cb.chunks.emplace_back(at, size);
+          at += size;
+          pk.body_size += size;
+        }
+      }
+    }
+  }
+  pk.size = pk.header_len + pk.body_size;
+  return 0;
+}
+
+}  // namespace bwcb

@@ -1,0 +1,90 @@
+// Host-visible interface of the CUDA kernels (plain C++; no CUDA types besides cudaStream_t).
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "../host/common.hpp"
+
+namespace bwcb {
+
+// One codeblock as the tier-1 kernels see it.
+struct CbDev {
+  uint32_t x0, y0, z0, t0;   // origin in the parameter's working buffer
+  uint32_t w, h, d, nt;      // extents along x, y, z, t
+  uint64_t out_off;          // byte offset of the codeblock's coded bytes
+  uint64_t scratch_off;      // compress: byte offset of its bit planes;
+                             // decompress: element offset of its magnitudes
+  uint32_t out_cap;          // compress: capacity of the coded-byte region
+  uint32_t sb;               // index into the SbDev table
+};
+
+// One subband.
+struct SbDev {
+  double gain_step2;   // (double)dwt_gain * (double)(qt_step_size * qt_step_size)
+  bwc_float qt_eff;    // qt_effective_step_size
+  uint32_t Kmax;
+  uint32_t cls;        // significance-context class: 0 low-pass, 1 high-pass, 2 diagonal
+};
+
+// Outputs of the tier-1 encoder.
+struct T1EncOut {
+  uint8_t *bytes;        // coded bytes, codeblock c at CbDev::out_off
+  uint8_t *K;            // [ncb]
+  uint8_t *Z;            // [ncb]
+  uint32_t *L;           // [ncb * kMaxPasses] truncation lengths
+  uint16_t *S;           // [ncb * (kMaxPasses + 1)] log slopes
+  uint32_t *slopes;      // [2]: min over non-zero slopes, max (atomics; init 0xFFFF / 0)
+  uint32_t *flags;       // [ncb]: bit 0 output overflow, bit 1 hull underflow
+  uint8_t *planes;       // scratch: bit planes, CbDev::scratch_off
+  uint64_t *snaps;       // scratch: [ncb * kMaxPasses * 2] end-of-pass coder states
+  int64_t *dmse;         // scratch: [ncb * kMaxPasses] distortion decrease per pass
+};
+
+struct FieldDims {
+  uint64_t width, height, depth, dt;
+};
+
+// field.cu
+void launch_fill_minmax(const void *src, bool src_double, uint64_t n, bwc_float *work,
+                        uint64_t *minmax_keys, cudaStream_t s);
+void launch_normalize(bwc_float *work, uint64_t n, const uint64_t *minmax_keys, uint8_t Qm,
+                      bwc_float *stats_out, cudaStream_t s);
+void launch_denormalize(const bwc_float *work, uint64_t n, bwc_float pmin, bwc_float pmax,
+                        uint8_t Qm, void *dst, bool dst_double, cudaStream_t s);
+
+// dwt.cu: the multi-level separable 9/7 transform of one parameter, in place.
+// level_ext[l] = extents (x, y, z, t) of the region transformed at level l; axis_on[l] bit a
+// set when axis a is transformed at level l.
+struct DwtPlan {
+  int levels;
+  uint64_t ext[16][4];
+  uint8_t axis_on[16];
+};
+void launch_dwt_forward(bwc_float *work, const FieldDims &dims, const DwtPlan &plan,
+                        cudaStream_t s);
+void launch_dwt_inverse(bwc_float *work, const FieldDims &dims, const DwtPlan &plan,
+                        cudaStream_t s);
+
+// t1_encode.cu: one warp per codeblock, codeblocks taken from *work_counter (zeroed by the
+// caller).  Codeblocks with more than state_cap stripe columns keep their column state in
+// gstate (at scratch_off) instead of shared memory.
+void launch_t1_encode_ex(const bwc_float *work, const FieldDims &dims, const CbDev *cbs,
+                         uint32_t ncb, const SbDev *sbs, uchar erres, const T1EncOut &out,
+                         uint32_t state_cap, uint16_t *gstate, uint32_t *work_counter, int grid,
+                         cudaStream_t s);
+
+// t1_decode.cu: decodes Z[c] passes of codeblock c from data + out_off (Lmax[c] bytes) and
+// writes the dequantised samples into the (zeroed) working buffer.
+void launch_t1_decode_ex(bwc_float *work, const FieldDims &dims, const CbDev *cbs, uint32_t ncb,
+                         const SbDev *sbs, const uint8_t *data, const uint8_t *K,
+                         const uint8_t *Z, const uint32_t *Lmax, uchar erres, bwc_raw *mags,
+                         uint32_t *flags, uint32_t state_cap, uint16_t *gstate,
+                         uint32_t *work_counter, int grid, cudaStream_t s);
+
+// gather.cu: dst[p.dst .. +size) = (p.from_blob ? blob : dev)[p.src .. +size)
+void launch_gather(uint8_t *dst, const uint8_t *blob, const uint8_t *dev,
+                   const GatherPiece *pieces, uint64_t npieces, cudaStream_t s);
+
+}  // namespace bwcb

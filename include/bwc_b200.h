@@ -1,0 +1,103 @@
+/*
+ * bwc_b200.h -- additional entry points of the B200 BigWhoop library.
+ *
+ * None of these has a counterpart in the reference API; they are additive exports beside the
+ * drop-in bwc.h interface.  Existing bwc_* signatures are unchanged.
+ *
+ * Device-resident buffers: bwc_compress and bwc_decompress accept CUDA device pointers as
+ * well as host pointers for stream->inp and stream->out (the pointer kind is queried with
+ * cudaPointerGetAttributes); device-resident input skips the host-to-device copy, a
+ * device-resident output receives the result by a device-to-device copy.
+ */
+#ifndef BWC_B200_H
+#define BWC_B200_H
+
+#include "bwc.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Library identification: returns PREC_BIT of this build (63 double, 31 single). */
+int bwc_b200_precision_bits(void);
+
+/* The reference keeps process-wide subband energy gains that every configure_codec and
+ * bwc_set_decomp call adds to (dwt.c:80, :808-1066); codestreams depend on that history.
+ * reset returns the table to its load-time state; get copies its 3 x 10 doubles. */
+void bwc_b200_reset_gain_state(void);
+void bwc_b200_get_gain_state(double *out30);
+
+/* Intermediate results of the next bwc_compress on `codec` (parameter 0 of tile 0), copied to
+ * host memory when the pointer is non-NULL:
+ *   normalized, transformed : the working buffer (tile-size bwc_float values) after
+ *                             normalisation and after the wavelet transform;
+ *   K, Z                    : per codeblock, in tier-1 order;
+ *   L                       : per codeblock MAXIMUM_NO_PASSES truncation lengths;
+ *   S                       : per codeblock MAXIMUM_NO_PASSES + 1 log slopes;
+ *   bytes / byte_offsets    : coded bytes of every codeblock (L[Z-1] each), packed in
+ *                             tier-1 order, and each codeblock's start in `bytes`;
+ *   stats                   : min, max, alpha, beta of parameter 0 (bwc_float).
+ * Capacities are the caller's: normalized/transformed hold the tile size, the per-codeblock
+ * arrays hold bwc_b200_num_codeblocks(codec, 0) entries, bytes holds bytes_cap bytes. */
+typedef struct
+{
+  bwc_float *normalized;
+  bwc_float *transformed;
+  uint8     *K;
+  uint8     *Z;
+  uint32    *L;
+  uint16    *S;
+  uint8     *bytes;
+  uint64     bytes_cap;
+  uint64    *byte_offsets;
+  bwc_float *stats;
+  uint32    *flags;
+} bwc_b200_stage_dump;
+
+uint64 bwc_b200_num_codeblocks(bwc_codec *const codec, uint8 const param);
+void   bwc_b200_set_stage_dump(bwc_codec *const codec, bwc_b200_stage_dump const *dump);
+
+/* Decompression counterpart: the working buffer after tier-1 decoding (dequantised
+ * coefficients) and after the inverse transform, parameter 0 of tile 0. */
+typedef struct
+{
+  bwc_float *dequantized;
+  bwc_float *reconstructed;
+} bwc_b200_decode_dump;
+
+void   bwc_b200_set_decode_dump(bwc_codec *const codec, bwc_b200_decode_dump const *dump);
+
+/* Host-only inspection (no samples are coded by these).
+ * codeblock_geometry: X0,Y0,Z0,TS0,X1,Y1,Z1,TS1 of codeblock c (tier-1 order) in the
+ *   parameter's working buffer, its subband's high-pass flags and Kmax;
+ * subband_steps: effective quantisation step, step size and energy gain of its subband;
+ * parsed_codeblock: after bwc_create_decompression, K (= Kmax - Kmsbs), Kmsbs, Z and the
+ *   MAXIMUM_NO_PASSES truncation lengths recovered from the packet headers;
+ * assemble_from_tier1: runs rate control, packet formation and codestream layout of a codec
+ *   prepared by bwc_create_compression on caller-supplied tier-1 results (all parameters'
+ *   codeblocks in tier-1 order; L and S strided by MAXIMUM_NO_PASSES and MAXIMUM_NO_PASSES + 1;
+ *   coded bytes at byte_offsets[c] of `bytes`; minmax = min, max per parameter) and writes the
+ *   codestream to stream->out.  Returns its size, 0 on error. */
+int    bwc_b200_codeblock_geometry(bwc_codec *const codec, uint8 const param, uint64 const c,
+                                   uint64 *geom10);
+int    bwc_b200_subband_steps(bwc_codec *const codec, uint8 const param, uint64 const c,
+                              double *out3);
+int    bwc_b200_parsed_codeblock(bwc_codec *const codec, uint8 const param, uint64 const c,
+                                 int64 *meta3, uint64 *L);
+size_t bwc_b200_assemble_from_tier1(bwc_codec *const codec, bwc_stream *const stream,
+                                    uint8 const *K, uint8 const *Z, uint64 const *L,
+                                    uint16 const *S, uint8 const *bytes,
+                                    uint64 const *byte_offsets, bwc_float const *minmax,
+                                    uint16 const slope_min, uint16 const slope_max);
+
+/* Device time of the stages of the last bwc_compress / bwc_decompress on this codec, in
+ * milliseconds (CUDA events on the codec's stream): [0] upload, [1] fill+normalise, [2] wavelet,
+ * [3] tier-1, [4] download of tier-1 results, [5] tier-2 (host), [6] codestream gather and
+ * download, [7] total.  Returns the number of entries written (at most n). */
+int    bwc_b200_last_timings(bwc_codec *const codec, double *out_ms, int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BWC_B200_H */
