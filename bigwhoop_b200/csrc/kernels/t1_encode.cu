@@ -119,8 +119,18 @@ __device__ void mq_terminate(Mq &e, const CbCtx &cc) {
 
 // Minimal number of bytes that decode a pass correctly, given the coder state at its end and the
 // bytes emitted later (mq.c:587-675; the single-precision build uses 32-bit split arithmetic).
+// Bytes at or beyond `cap` read as zero (the reference's buffer is zero-filled past its data);
+// a scan that has not settled after 64 bytes sets *bad (it settles within a few bytes).
 __device__ int64_t truncation_length(uint32_t A, uint32_t C, int32_t t, uint32_t T, int64_t L,
-                                     const uint8_t *b) {
+                                     const uint8_t *b0, uint32_t cap, uint32_t *bad) {
+  struct Bytes {
+    const uint8_t *p;
+    int64_t cap;
+    __device__ __forceinline__ uint32_t operator[](int64_t i) const {
+      return (i >= 0 && i < cap) ? p[i] : 0u;
+    }
+  } b{b0, (int64_t)cap};
+  int guard = 0;
 #ifdef BWC_SINGLE_PRECISION
   int32_t CrFrac = (int32_t)((uint32_t)C << t);
   int32_t CArFrac = (int32_t)((uint32_t)A << t) + CrFrac;
@@ -131,6 +141,10 @@ __device__ int64_t truncation_length(uint32_t A, uint32_t C, int32_t t, uint32_t
   CArFrac &= 0x7FFFFFF;
   int s = 8;
   while ((CrDec > 0xff) || (CArDec <= 0xff)) {
+    if (++guard > 64) {
+      *bad = 1;
+      break;
+    }
     const int32_t buff = (L >= 0) ? (int32_t)b[L] : 0;
     L++;
     CrDec -= buff << (8 - s);
@@ -150,6 +164,10 @@ __device__ int64_t truncation_length(uint32_t A, uint32_t C, int32_t t, uint32_t
   int64_t CAr = ((int64_t)A << t) + Cr;
   int s = 8;
   while (((Cr >> 27) > 0xff) || ((CAr >> 27) <= 0xff)) {
+    if (++guard > 64) {
+      *bad = 1;
+      break;
+    }
     const int64_t buff = (L >= 0) ? (int64_t)b[L] : 0;
     L++;
     Cr -= buff << (35 - s);
@@ -567,14 +585,16 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     __syncwarp();
     // ---- truncation lengths ------------------------------------------------------------------
     uint32_t *Lout = out.L + (uint64_t)c * kMaxPasses;
+    uint32_t scan_bad = 0;
     for (int j = lane; j < Z; j += 32) {
       const uint64_t s0 = snaps[2 * j];
       const int64_t Ls = (int64_t)snaps[2 * j + 1];
       const uint32_t A = (uint32_t)(s0 >> 48), T = (uint32_t)((s0 >> 40) & 0xFF);
       const int32_t t = (int32_t)(int8_t)((s0 >> 32) & 0xFF);
       const uint32_t C = (uint32_t)s0;
-      Lout[j] = (uint32_t)truncation_length(A, C, t, T, Ls, cc.out);
+      Lout[j] = (uint32_t)truncation_length(A, C, t, T, Ls, cc.out, cc.cap, &scan_bad);
     }
+    if (__any_sync(0xffffffffu, scan_bad)) flags |= 4u;
     __syncwarp();
     // ---- convex hull and log slopes (lane 0) --------------------------------------------------
     if (lane == 0) {

@@ -1,0 +1,130 @@
+"""Host-side parity with the reference (no GPU): geometry, energy-gain state, tier-2 rate
+control, packet headers, codestream layout and codestream parsing.
+
+The reference's own tier-1 output (codeblock lengths, slopes, coded bytes) is fed into this
+library's tier-2 through bwc_b200_assemble_from_tier1; the codestream must be byte-identical to
+the one the reference assembles from the same data.
+"""
+import numpy as np
+import pytest
+
+from conftest import need_ref
+from bigwhoop_b200 import bwc, fields
+
+CASES = [
+    # shape, precision, dtype, decomp, codeblocks, rate
+    ((64, 64, 64), "double", np.float64, (3, 3, 3, 0), (4, 4, 4, 0), "2"),
+    ((64, 64, 64), "double", np.float64, None, None, "0.5,1,2,4"),
+    ((33, 47, 61), "double", np.float64, (2, 2, 2, 0), (5, 5, 4, 0), "1,2"),
+    ((33, 47, 61), "single", np.float32, (2, 2, 2, 0), (5, 5, 4, 0), "1,2"),
+    ((33, 47, 61), "double", np.float32, (2, 2, 2, 0), (5, 5, 4, 0), "0.25"),
+    ((8, 20, 24, 30), "double", np.float64, (2, 2, 2, 1), (3, 3, 3, 1), "0.25,8"),
+    ((40, 17, 90), "double", np.float64, (3, 2, 4, 0), (4, 3, 5, 0), "4,0.5"),
+    ((1, 1, 300), "double", np.float64, (4, 0, 0, 0), (6, 0, 0, 0), "2"),
+]
+
+
+def _field(shape, dtype, seed=3):
+    return fields.spectral_field(shape, seed).astype(dtype)
+
+
+def _assemble_both(f, precision, decomp, cb, rate):
+    ref = need_ref(precision)
+    ref.reset_gain_lut(precision)
+    bwc.reset_gain_state(precision)
+    rc = ref.RefCompressor(f, precision=precision, decomp=decomp, cb=cb, rate=rate)
+    mc = bwc.Compressor(f, precision=precision, decomp=decomp, codeblocks=cb, rate=rate)
+    try:
+        assert np.array_equal(ref.gain_lut(precision), bwc.gain_state(precision))
+        ncb = rc.num_codeblocks()
+        assert mc.num_codeblocks() == ncb
+        L = mc.L
+        for c in range(ncb):
+            cbk = rc.codeblock(c, with_data=False)
+            g = np.zeros(10, np.uint64)
+            assert L.bwc_b200_codeblock_geometry(mc.codec, 0, c, g.ctypes.data) == 0
+            assert np.array_equal(g, cbk.geom), (c, g, cbk.geom)
+            st = np.zeros(3)
+            L.bwc_b200_subband_steps(mc.codec, 0, c, st.ctypes.data)
+            assert np.array_equal(st, cbk.subband), (c, st, cbk.subband)
+        rc.normalize(); rc.dwt(); rc.t1()
+        MP = ref.MAX_PASSES[precision]
+        K = np.zeros(ncb, np.uint8); Z = np.zeros(ncb, np.uint8)
+        Ls = np.zeros(ncb * MP, np.uint64); Ss = np.zeros(ncb * (MP + 1), np.uint16)
+        offs = np.zeros(ncb, np.uint64); data = bytearray()
+        for c in range(ncb):
+            cbk = rc.codeblock(c)
+            K[c], Z[c] = cbk.K, cbk.Z
+            Ls[c * MP:c * MP + cbk.Z] = cbk.L
+            Ss[c * (MP + 1):c * (MP + 1) + cbk.Z + 1] = cbk.S
+            offs[c] = len(data)
+            data += cbk.data
+        smin, smax = rc.tile_slopes()
+        stats = rc.stats()
+        rc.t2()
+        cs_ref = rc.assemble()
+        dt = np.float64 if precision == "double" else np.float32
+        mm = np.array(stats[:2], dt)
+        buf = np.frombuffer(bytes(data) + b"\0" * 64, np.uint8).copy()
+        out = np.zeros(len(cs_ref) + 4096, np.uint8)
+        stream = L.bwc_init_stream(f.ctypes.data, out.ctypes.data, 0)
+        n = L.bwc_b200_assemble_from_tier1(mc.codec, stream, K.ctypes.data, Z.ctypes.data,
+                                           Ls.ctypes.data, Ss.ctypes.data, buf.ctypes.data,
+                                           offs.ctypes.data, mm.ctypes.data, smin, smax)
+        return cs_ref, bytes(out[:n])
+    finally:
+        rc.close()
+        mc.close()
+
+
+@pytest.mark.parametrize("shape,precision,dtype,decomp,cb,rate", CASES)
+def test_tier2_codestream_identical(shape, precision, dtype, decomp, cb, rate):
+    f = _field(shape, dtype)
+    cs_ref, cs_me = _assemble_both(f, precision, decomp, cb, rate)
+    assert len(cs_me) == len(cs_ref)
+    assert cs_me == cs_ref
+
+
+@pytest.mark.parametrize("shape,precision,dtype,decomp,cb,rate", CASES[:6])
+def test_parse_identical(shape, precision, dtype, decomp, cb, rate):
+    ref = need_ref(precision)
+    f = _field(shape, dtype)
+    ref.reset_gain_lut(precision)
+    cs = ref.compress(f, precision=precision, decomp=decomp, cb=cb, rate=rate)
+    rd = ref.RefDecompressor(cs, f.shape, f.dtype, precision=precision)
+    d = bwc.Decompressor(cs, precision=precision)
+    try:
+        L = bwc.load(precision)
+        ncb = rd.L.rp_num_codeblocks(rd.h, 0)
+        MP = ref.MAX_PASSES[precision]
+        for c in range(ncb):
+            m1 = np.zeros(3, np.int64); L1 = np.zeros(MP, np.uint64)
+            rd.L.rp_dcodeblock(rd.h, 0, c, m1.ctypes.data, L1.ctypes.data)
+            m2 = np.zeros(3, np.int64); L2 = np.zeros(MP, np.uint64)
+            assert L.bwc_b200_parsed_codeblock(d.codec, 0, c, m2.ctypes.data, L2.ctypes.data) == 0
+            assert np.array_equal(m1, m2), (c, m1, m2)
+            assert np.array_equal(L1, L2), c
+    finally:
+        rd.close()
+        d.close()
+
+
+def test_gain_state_accumulates_like_reference():
+    """Every configure_codec / bwc_set_decomp adds to the process-wide gain table."""
+    ref = need_ref("double")
+    ref.reset_gain_lut("double")
+    bwc.reset_gain_state("double")
+    f = _field((16, 16, 16), np.float64)
+    for _ in range(3):
+        rc = ref.RefCompressor(f, decomp=(2, 2, 2, 0), rate="2")
+        mc = bwc.Compressor(f, decomp=(2, 2, 2, 0), rate="2")
+        assert np.array_equal(ref.gain_lut("double"), bwc.gain_state("double"))
+        rc.close()
+        mc.close()
+    g = bwc.gain_state("double")
+    # six table initialisations: level-1 low-pass entry is six times a single one (to rounding)
+    bwc.reset_gain_state("double")
+    mc = bwc.Compressor(f, rate="2")   # one initialisation
+    one = bwc.gain_state("double")
+    mc.close()
+    assert g[0, 1] == pytest.approx(6 * one[0, 1], rel=1e-12)
