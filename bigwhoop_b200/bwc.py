@@ -300,8 +300,8 @@ class Compressor:
         return n
 
     def timings(self):
-        out = np.zeros(8)
-        k = self.L.bwc_b200_last_timings(self.codec, out.ctypes.data, 8)
+        out = np.zeros(9)
+        k = self.L.bwc_b200_last_timings(self.codec, out.ctypes.data, 9)
         return out[:k]
 
     def close(self):
@@ -367,8 +367,8 @@ class Decompressor:
         return self.out
 
     def timings(self):
-        out = np.zeros(8)
-        k = self.L.bwc_b200_last_timings(self.codec, out.ctypes.data, 8)
+        out = np.zeros(9)
+        k = self.L.bwc_b200_last_timings(self.codec, out.ctypes.data, 9)
         return out[:k]
 
     def close(self):

@@ -28,11 +28,6 @@
 
 namespace bwcb {
 
-void launch_t1_encode_ex(const bwc_float *work, const FieldDims &dims, const CbDev *cbs,
-                         uint32_t ncb, const SbDev *sbs, uchar erres, const T1EncOut &out,
-                         uint32_t state_cap, uint16_t *gstate, uint32_t *work_counter, int grid,
-                         cudaStream_t s);
-
 namespace {
 
 bool cuda_ok(cudaError_t e, const char *what) {
@@ -128,16 +123,16 @@ struct DeviceState {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[8] = {};
   DevBuf in, work, keys, stats, cbtab, sbtab, bytes, scratch, snaps, dmse, K, Z, L, S, flags,
-      slopes, counter, cs, blob, pieces, outbuf, mags, lmax;
+      slopes, counter, cs, blob, pieces, outbuf, mags, lmax, symbols, pcount, poff, symused;
   bool dump_set = false, ddump_set = false;
   bwc_b200_stage_dump dump{};
   bwc_b200_decode_dump ddump{};
-  double timings[8] = {};
+  double timings[10] = {};   // stage times (ms); [8] tier-1 symbols coded (millions)
 
   ~DeviceState() {
     DevBuf *all[] = {&in, &work, &keys, &stats, &cbtab, &sbtab, &bytes, &scratch, &snaps, &dmse,
                      &K, &Z, &L, &S, &flags, &slopes, &counter, &cs, &blob, &pieces, &outbuf,
-                     &mags, &lmax};
+                     &mags, &lmax, &symbols, &pcount, &poff, &symused};
     if (stream) cudaStreamSynchronize(stream);
     for (DevBuf *b : all) b->drop();
     for (auto &e : ev)
@@ -333,9 +328,21 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
   cudaMemsetAsync(dv->keys.p, 0, 16 * info.nPar, s);
   for (int p = 0; p < info.nPar; ++p) cudaMemsetAsync(dv->keys.as<uint64_t>() + 2 * p, 0xFF, 8, s);
 
-  const uint32_t state_cap = std::min<uint32_t>(max_cols, 6144);
-  const size_t smem = (32 * 2 + 32 * 12) * 4 + (size_t)state_cap * 2 * 4;
-  const int grid = t1_grid(nullptr, smem);
+  if (t1_model_smem(max_cols) > 200 * 1024) {
+    warn("o##########################################################o\n"
+         "| ERROR: codeblocks above 2^18 samples are not supported   |\n"
+         "o##########################################################o\n");
+    return 0;
+  }
+  // symbol arena: sized for about 1.1 symbols per sample and bit plane; a full arena is
+  // detected per codeblock and the parameter is coded again with a larger one
+  uint64_t total_samples = 0;
+  for (uint64_t i = 0; i < ncb; ++i)
+    total_samples += (uint64_t)allcb[i].w * ((allcb[i].h + 3) / 4) * 4 * allcb[i].d * allcb[i].nt;
+  uint64_t arena = std::max<uint64_t>(1 << 20, total_samples * (kPrecBit + 1) * 9 / 8);
+  if (!dv->pcount.ensure(ncb * kMaxPasses * 4) || !dv->poff.ensure(ncb * kMaxPasses * 8) ||
+      !dv->symused.ensure(8))
+    return 0;
   float t_norm = 0, t_dwt = 0, t_t1 = 0;
   for (int p = 0; p < info.nPar; ++p) {
     cudaEvent_t a, b2, c2, d2;
@@ -363,10 +370,34 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
     o.planes = dv->scratch.as<uint8_t>();
     o.snaps = dv->snaps.as<uint64_t>() + cb_base[p] * kMaxPasses * 2;
     o.dmse = dv->dmse.as<int64_t>() + cb_base[p] * kMaxPasses;
-    launch_t1_encode_ex(dv->work.as<bwc_float>(), dims, dv->cbtab.as<CbDev>() + cb_base[p],
-                        (uint32_t)cbs[p].size(), dv->sbtab.as<SbDev>(), c.error_resilience, o,
-                        state_cap, dv->scratch.as<uint16_t>(), dv->counter.as<uint32_t>() + p,
-                        grid, s);
+    o.pass_count = dv->pcount.as<uint32_t>() + cb_base[p] * kMaxPasses;
+    o.pass_off = dv->poff.as<uint64_t>() + cb_base[p] * kMaxPasses;
+    o.sym_used = dv->symused.as<unsigned long long>();
+    for (int attempt = 0;; ++attempt) {
+      if (!dv->symbols.ensure(arena + 256)) return 0;
+      o.symbols = dv->symbols.as<uint8_t>();
+      o.sym_cap = dv->symbols.cap - 256;   // slack for the MQ kernel's read-ahead
+      cudaMemsetAsync(dv->symused.p, 0, 8, s);
+      cudaMemsetAsync(o.flags, 0, cbs[p].size() * 4, s);
+      launch_t1_encode(dv->work.as<bwc_float>(), dims, dv->cbtab.as<CbDev>() + cb_base[p],
+                       (uint32_t)cbs[p].size(), dv->sbtab.as<SbDev>(), c.error_resilience, o,
+                       max_cols, s);
+      unsigned long long used = 0;
+      cudaMemcpyAsync(&used, dv->symused.p, 8, cudaMemcpyDeviceToHost, s);
+      if (!cuda_ok(cudaStreamSynchronize(s), "tier-1 encoding")) return 0;
+      if (p == 0) dv->timings[8] = 0;
+      if (used <= o.sym_cap) {
+        dv->timings[8] += (double)used * 1e-6;
+        break;
+      }
+      if (attempt >= 3) {
+        warn("o##########################################################o\n"
+             "| ERROR: tier-1 symbol arena exhausted                     |\n"
+             "o##########################################################o\n");
+        return 0;
+      }
+      arena = used + (used >> 3) + (1 << 20);
+    }
     cudaEventRecord(d2, s);
     if (!cuda_ok(cudaStreamSynchronize(s), "compression kernels")) return 0;
     float x;
@@ -667,7 +698,7 @@ extern "C" void bwc_b200_set_decode_dump(bwc_codec *const codec, bwc_b200_decode
 
 extern "C" int bwc_b200_last_timings(bwc_codec *const codec, double *out_ms, int n) {
   if (!codec || !codec->tile || !codec->tile->dev) return 0;
-  const int k = std::min(n, 8);
+  const int k = std::min(n, 9);
   for (int i = 0; i < k; ++i) out_ms[i] = codec->tile->dev->timings[i];
   return k;
 }

@@ -28,7 +28,7 @@ struct SbDev {
   uint32_t cls;        // significance-context class: 0 low-pass, 1 high-pass, 2 diagonal
 };
 
-// Outputs of the tier-1 encoder.
+// Outputs and scratch of the tier-1 encoder.
 struct T1EncOut {
   uint8_t *bytes;        // coded bytes, codeblock c at CbDev::out_off
   uint8_t *K;            // [ncb]
@@ -36,10 +36,16 @@ struct T1EncOut {
   uint32_t *L;           // [ncb * kMaxPasses] truncation lengths
   uint16_t *S;           // [ncb * (kMaxPasses + 1)] log slopes
   uint32_t *slopes;      // [2]: min over non-zero slopes, max (atomics; init 0xFFFF / 0)
-  uint32_t *flags;       // [ncb]: bit 0 output overflow, bit 1 hull underflow
+  uint32_t *flags;       // [ncb]: 1 coded-byte overflow, 2 hull stack underflow,
+                         //        4 unsettled truncation scan, 8 symbol arena full
   uint8_t *planes;       // scratch: bit planes, CbDev::scratch_off
   uint64_t *snaps;       // scratch: [ncb * kMaxPasses * 2] end-of-pass coder states
   int64_t *dmse;         // scratch: [ncb * kMaxPasses] distortion decrease per pass
+  uint8_t *symbols;      // scratch: symbol arena
+  uint64_t sym_cap;      //   its capacity in bytes
+  unsigned long long *sym_used;   // bump counter (zeroed by the caller)
+  uint32_t *pass_count;  // scratch: [ncb * kMaxPasses] symbols per pass
+  uint64_t *pass_off;    // scratch: [ncb * kMaxPasses] arena offset of each pass's symbols
 };
 
 struct FieldDims {
@@ -67,13 +73,12 @@ void launch_dwt_forward(bwc_float *work, const FieldDims &dims, const DwtPlan &p
 void launch_dwt_inverse(bwc_float *work, const FieldDims &dims, const DwtPlan &plan,
                         cudaStream_t s);
 
-// t1_encode.cu: one warp per codeblock, codeblocks taken from *work_counter (zeroed by the
-// caller).  Codeblocks with more than state_cap stripe columns keep their column state in
-// gstate (at scratch_off) instead of shared memory.
-void launch_t1_encode_ex(const bwc_float *work, const FieldDims &dims, const CbDev *cbs,
-                         uint32_t ncb, const SbDev *sbs, uchar erres, const T1EncOut &out,
-                         uint32_t state_cap, uint16_t *gstate, uint32_t *work_counter, int grid,
-                         cudaStream_t s);
+// t1_encode.cu: context modelling (one CTA per codeblock, max_cols = largest number of stripe
+// columns of a codeblock) followed by MQ coding (one thread per codeblock).
+size_t t1_model_smem(uint32_t max_cols);
+void launch_t1_encode(const bwc_float *work, const FieldDims &dims, const CbDev *cbs,
+                      uint32_t ncb, const SbDev *sbs, uchar erres, const T1EncOut &out,
+                      uint32_t max_cols, cudaStream_t s);
 
 // t1_decode.cu: decodes Z[c] passes of codeblock c from data + out_off (Lmax[c] bytes) and
 // writes the dequantised samples into the (zeroed) working buffer.
