@@ -386,8 +386,8 @@ class Decompressor:
             pass
 
 
-def decompress_array(codestream, precision="double"):
-    d = Decompressor(codestream, precision=precision)
+def decompress_array(codestream, precision="double", layer=0):
+    d = Decompressor(codestream, precision=precision, layer=layer)
     try:
         return d.decompress()
     finally:

@@ -221,6 +221,31 @@ class RefDecompressor:
         assert self.L.rp_decompress_full(self.h) == 0
         return self.out
 
+    # stage by stage: t1 (decode + dequantise into a zeroed buffer), idwt, finish (denormalise
+    # and write the output)
+    def t1(self, p=0):
+        assert self.L.rp_dstage_t1(self.h, p) == 0
+
+    def idwt(self, p=0):
+        assert self.L.rp_dstage_idwt(self.h, p) == 0
+
+    def finish(self, p=0):
+        assert self.L.rp_dstage_finish(self.h, p) == 0
+        return self.out
+
+    def work(self):
+        dt = np.float64 if self.L.rp_prec_bytes() == 8 else np.float32
+        n = int(np.prod(self.out.shape))
+        buf = np.zeros(n, dtype=dt)
+        self.L.rp_copy_work(self.h, buf.ctypes.data)
+        return buf
+
+    def codeblock(self, c, p=0):
+        """(K, Kmsbs, Z) of codeblock c as parsed from the codestream."""
+        meta = np.zeros(3, dtype=np.int64)
+        assert self.L.rp_dcodeblock(self.h, p, c, meta.ctypes.data, None) == 0
+        return tuple(int(v) for v in meta)
+
 
 def reset_gain_lut(precision="double"):
     load(precision).rp_reset_gain_lut()
@@ -244,8 +269,8 @@ def compress(field, **kw):
         rc.close()
 
 
-def decompress(codestream, shape, dtype, precision="double"):
-    rd = RefDecompressor(codestream, shape, dtype, precision=precision)
+def decompress(codestream, shape, dtype, precision="double", layer=0):
+    rd = RefDecompressor(codestream, shape, dtype, precision=precision, layer=layer)
     try:
         return rd.decompress().copy()
     finally:

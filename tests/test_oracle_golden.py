@@ -1,0 +1,113 @@
+"""The oracle, pinned (no GPU needed).
+
+1. The golden fixtures (tests/golden, produced by the reference library) are reproduced by the
+   reference library built here, when it is present.
+2. The C restatement of the hot path (oracle/restate) reproduces every golden value stage by
+   stage: normalisation, forward transform, each codeblock's tier-1 output, and on the decoder
+   side tier-1 decoding, the inverse transform and denormalisation.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, need_ref
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+INDEX = json.load(open(os.path.join(GOLDEN, "cases.json")))
+NAMES = sorted(INDEX)
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def load_case(name):
+    return INDEX[name], dict(np.load(os.path.join(GOLDEN, name + ".npz")))
+
+
+def restated(precision):
+    from oracle import restated as rs
+    if not rs.available(precision):
+        pytest.skip("restatement not built (make -C oracle restate)")
+    return rs
+
+
+def gain_step2(sub, precision):
+    qt_step, gain = sub[1], sub[2]
+    if precision == "single":
+        s2 = float(np.float32(qt_step) * np.float32(qt_step))
+    else:
+        s2 = qt_step * qt_step
+    return gain * s2
+
+
+def qm_of(meta, precision):
+    if meta["qm"] is not None:
+        return meta["qm"]
+    return 62 if precision == "double" else 30
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_reference_reproduces_golden(name):
+    import sys
+    sys.path.insert(0, GOLDEN)
+    from make_golden import generate
+    meta, g = load_case(name)
+    need_ref(meta["precision"])
+    arrays, meta2 = generate(name)
+    assert np.array_equal(arrays["field"], g["field"]), "field generator changed"
+    for k in ("codestream", "K", "Z", "L", "S", "cb_data", "dK", "dZ", "geom"):
+        assert np.array_equal(arrays[k], g[k]), k
+    for k in ("normalized_sha", "transformed_sha", "dequantized_sha", "reconstructed_sha", "output_sha"):
+        assert meta2[k] == meta[k], k
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_restatement_encoder_matches_golden(name):
+    meta, g = load_case(name)
+    precision = meta["precision"]
+    rs = restated(precision)
+    f = g["field"]
+    dims = rs.dims_of(f.shape)
+    work, stats = rs.fill_normalize(f, qm_of(meta, precision), precision)
+    assert np.array_equal(stats.astype(np.float64), g["stats"]), (stats, g["stats"])
+    assert sha(work) == meta["normalized_sha"]
+    rs.dwt_forward(work, dims, meta["decomp"], precision)
+    assert sha(work) == meta["transformed_sha"]
+    for c in range(meta["codeblocks_n"]):
+        geo = g["geom"][c]
+        cb = rs.make_codeblock(geo[:8], g["subband"][c][0], gain_step2(g["subband"][c], precision),
+                               geo[8], precision)
+        K, Z, Ls, Ss, data = rs.t1_encode(work, dims, cb, meta["erres"], precision)
+        assert (K, Z) == (g["K"][c], g["Z"][c]), c
+        assert np.array_equal(Ls, g["L"][c][:Z]), c
+        assert np.array_equal(Ss, g["S"][c][:Z + 1]), c
+        lo, hi = int(g["cb_offsets"][c]), int(g["cb_offsets"][c + 1])
+        assert data[:hi - lo] == bytes(g["cb_data"][lo:hi]), c
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_restatement_decoder_matches_golden(name):
+    meta, g = load_case(name)
+    precision = meta["precision"]
+    rs = restated(precision)
+    f = g["field"]
+    dims = rs.dims_of(f.shape)
+    work = np.zeros(f.size, np.float64 if precision == "double" else np.float32)
+    for c in range(meta["codeblocks_n"]):
+        K, Z = int(g["dK"][c]), int(g["dZ"][c])
+        if Z == 0:
+            continue
+        geo = g["geom"][c]
+        cb = rs.make_codeblock(geo[:8], g["subband"][c][0], 0.0, geo[8], precision)
+        lo = int(g["cb_offsets"][c])
+        n = int(g["L"][c][Z - 1])
+        rs.t1_decode(work, dims, cb, K, Z, bytes(g["cb_data"][lo:lo + n]), meta["erres"], precision)
+    assert sha(work) == meta["dequantized_sha"]
+    rs.dwt_inverse(work, dims, meta["decomp"], precision)
+    assert sha(work) == meta["reconstructed_sha"]
+    out = rs.denormalize(work, g["stats"][0], g["stats"][1], qm_of(meta, precision), f.dtype, precision)
+    assert sha(out.reshape(f.shape)) == meta["output_sha"]
