@@ -5,7 +5,9 @@
 // :523-548 reader, :561-612 flush).  Tag trees: 4D quad trees over the codeblocks of a
 // precinct with threshold-incremental coding (tagtree.c:107-445), including the reference's
 // parent linking, which keeps advancing the time-axis parent pointer across levels.
+#include <algorithm>
 #include <cstdlib>
+#include <type_traits>
 
 #include "common.hpp"
 
@@ -121,8 +123,10 @@ void tagtree_set(TagTree &tt, uint64_t leaf, uint16_t value) {
   } while (n >= 0 && tt.nodes[n].value > value);
 }
 
-void tagtree_encode(TagTree &tt, BitWriter &bw, uint32_t threshold, uint64_t leaf,
-                    uchar estimate) {
+// encode_tagtree (tagtree.c:311-373): root to leaf, each node's value coded incrementally up
+// to `threshold`; only a non-estimating call records the thresholds reached.
+template <class Writer, class Tree>
+static void tagtree_walk(Tree &tt, Writer &bw, uint32_t threshold, uint64_t leaf, bool store) {
   int64_t branch[64];
   int nb = 0;
   int64_t n = (int64_t)leaf;
@@ -132,7 +136,7 @@ void tagtree_encode(TagTree &tt, BitWriter &bw, uint32_t threshold, uint64_t lea
   }
   uint32_t tmin = 0;
   for (;;) {
-    TagNode &node = tt.nodes[n];
+    auto &node = tt.nodes[n];
     uint32_t tmp = node.threshold;
     if (tmp < tmin) tmp = tmin;
     while (node.value >= tmp && tmp < threshold) {
@@ -140,10 +144,21 @@ void tagtree_encode(TagTree &tt, BitWriter &bw, uint32_t threshold, uint64_t lea
       bw.emit(node.value >= tmp ? 0 : 1);
     }
     tmin = std::min<uint32_t>(node.value, tmp);
-    if (!estimate) node.threshold = (uint16_t)tmp;
+    if constexpr (!std::is_const_v<Tree>) {
+      if (store) node.threshold = (uint16_t)tmp;
+    }
     if (n == (int64_t)leaf) break;
     n = branch[--nb];
   }
+}
+
+void tagtree_encode(TagTree &tt, BitWriter &bw, uint32_t threshold, uint64_t leaf,
+                    uchar estimate) {
+  tagtree_walk(tt, bw, threshold, leaf, !estimate);
+}
+
+void tagtree_estimate(const TagTree &tt, RawBits &out, uint32_t threshold, uint64_t leaf) {
+  tagtree_walk(tt, out, threshold, leaf, false);
 }
 
 uchar tagtree_decode(TagTree &tt, BitReader &br, uint32_t threshold, uint64_t leaf) {

@@ -203,10 +203,28 @@ struct BitReader {
   uint64_t bytes_used() const { return T == 0xFF ? L + 1 : L; }
 };
 
+// Unstuffed bit string (most-significant bit first), for header pieces that are assembled
+// and stuffed later.
+struct RawBits {
+  std::vector<uint64_t> words;
+  uint64_t n = 0;
+  void emit(uint64_t bit) {
+    if ((n & 63) == 0) words.push_back(0);
+    if (bit) words.back() |= 1ull << (63 - (n & 63));
+    ++n;
+  }
+  void clear() {
+    words.clear();
+    n = 0;
+  }
+};
+
 void tagtree_init(TagTree &tt, uint64_t lx, uint64_t ly, uint64_t lz, uint64_t lts);
 void tagtree_reset(TagTree &tt);
 void tagtree_set(TagTree &tt, uint64_t leaf, uint16_t value);
 void tagtree_encode(TagTree &tt, BitWriter &bw, uint32_t threshold, uint64_t leaf, uchar estimate);
+// the bits an estimating tagtree_encode would emit (the tree is left unchanged)
+void tagtree_estimate(const TagTree &tt, RawBits &out, uint32_t threshold, uint64_t leaf);
 uchar tagtree_decode(TagTree &tt, BitReader &br, uint32_t threshold, uint64_t leaf);
 
 // ---- tier 2 and codestream (tier2.cpp, codestream.cpp) ------------------------------------------

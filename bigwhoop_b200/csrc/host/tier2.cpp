@@ -188,6 +188,204 @@ static int64_t create_quality_layer(bwc_codec *codec, Tile &tile, uint16_t thres
   return size;
 }
 
+// ---- rate-control probes ------------------------------------------------------------------
+// Within the bisection of one layer, probes differ only in where each codeblock is truncated:
+// the tag trees, the previous layer's truncation points and the length-code states stay fixed
+// (an estimating probe changes none of them).  So each codeblock's tag-tree bits are derived
+// once per layer, its truncation point comes from a binary search over its right-to-left slope
+// records, and a packet header's size is counted by stuffing its bits a chunk at a time.  The
+// result equals create_quality_layer(..., est = 1) exactly (same sums, same header bytes).
+
+namespace {
+
+// byte count of a bit string written with BitWriter::emit and BitWriter::flush
+struct StuffCounter {
+  uint32_t T = 0;
+  int t = 8;
+  uint64_t bytes = 0;
+  void put(uint64_t v, int n) {   // the n (<= 64) low bits of v, most significant first
+    while (n > 0) {
+      const int k = n < t ? n : t;
+      const uint32_t chunk = (uint32_t)(v >> (n - k)) & ((1u << k) - 1u);
+      T |= chunk << (t - k);
+      t -= k;
+      n -= k;
+      if (t == 0) {
+        bytes++;
+        t = (T == 0xFF) ? 7 : 8;
+        T = 0;
+      }
+    }
+  }
+  void put_bits(const RawBits &rb, uint64_t off, uint64_t n) {
+    while (n) {
+      const uint64_t b = off & 63;
+      uint64_t m = 64 - b;
+      if (m > n) m = n;
+      if (m > 56) m = 56;
+      const uint64_t v = (rb.words[off >> 6] << b) >> (64 - m);
+      put(v, (int)m);
+      off += m;
+      n -= m;
+    }
+  }
+  void put_ones(int n) {
+    while (n > 0) {
+      const int m = n < 32 ? n : 32;
+      put((1ull << m) - 1, m);
+      n -= m;
+    }
+  }
+  uint64_t finish() const { return bytes + (t != 8 ? 1 : 0); }
+};
+
+struct ProbeCb {
+  const Codeblock *cb;
+  int16_t zprev;            // truncation point of the previous layer
+  uint32_t rec_off, rec_n;  // slope records
+  uint64_t incl_off, msbs_off;
+  uint32_t incl_n, msbs_n;
+};
+
+struct ProbePacket {
+  uint32_t first, count;
+};
+
+struct Probe {
+  // right-to-left slope records of every codeblock: z in decreasing order with strictly
+  // increasing S; max{z : S[z] >= t} is the first record whose S >= t
+  std::vector<uint16_t> rec_s;
+  std::vector<int16_t> rec_z;
+  std::vector<uint32_t> rec_off;   // per codeblock in tile order (parameters concatenated)
+  std::vector<ProbeCb> cbs;
+  std::vector<ProbePacket> packets;
+  RawBits pool;
+};
+
+void build_records(Tile &tile, Probe &pr) {
+  for (Parameter &par : tile.params)
+    for (Codeblock &cb : par.codeblocks) {
+      pr.rec_off.push_back((uint32_t)pr.rec_s.size());
+      int best = -1;
+      for (int z = cb.enc.Z; z >= 0; --z) {
+        if ((int)cb.enc.S[z] > best) {
+          best = cb.enc.S[z];
+          pr.rec_s.push_back(cb.enc.S[z]);
+          pr.rec_z.push_back((int16_t)z);
+        }
+      }
+    }
+  pr.rec_off.push_back((uint32_t)pr.rec_s.size());
+}
+
+// per-layer tables in the order create_quality_layer and create_packet visit codeblocks
+void build_layer(Tile &tile, int q, Probe &pr) {
+  pr.cbs.clear();
+  pr.packets.clear();
+  pr.pool.clear();
+  uint64_t cb_base = 0;
+  for (Parameter &par : tile.params) {
+    for (Resolution &res : par.res) {
+      for (uint64_t p = 0; p < res.nprec; ++p) {
+        ProbePacket pk{(uint32_t)pr.cbs.size(), 0};
+        for (uint8_t m = 0; m < res.nsub; ++m) {
+          const Subband &sb = par.subbands[res.first_subband + m];
+          const Precinct &prc = par.precincts[sb.first_precinct + p];
+          for (uint64_t k = 0; k < prc.ncb; ++k) {
+            const uint64_t ci = prc.first_cb + k;
+            Codeblock &cb = par.codeblocks[ci];
+            ProbeCb e{};
+            e.cb = &cb;
+            e.zprev = cb.cp()[q - 1];
+            e.rec_off = pr.rec_off[cb_base + ci];
+            e.rec_n = pr.rec_off[cb_base + ci + 1] - e.rec_off;
+            if (e.zprev == 0) {
+              e.incl_off = pr.pool.n;
+              tagtree_estimate(prc.incl, pr.pool, (uint32_t)(q + 1), k);
+              e.incl_n = (uint32_t)(pr.pool.n - e.incl_off);
+              e.msbs_off = pr.pool.n;
+              for (uint32_t kk = 1; kk <= cb.enc.Kmsbs + 1u; ++kk)
+                tagtree_estimate(prc.msbs, pr.pool, kk, k);
+              e.msbs_n = (uint32_t)(pr.pool.n - e.msbs_off);
+            }
+            pr.cbs.push_back(e);
+            pk.count++;
+          }
+        }
+        pr.packets.push_back(pk);
+      }
+    }
+    cb_base += par.codeblocks.size();
+  }
+}
+
+inline int16_t truncation_point(const Probe &pr, const ProbeCb &e, uint16_t threshold) {
+  uint32_t lo = 0, hi = e.rec_n;   // first record with S >= threshold
+  const uint16_t *s = pr.rec_s.data() + e.rec_off;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (s[mid] >= threshold) hi = mid; else lo = mid + 1;
+  }
+  return (lo < e.rec_n) ? pr.rec_z[e.rec_off + lo] : (int16_t)-1;
+}
+
+// create_quality_layer(codec, tile, threshold, q, 1) for the tables of layer q
+int64_t probe_layer(const Probe &pr, uint16_t threshold) {
+  int64_t size = 0;
+  for (const ProbePacket &pk : pr.packets) {
+    StuffCounter sc;
+    sc.put(1, 1);
+    bool e = false;
+    for (uint32_t i = pk.first; i < pk.first + pk.count; ++i) {
+      const ProbeCb &c = pr.cbs[i];
+      const CodedBlock &enc = c.cb->enc;
+      const int16_t z = truncation_point(pr, c, threshold);
+      int16_t cpq;
+      if (z < c.zprev) {
+        cpq = c.zprev;
+        if (cpq == 1) size += (int64_t)enc.L[0];
+      } else {
+        cpq = z;
+        if (z > 0) {
+          size += (int64_t)enc.L[z - 1];
+          if (z > 1 && c.zprev > 0) size -= (int64_t)enc.L[c.zprev - 1];
+        }
+      }
+      const int dz = cpq - c.zprev;
+      if (dz > 0) e = true;
+      if (c.zprev == 0) {
+        sc.put_bits(pr.pool, c.incl_off, c.incl_n);
+        if (cpq) sc.put_bits(pr.pool, c.msbs_off, c.msbs_n);
+      } else {
+        sc.put(dz ? 1 : 0, 1);
+      }
+      if (!dz) continue;
+      // encode_delta_z
+      if (dz == 1) sc.put(0, 1);
+      else if (dz == 2) sc.put(2, 2);
+      else if (dz < 6) sc.put(12u | (uint32_t)(dz - 3), 4);
+      else if (dz < 37) sc.put((15u << 5) | (uint32_t)(dz - 6), 9);
+      else if (dz < 293) sc.put((511u << 8) | (uint32_t)(dz - 37), 17);
+      // encode_length with the estimate state
+      const int16_t z_curr = cpq - 1, z_prev = c.zprev - 1;
+      const uint16_t beta = c.cb->beta_est;
+      uint16_t max_beta = beta;
+      const uint32_t L = (uint32_t)(enc.L[z_curr] - ((z_prev >= 0) ? enc.L[z_prev] : 0));
+      const uint16_t cp_bits = ilog2_u16((uint64_t)(z_curr - z_prev));
+      const int32_t L_bits = (int32_t)ilog2_u16(L) + 1 - cp_bits;
+      max_beta = (max_beta < L_bits) ? (uint16_t)L_bits : max_beta;
+      sc.put_ones(max_beta - beta);
+      sc.put(0, 1);
+      const int sh = max_beta + cp_bits - 1;
+      if (sh >= 0 && sh < 31) sc.put(L & (uint32_t)((2ull << sh) - 1), sh + 1);
+    }
+    size += e ? (int64_t)sc.finish() : 1;
+  }
+  return size;
+}
+
+}  // namespace
+
 // create_quality_layers (tier2.c:1115-1254)
 static uchar create_quality_layers(bwc_codec *codec, Tile &tile) {
   const bwc_gl_ctrl &c = codec->control;
@@ -197,6 +395,9 @@ static uchar create_quality_layers(bwc_codec *codec, Tile &tile) {
   const uint64_t tile_size = tile.box.size() * (uint64_t)info.nPar;
   const uint64_t header_size =
       (uint64_t)ceilf((float)(main_header + tile.header_size) / (float)c.nLayers);
+  static const bool check = getenv("BWC_B200_CHECK_PROBES") != nullptr;
+  Probe probe;
+  build_records(tile, probe);
   for (uint8_t l = 0; l < c.nLayers; ++l) {
     uint16_t slope;
     target = (int64_t)ceilf(c.bitrate[l] * (float)tile_size / 8.0f);
@@ -204,9 +405,18 @@ static uchar create_quality_layers(bwc_codec *codec, Tile &tile) {
       uint16_t smin = tile.slope_min, smax = tile.slope_max;
       uint16_t tmp = smin;
       slope = smin;
+      build_layer(tile, l, probe);
       while (smin < smax) {
         slope = (uint16_t)((smax + smin) >> 1);
-        est = create_quality_layer(codec, tile, slope, l, 1);
+        est = probe_layer(probe, slope);
+        if (check) {
+          const int64_t slow = create_quality_layer(codec, tile, slope, l, 1);
+          if (slow != est) {
+            fprintf(stderr, "bwc: rate-control probe mismatch (layer %d, slope %u: %lld vs %lld)\n",
+                    l, slope, (long long)est, (long long)slow);
+            return 1;
+          }
+        }
         if (est >= 0)
           est += est_tile + (int64_t)header_size;
         else

@@ -128,3 +128,19 @@ def test_gain_state_accumulates_like_reference():
     one = bwc.gain_state("double")
     mc.close()
     assert g[0, 1] == pytest.approx(6 * one[0, 1], rel=1e-12)
+
+
+def test_fast_rate_control_probes_equal_the_plain_probes():
+    """With BWC_B200_CHECK_PROBES set, every rate-control probe is also evaluated the plain way
+    (create_quality_layer with estimation) and any difference fails the compression."""
+    import os
+    import subprocess
+    import sys
+    need_ref("double")
+    env = dict(os.environ, BWC_B200_CHECK_PROBES="1")
+    here = os.path.dirname(os.path.abspath(__file__))
+    r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-x", "-k", "tier2_codestream_identical",
+                        os.path.join(here, "test_host_parity.py")], env=env, capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "mismatch" not in r.stderr
