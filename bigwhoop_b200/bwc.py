@@ -54,7 +54,10 @@ COMP, DECOMP = 0, 1
 
 
 def lib_path(precision="double"):
-    return os.path.join(HERE, "lib", precision, "libbwc.so")
+    """The library of one precision build; BWC_B200_LIB_DIR points at another build tree
+    (holding double/libbwc.so and single/libbwc.so)."""
+    base = os.environ.get("BWC_B200_LIB_DIR") or os.path.join(HERE, "lib")
+    return os.path.join(base, precision, "libbwc.so")
 
 
 class bwc_gl_inf(C.Structure):

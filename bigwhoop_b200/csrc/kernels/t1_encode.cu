@@ -25,10 +25,11 @@
 // Symbols are counted, offsets come from a CTA-wide prefix sum, and each thread writes its
 // columns' symbols.  Per pass the kernel records the symbol count and the distortion decrease.
 //
-// t1_mq_kernel -- one thread per codeblock.  Runs the MQ arithmetic coder over the codeblock's
+// t1_mq_kernel -- one lane per codeblock.  Runs the MQ arithmetic coder over the codeblock's
 // symbol stream (the only part that is inherently sequential), records the coder state at the
 // end of every pass, terminates, derives the minimal truncation length of every pass, builds
-// the convex hull and the 16-bit log slopes.  A warp codes 32 codeblocks concurrently.
+// the convex hull and the 16-bit log slopes.  A warp codes 1 to 32 codeblocks concurrently
+// (mq_lanes_per_warp).
 //
 // Stripe-column state (shared memory, one byte each): lo = significance | sign << 4 (read by
 // neighbours), hi = visited-in-significance-pass | refined << 4 (owner only).  Bit planes: one
@@ -582,6 +583,7 @@ __global__ void __launch_bounds__(kModelThreads)
 
 // ---- kernel 2: MQ coding, truncation lengths, convex hull ------------------------------------
 
+// MQ encoder state (mq.c:68-110)
 struct Mq {
   uint32_t A, C, T;
   int32_t t;
@@ -594,71 +596,41 @@ struct ByteOut {
   uint32_t flags;
 };
 
-__device__ __forceinline__ void mq_transfer(Mq &e, ByteOut &bo) {
-  if (e.T == 0xFF) {
-    if (e.L >= 0) {
-      if ((uint32_t)e.L < bo.cap) bo.out[e.L] = (uint8_t)e.T; else bo.flags |= 1u;
-    }
-    e.L++;
-    e.T = (e.C >> 20) & 0xFF;
-    e.C &= 0xFFFFF;
-    e.t = 7;
-  } else {
-    if (e.C & 0x8000000) {
-      e.T++;
-      e.C &= 0x7FFFFFF;
-    }
-    if (e.L >= 0) {
-      if ((uint32_t)e.L < bo.cap) bo.out[e.L] = (uint8_t)e.T; else bo.flags |= 1u;
-    }
-    e.L++;
-    if (e.T == 0xFF) {
-      e.T = (e.C >> 20) & 0xFF;
-      e.C &= 0xFFFFF;
-      e.t = 7;
-    } else {
-      e.T = (e.C >> 19) & 0xFF;
-      e.C &= 0x7FFFF;
-      e.t = 8;
-    }
+__device__ __forceinline__ void put_byte(const Mq &e, ByteOut &bo) {
+  if (e.L >= 0) {
+    if ((uint32_t)e.L < bo.cap) bo.out[e.L] = (uint8_t)e.T; else bo.flags |= 1u;
   }
 }
 
-// mq_bit_encode (mq.c:478-556); renormalisation shifts in blocks up to the next byte transfer
-__device__ __forceinline__ void mq_encode(Mq &e, uint8_t *ctx, const uint32_t *tbl, uint32_t k,
-                                          uint32_t s, ByteOut &bo) {
-  const uint32_t ent = tbl[ctx[k]];
-  const uint32_t p = ent & 0xFFFF;
-  e.A -= p;
-  if (s == ((ent >> 16) & 1)) {
-    if (e.A >= 0x8000) {
-      e.C += p;
-      return;
-    }
-    if (e.A < p) e.A = p; else e.C += p;
-    ctx[k] = (uint8_t)((ent >> 17) & 0x7F);
-  } else {
-    if (e.A < p) e.C += p; else e.A = p;
-    ctx[k] = (uint8_t)((ent >> 24) & 0x7F);
+// transfer_byte (mq.c:85-127), due now (t == 0)
+__device__ __forceinline__ void mq_transfer(Mq &e, ByteOut &bo) {
+  if (e.T != 0xFF && (e.C & 0x8000000u)) {
+    e.T++;
+    e.C &= 0x7FFFFFFu;
   }
-  int n = __clz(e.A) - 16;   // shifts until A >= 0x8000
-  while (n > 0) {
-    const int sh = min(n, e.t);
-    e.A <<= sh;
-    e.C <<= sh;
-    e.t -= sh;
-    n -= sh;
-    if (e.t == 0) mq_transfer(e, bo);
+  put_byte(e, bo);
+  e.L++;
+  if (e.T == 0xFF) {
+    e.T = (e.C >> 20) & 0xFF;
+    e.C &= 0xFFFFFu;
+    e.t += 7;
+  } else {
+    e.T = (e.C >> 19) & 0xFF;
+    e.C &= 0x7FFFFu;
+    e.t += 8;
   }
 }
 
 __device__ void mq_terminate(Mq &e, ByteOut &bo) {
+  // mq_termination (mq.c:706-759)
   int n = 12 - e.t;
   e.C <<= e.t;
+  e.t = 0;
   while (n > 0) {
     mq_transfer(e, bo);
     n -= e.t;
     e.C <<= e.t;
+    e.t = 0;
   }
   mq_transfer(e, bo);
 }
@@ -731,55 +703,30 @@ __device__ uint16_t slope2log(double lambda) {
   return (uint16_t)r;
 }
 
-// sequential reader of a 16-byte aligned symbol stream, one 16-byte load ahead (the arena has
-// slack after its last chunk for that read-ahead)
-struct SymReader {
-  const uint4 *p;
-  uint4 nxt;
-  uint64_t lo, hi;
-  int k;
-  __device__ __forceinline__ explicit SymReader(const uint8_t *base) {
-    p = reinterpret_cast<const uint4 *>(base);
-    const uint4 v = p[0];
-    lo = ((uint64_t)v.y << 32) | v.x;
-    hi = ((uint64_t)v.w << 32) | v.z;
-    nxt = p[1];
-    p += 2;
-    k = 0;
-  }
-  __device__ __forceinline__ uint32_t next() {
-    const uint32_t s = (uint32_t)(((k < 8) ? (lo >> (8 * k)) : (hi >> (8 * (k - 8)))) & 0xFF);
-    if (++k == 16) {
-      lo = ((uint64_t)nxt.y << 32) | nxt.x;
-      hi = ((uint64_t)nxt.w << 32) | nxt.z;
-      nxt = *p++;
-      k = 0;
-    }
-    return s;
-  }
-};
-
 __global__ void __launch_bounds__(kMqThreads) t1_mq_kernel(const CbDev *__restrict__ cbs,
                                                            uint32_t ncb,
                                                            const SbDev *__restrict__ sbs,
-                                                           T1EncOut out) {
+                                                           T1EncOut out, uint32_t lanes) {
   __shared__ uint32_t tbl[94];
   // context states, [context][thread]: every lane of a warp hits its own bank
   __shared__ uint32_t ctx_all[dev::kCtxTotal][kMqThreads];
   for (int i = threadIdx.x; i < 94; i += blockDim.x) tbl[i] = dev::c_mq_states[i];
   __syncthreads();
   // Every lane of the warp stays in the coding loop below (it synchronises warp-wide); lanes
-  // without a codeblock to code take part with Z = 0.  A codeblock whose symbol stream did not
+  // without a codeblock to code (beyond `lanes`, or past the last codeblock) take part with Z = 0.  A codeblock whose symbol stream did not
   // fit the arena is skipped: the host retries with a larger one.
-  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool lane_used = threadIdx.x < lanes;
+  const uint32_t c = blockIdx.x * lanes + (lane_used ? threadIdx.x : 0u);
   const uint32_t cc = (c < ncb) ? c : 0u;
-  const int K = (c < ncb) ? out.K[c] : 0;
+  const int K = (lane_used && c < ncb) ? out.K[c] : 0;
   const bool live = (K != 0) && !(out.flags[cc] & 8u);
   const CbDev cb = cbs[cc];
   const SbDev sb = sbs[cb.sb];
   const int Z = live ? out.Z[c] : 0;
+  // context slots hold their current state's table entry
   uint32_t *ctx = &ctx_all[0][threadIdx.x];   // context k at ctx[k * kMqThreads]
-  for (int i = 0; i < dev::kCtxTotal; ++i) ctx[i * kMqThreads] = dev::mq_initial_state(i);
+  for (int i = 0; i < dev::kCtxTotal; ++i)
+    ctx[i * kMqThreads] = tbl[dev::mq_initial_state(i)];
   const uint32_t *pcount = out.pass_count + (uint64_t)cc * kMaxPasses;
   const uint64_t *poff = out.pass_off + (uint64_t)cc * kMaxPasses;
   uint64_t *snaps = out.snaps + (uint64_t)cc * kMaxPasses * 2;
@@ -788,21 +735,20 @@ __global__ void __launch_bounds__(kMqThreads) t1_mq_kernel(const CbDev *__restri
   Mq e{0x8000u, 0u, 0u, 12, -1};
   auto snapshot = [&](int p) {
     snaps[2 * p] = ((uint64_t)e.A << 48) | ((uint64_t)(e.T & 0xFF) << 40) |
-                   ((uint64_t)(uint8_t)e.t << 32) | (uint64_t)e.C;
+                   ((uint64_t)(uint8_t)e.t << 32) | (uint64_t)(uint32_t)e.C;
     snaps[2 * p + 1] = (uint64_t)(int64_t)e.L;
   };
-  // One flat loop over the codeblock's symbols, kept converged across the warp's 32 codeblocks:
-  // the coding step is predicated, byte transfers run under warp-uniform tests, pass ends (rare,
-  // per lane) are the only divergent branch.  The next symbol's context state and table entry
-  // are fetched while the current symbol is coded; a state the current symbol just changed
-  // overrides them.
   int p = -1;
   uint32_t rem = 0;
-  const uint32_t *src = nullptr;   // current pass's symbols, four per 32-bit word
-  uint32_t w0 = 0, w1 = 0;         // current and next word
-  int kk = 0;                      // symbols left in w0
-  bool active = true;
-  uint32_t sym = 0, k = 0, st = 0, ent = 0;
+  // symbols of the current pass, four per word, the next word already in flight
+  const uint32_t *src = nullptr;
+  uint32_t w0 = 0, w1 = 0;
+  int kk = 0;
+  auto start_pass = [&](const uint8_t *base) {
+    src = reinterpret_cast<const uint32_t *>(base);
+    w1 = *src++;
+    kk = 0;
+  };
   auto next_symbol = [&]() -> uint32_t {
     if (kk == 0) {
       w0 = w1;
@@ -814,6 +760,12 @@ __global__ void __launch_bounds__(kMqThreads) t1_mq_kernel(const CbDev *__restri
     --kk;
     return v;
   };
+  bool active = true;
+  uint32_t sym = 0, k = 0, ent = 0;
+  // One flat loop over the codeblock's symbols, kept converged across the warp's 32 codeblocks:
+  // the coding step is predicated, byte transfers run under warp-uniform tests, pass ends (rare,
+  // per lane) are the only divergent branch.  The next symbol's context is fetched while the
+  // current symbol is coded; a context the current symbol just changed overrides it.
   while (__any_sync(0xffffffffu, active)) {
     if (active && rem == 0) {
       if (p >= 0) snapshot(p);
@@ -822,49 +774,43 @@ __global__ void __launch_bounds__(kMqThreads) t1_mq_kernel(const CbDev *__restri
         active = false;
       } else {
         rem = pcount[p];
-        src = reinterpret_cast<const uint32_t *>(out.symbols + poff[p]);
-        w1 = src[0];
-        ++src;
-        kk = 0;
+        start_pass(out.symbols + poff[p]);
         sym = next_symbol();
         k = sym >> 1;
-        st = ctx[k * kMqThreads];
-        ent = tbl[st];
+        ent = ctx[k * kMqThreads];
       }
     }
     uint32_t nsym = 0;
     if (active && rem > 1) nsym = next_symbol();
     const uint32_t nk = nsym >> 1;
-    const uint32_t nst_spec = ctx[nk * kMqThreads];
-    const uint32_t nent_spec = tbl[nst_spec];
-    // code (k, s) with state st / entry ent (mq.c:478-556)
-    const uint32_t s = sym & 1;
+    const uint32_t nent_spec = ctx[nk * kMqThreads];
+    // mq_bit_encode (mq.c:478-556)
     const uint32_t pq = ent & 0xFFFF;
     const uint32_t A1 = e.A - pq;
-    const bool is_mps = (s == ((ent >> 16) & 1));
+    const bool is_mps = ((sym ^ (ent >> 16)) & 1) == 0;
     const bool small = A1 < pq;
-    const bool keep = !active || (is_mps && (A1 >= 0x8000));   // no renormalisation
+    const bool keep = !active || (is_mps && A1 >= 0x8000u);   // no renormalisation
     if (active) {
       e.C += (keep || (is_mps != small)) ? pq : 0u;
       e.A = (is_mps == small) ? pq : A1;
     }
-    const uint32_t newst = keep ? st : (is_mps ? (ent >> 17) & 0x7F : (ent >> 24) & 0x7F);
-    if (active) ctx[k * kMqThreads] = newst;
-    int sh_left = keep ? 0 : (__clz(e.A) - 16);
-    // renormalisation: shift up to the next byte transfer, transfer, repeat (at most 3 times)
+    const uint32_t nidx = is_mps ? (ent >> 17) & 0x7F : (ent >> 24) & 0x7F;
+    const uint32_t nent = keep ? ent : tbl[nidx];
+    ctx[k * kMqThreads] = nent;
+    int sh = keep ? 0 : (__clz(e.A) - 16);   // shifts until A >= 0x8000
+    // shift up to each due transfer, transfer, continue (at most three transfers)
     for (int r = 0; r < 3; ++r) {
-      const int sh = min(sh_left, e.t);
-      e.A <<= sh;
-      e.C <<= sh;
-      e.t -= sh;
-      sh_left -= sh;
+      const int s1 = min(sh, e.t);
+      e.A <<= s1;
+      e.C <<= s1;
+      e.t -= s1;
+      sh -= s1;
       const bool go = (e.t == 0);
       if (!__any_sync(0xffffffffu, go)) break;
       if (go) mq_transfer(e, bo);
     }
     const bool same = (nk == k);
-    st = same ? newst : nst_spec;
-    ent = same ? (keep ? ent : tbl[newst]) : nent_spec;
+    ent = same ? nent : nent_spec;
     sym = nsym;
     k = nk;
     if (active) --rem;
@@ -961,6 +907,18 @@ __global__ void __launch_bounds__(kMqThreads) t1_mq_kernel(const CbDev *__restri
 
 size_t t1_model_smem(uint32_t max_cols) { return (size_t)max_cols * 3; }
 
+// Codeblocks per MQ warp.  Each lane runs one codeblock's coder, a long dependent chain, so a
+// warp is latency-bound and its lanes' pass ends and byte transfers diverge; fewer lanes per
+// warp waste less, until the warps' instructions saturate the schedulers.  Measured on B200
+// (FP64, 32x32x16 codeblocks): 1030 codeblocks code fastest at 1 per warp, 8192 at 4 per warp,
+// i.e. at about three warps per scheduler (148 SMs x 4).
+uint32_t mq_lanes_per_warp(uint32_t ncb) {
+  const uint32_t target_warps = (uint32_t)dev::kNumSMs * 4 * 3;
+  uint32_t lanes = 1;
+  while (lanes < 32 && ncb / (lanes * 2) >= target_warps) lanes *= 2;
+  return lanes;
+}
+
 void launch_t1_encode(const bwc_float *work, const FieldDims &dims, const CbDev *cbs, uint32_t ncb,
                       const SbDev *sbs, uchar erres, const T1EncOut &out, uint32_t max_cols,
                       cudaStream_t s) {
@@ -968,7 +926,8 @@ void launch_t1_encode(const bwc_float *work, const FieldDims &dims, const CbDev 
   const size_t smem = t1_model_smem(max_cols);
   cudaFuncSetAttribute(t1_model_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   t1_model_kernel<<<ncb, kModelThreads, smem, s>>>(work, dims, cbs, ncb, sbs, erres, out);
-  t1_mq_kernel<<<(ncb + kMqThreads - 1) / kMqThreads, kMqThreads, 0, s>>>(cbs, ncb, sbs, out);
+  const uint32_t lanes = mq_lanes_per_warp(ncb);
+  t1_mq_kernel<<<(ncb + lanes - 1) / lanes, kMqThreads, 0, s>>>(cbs, ncb, sbs, out, lanes);
 }
 
 }  // namespace bwcb
