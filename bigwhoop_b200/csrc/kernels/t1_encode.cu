@@ -450,7 +450,9 @@ __global__ void __launch_bounds__(kModelThreads)
         // significance propagation: fixed point of the post-pass significance
         for (uint32_t col = c0; col < c1; ++col) fin[col] = lo[col] & 0xF;
         __syncthreads();
-        for (int it = 0;; ++it) {
+        // every round that changes anything makes at least one more sample significant, so
+        // 4 * ncols + 1 rounds always suffice; the bound only guards against a logic error
+        for (uint32_t it = 0; it <= 4 * g.ncols; ++it) {
           int changed = 0;
           for (uint32_t col = c0; col < c1; ++col) {
             const uint32_t j = (col / g.W) % g.nstripes;
