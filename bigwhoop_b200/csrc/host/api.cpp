@@ -122,6 +122,7 @@ struct DeviceState {
   int device = -1;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[8] = {};
+  DevBuf temp;     // second field-sized buffer: the transform reads one and writes the other
   DevBuf in, work, keys, stats, cbtab, sbtab, bytes, scratch, snaps, dmse, K, Z, L, S, flags,
       slopes, counter, cs, blob, pieces, outbuf, mags, lmax, symbols, pcount, poff, symused;
   bool dump_set = false, ddump_set = false;
@@ -308,7 +309,8 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
     allcb.insert(allcb.end(), cbs[p].begin(), cbs[p].end());
     allsb.insert(allsb.end(), sbs[p].begin(), sbs[p].end());
   }
-  if (!dv->work.ensure(n * sizeof(bwc_float)) || !dv->keys.ensure(16 * info.nPar) ||
+  if (!dv->work.ensure(n * sizeof(bwc_float)) || !dv->temp.ensure(n * sizeof(bwc_float)) ||
+      !dv->keys.ensure(16 * info.nPar) ||
       !dv->stats.ensure(4 * sizeof(bwc_float) * info.nPar) ||
       !dv->cbtab.ensure(sizeof(CbDev) * ncb) || !dv->sbtab.ensure(sizeof(SbDev) * allsb.size()) ||
       !dv->bytes.ensure(byte_base[info.nPar]) || !dv->scratch.ensure(scr_base[info.nPar]) ||
@@ -348,14 +350,15 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
     cudaEvent_t a, b2, c2, d2;
     cudaEventCreate(&a); cudaEventCreate(&b2); cudaEventCreate(&c2); cudaEventCreate(&d2);
     cudaEventRecord(a, s);
-    launch_fill_minmax(src + (uint64_t)p * n * dsz, dsz == 8, n, dv->work.as<bwc_float>(),
+    launch_fill_minmax(src + (uint64_t)p * n * dsz, dsz == 8, n, dv->temp.as<bwc_float>(),
                        dv->keys.as<uint64_t>() + 2 * p, s);
-    launch_normalize(dv->work.as<bwc_float>(), n, dv->keys.as<uint64_t>() + 2 * p, c.Qm,
+    launch_normalize(dv->temp.as<bwc_float>(), n, dv->keys.as<uint64_t>() + 2 * p, c.Qm,
                      dv->stats.as<bwc_float>() + 4 * p, s);
     if (p == 0 && dv->dump_set && dv->dump.normalized)
-      cudaMemcpyAsync(dv->dump.normalized, dv->work.p, n * sizeof(bwc_float), cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(dv->dump.normalized, dv->temp.p, n * sizeof(bwc_float), cudaMemcpyDeviceToHost, s);
     cudaEventRecord(b2, s);
-    launch_dwt_forward(dv->work.as<bwc_float>(), dims, make_plan(c, tile.params[p]), s);
+    launch_dwt_forward(dv->work.as<bwc_float>(), dv->temp.as<bwc_float>(), dims,
+                       make_plan(c, tile.params[p]), s);
     if (p == 0 && dv->dump_set && dv->dump.transformed)
       cudaMemcpyAsync(dv->dump.transformed, dv->work.p, n * sizeof(bwc_float), cudaMemcpyDeviceToHost, s);
     cudaEventRecord(c2, s);
@@ -590,7 +593,8 @@ static uchar decompress_impl(bwc_codec *codec, bwc_stream *stream) {
     uint64_t gstate_bytes = 0;
     if (big)
       for (uint64_t i = 0; i < ncb; ++i) gstate_bytes = std::max<uint64_t>(gstate_bytes, cbs[i].scratch_off);
-    if (!dv->work.ensure(n * sizeof(bwc_float)) || !dv->cbtab.ensure(sizeof(CbDev) * ncb) ||
+    if (!dv->work.ensure(n * sizeof(bwc_float)) || !dv->temp.ensure(n * sizeof(bwc_float)) ||
+        !dv->cbtab.ensure(sizeof(CbDev) * ncb) ||
         !dv->sbtab.ensure(sizeof(SbDev) * sbs.size()) || !dv->bytes.ensure(off + 64) ||
         !dv->mags.ensure(st * sizeof(bwc_raw)) || !dv->K.ensure(ncb) || !dv->Z.ensure(ncb) ||
         !dv->lmax.ensure(ncb * 4) || !dv->flags.ensure(ncb * 4) || !dv->counter.ensure(4) ||
@@ -612,18 +616,19 @@ static uchar decompress_impl(bwc_codec *codec, bwc_stream *stream) {
     cudaEvent_t a, b2, c2, d2;
     cudaEventCreate(&a); cudaEventCreate(&b2); cudaEventCreate(&c2); cudaEventCreate(&d2);
     cudaEventRecord(a, s);
-    cudaMemsetAsync(dv->work.p, 0, n * sizeof(bwc_float), s);
+    cudaMemsetAsync(dv->temp.p, 0, n * sizeof(bwc_float), s);
     const int grid = t1_grid(nullptr, smem);
-    launch_t1_decode_ex(dv->work.as<bwc_float>(), dims, dv->cbtab.as<CbDev>(), (uint32_t)ncb,
+    launch_t1_decode_ex(dv->temp.as<bwc_float>(), dims, dv->cbtab.as<CbDev>(), (uint32_t)ncb,
                         dv->sbtab.as<SbDev>(), dv->bytes.as<uint8_t>(), dv->K.as<uint8_t>(),
                         dv->Z.as<uint8_t>(), dv->lmax.as<uint32_t>(), c.error_resilience,
                         dv->mags.as<bwc_raw>(), dv->flags.as<uint32_t>(), state_cap,
                         big ? dv->scratch.as<uint16_t>() : nullptr, dv->counter.as<uint32_t>(),
                         grid, s);
     if (p == 0 && dv->ddump_set && dv->ddump.dequantized)
-      cudaMemcpyAsync(dv->ddump.dequantized, dv->work.p, n * sizeof(bwc_float), cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(dv->ddump.dequantized, dv->temp.p, n * sizeof(bwc_float), cudaMemcpyDeviceToHost, s);
     cudaEventRecord(b2, s);
-    launch_dwt_inverse(dv->work.as<bwc_float>(), dims, make_plan(c, par), s);
+    launch_dwt_inverse(dv->work.as<bwc_float>(), dv->temp.as<bwc_float>(), dims,
+                       make_plan(c, par), s);
     if (p == 0 && dv->ddump_set && dv->ddump.reconstructed)
       cudaMemcpyAsync(dv->ddump.reconstructed, dv->work.p, n * sizeof(bwc_float), cudaMemcpyDeviceToHost, s);
     cudaEventRecord(c2, s);

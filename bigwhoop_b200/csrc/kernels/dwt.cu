@@ -2,18 +2,14 @@
 // (dwt.c:354-466 lifting, :286-342 boundary extension, :645-789 de-/interleave,
 // :1216-2246 level/axis drivers).
 //
-// Lines are staged in shared memory and lifted in place with four data-parallel steps.  The
-// reference extends each line by whole-point symmetric reflection (repeated for lines shorter
-// than the filter) and lifts the extension too; since reflection preserves index parity and
-// each lifting step updates mirrored samples with mirrored operands, reading neighbours through
-// the reflected index gives bit-identical results for every sample inside the line, which is
-// what is done here.  Arithmetic is the reference's: float-literal lifting constants in the
-// codec's type, a + c * (b0 + b1) with separately rounded products and sums.
-//
-//   rows kernel  (x axis): one CTA per group of rows, lines contiguous in HBM;
-//   cols kernel  (y/z/t axes): one CTA per tile of consecutive x columns and its whole line,
-//                 loaded as coalesced x-rows and lifted column-wise.
-// After lifting, even samples (low-pass) are stored first, odd samples (high-pass) after them.
+// Each level's spatial axes are transformed by one fused pass (dwt_level_kernel: a 3D tile with
+// halos in shared memory, lifted along x, y and z, interior stored de-interleaved), reading one
+// field-sized buffer and writing the other; the time axis of 4D fields, when transformed, gets
+// an in-place pass of its own (dwt_cols_kernel) in the reference's axis order.  Arithmetic is
+// the reference's: float-literal lifting constants in the codec's type, a + c * (b0 + b1) with
+// separately rounded products and sums, and whole-point symmetric extension of every line
+// (repeated for lines shorter than the filter), which the tiles reproduce by loading reflected
+// samples into their halos and lifting them like the reference lifts its extended lines.
 #include <algorithm>
 #include <cstdio>
 
@@ -62,69 +58,7 @@ __device__ __forceinline__ void inv_step(bwc_float *w, int n, int stride, int i)
   w[i * stride] = v;
 }
 
-// ---- x axis: rows --------------------------------------------------------------------------
-// block handles `rows` consecutive lines (index r -> (y, z, t) within the region)
-template <bool kForward>
-__global__ void __launch_bounds__(256) dwt_rows_kernel(bwc_float *__restrict__ work, int n,
-                                                       int rows_per_block, uint64_t nlines,
-                                                       uint32_t ey, uint32_t ez,
-                                                       uint64_t row_stride, uint64_t slab_stride,
-                                                       uint64_t vol_stride) {
-  extern __shared__ unsigned char smem_raw[];
-  bwc_float *sm = reinterpret_cast<bwc_float *>(smem_raw);
-  const uint64_t first = (uint64_t)blockIdx.x * rows_per_block;
-  const uint64_t left = nlines - first;
-  const int nrows = (int)(left < (uint64_t)rows_per_block ? left : (uint64_t)rows_per_block);
-  const int half = (n + 1) >> 1;
-  // load (forward: natural order; inverse: interleave lows/highs)
-  for (int r = 0; r < nrows; ++r) {
-    const uint64_t line = first + r;
-    const uint64_t y = line % ey, z = (line / ey) % ez, t = line / ((uint64_t)ey * ez);
-    const bwc_float *src = work + y * row_stride + z * slab_stride + t * vol_stride;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      int j = i;
-      if (!kForward) j = (i < half) ? 2 * i : 2 * (i - half) + 1;
-      sm[r * n + j] = src[i];
-    }
-  }
-  __syncthreads();
-  // each lifting step updates the samples of one parity of every row in parallel
-  const int tid = threadIdx.x, nth = blockDim.x;
-  const int per_row_odd = n >> 1, per_row_even = (n + 1) >> 1;
-#define ROW_STEP(FN, K, PAR)                                                           \
-  {                                                                                    \
-    const int cnt = (PAR) ? per_row_odd : per_row_even;                                \
-    for (int q = tid; q < nrows * cnt; q += nth) {                                     \
-      const int r = q / cnt, i = 2 * (q - r * cnt) + (PAR);                            \
-      FN<K>(sm + r * n, n, 1, i);                                               \
-    }                                                                                  \
-    __syncthreads();                                                                   \
-  }
-  if (kForward) {
-    ROW_STEP(fwd_step, 0, 1)
-    ROW_STEP(fwd_step, 1, 0)
-    ROW_STEP(fwd_step, 2, 1)
-    ROW_STEP(fwd_step, 3, 0)
-  } else {
-    ROW_STEP(inv_step, 0, 0)
-    ROW_STEP(inv_step, 1, 1)
-    ROW_STEP(inv_step, 2, 0)
-    ROW_STEP(inv_step, 3, 1)
-  }
-#undef ROW_STEP
-  for (int r = 0; r < nrows; ++r) {
-    const uint64_t line = first + r;
-    const uint64_t y = line % ey, z = (line / ey) % ez, t = line / ((uint64_t)ey * ez);
-    bwc_float *dst = work + y * row_stride + z * slab_stride + t * vol_stride;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      int j = i;
-      if (kForward) j = (i < half) ? 2 * i : 2 * (i - half) + 1;
-      dst[i] = sm[r * n + j];
-    }
-  }
-}
-
-// ---- y/z/t axes: columns ---------------------------------------------------------------------
+// ---- one axis in place: the time axis of 4D fields --------------------------------------------
 // block (tx, ty): tile of TX consecutive x positions, whole line of length n along the axis
 // with element stride `astride`; other coordinates: x-tile index, b (count eb, stride sb),
 // c (stride sc).
@@ -187,21 +121,6 @@ __global__ void __launch_bounds__(256) dwt_cols_kernel(bwc_float *__restrict__ w
 constexpr size_t kSmemBudget = 96 * 1024;
 
 template <bool kForward>
-void rows_pass(bwc_float *work, const FieldDims &d, const uint64_t *e, cudaStream_t s) {
-  const int n = (int)e[0];
-  const uint64_t nlines = e[1] * e[2] * e[3];
-  int rows = (int)std::max<size_t>(1, std::min<size_t>(kSmemBudget / (n * sizeof(bwc_float)),
-                                                       (size_t)std::max(1, 4096 / n)));
-  const size_t smem = (size_t)rows * n * sizeof(bwc_float);
-  const uint64_t blocks = (nlines + rows - 1) / rows;
-  auto k = dwt_rows_kernel<kForward>;
-  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBudget);
-  k<<<(unsigned)blocks, 256, smem, s>>>(work, n, rows, nlines, (uint32_t)e[1], (uint32_t)e[2],
-                                        d.width, d.width * d.height,
-                                        d.width * d.height * d.depth);
-}
-
-template <bool kForward>
 void cols_pass(bwc_float *work, const FieldDims &d, const uint64_t *e, int axis, cudaStream_t s) {
   const int n = (int)e[axis];
   const uint64_t stride[4] = {1, d.width, d.width * d.height, d.width * d.height * d.depth};
@@ -222,25 +141,323 @@ void cols_pass(bwc_float *work, const FieldDims &d, const uint64_t *e, int axis,
                                             stride[ob[1]], ntx);
 }
 
-}  // namespace
+// ---- fused x/y/z pass of one level ---------------------------------------------------------
+// One CTA transforms a tile of the level's region along every transformed spatial axis at once:
+// it loads the tile plus a 4-sample halo on each side of every transformed axis (whole-point
+// symmetric reflection at the region's edges, exactly the reference's line extension), lifts
+// along x, then y, then z in shared memory (forward; z, y, x for the inverse), and stores the
+// tile's interior -- de-interleaved (lows first) for the forward transform, in natural order for
+// the inverse.  Four lifting steps of radius one make every interior sample exact with a
+// 4-sample halo.  Tiles read `src` and write `dst`, two different buffers, so no tile can see
+// another tile's output.
+//
+// Tile: 32 x 16 x 16 samples with halos (interior 24 x 8 x 8 along transformed axes, the whole
+// 32 / 16 / 16 along untransformed ones).  Global loads and stores go a row per warp, so they
+// are contiguous; the lifting runs on whole lines held in registers, one line per thread, so
+// each axis costs one shared-memory read and write per sample.
+constexpr int kLX = 32, kLY = 16, kLZ = 16, kH = 4;
+constexpr int kFusedThreads = 256;
 
-void launch_dwt_forward(bwc_float *work, const FieldDims &dims, const DwtPlan &plan,
-                        cudaStream_t s) {
-  for (int l = 0; l < plan.levels; ++l) {
-    const uint64_t *e = plan.ext[l];
-    if (plan.axis_on[l] & 1) rows_pass<true>(work, dims, e, s);
-    for (int a = 1; a < 4; ++a)
-      if (plan.axis_on[l] & (1 << a)) cols_pass<true>(work, dims, e, a, s);
+struct LevelGeom {
+  uint32_t ex, ey, ez;       // region extents
+  uint32_t tx, ty, tz;       // interior tile extents (24 / 8 / 8 or 32 / 16 / 16)
+  uint32_t hx, hy, hz;       // halos (4 or 0)
+  uint32_t ntx, nty, ntz;    // tiles per axis
+  uint64_t sy, sz, st;       // buffer strides
+};
+
+__device__ __forceinline__ int reflect(int i, int n) {
+  while (i < 0 || i > n - 1) i = (i < 0) ? -i : 2 * (n - 1) - i;
+  return i;
+}
+
+// forward / inverse lifting step kStep at s[0] with neighbours s[-d], s[+d] (dwt.c:354-466)
+template <bool kFwd, int kStep>
+__device__ __forceinline__ void lift_at(bwc_float *s, int d) {
+  const bwc_float ab = dev::fadd(s[-d], s[d]);
+  bwc_float v = s[0];
+  if (kFwd) {
+    if (kStep == 0) v = dev::fadd(v, dev::fmul(kAlpha, ab));
+    if (kStep == 1) v = dev::fadd(v, dev::fmul(kBeta, ab));
+    if (kStep == 2) v = dev::fmul(kKappaH, dev::fadd(v, dev::fmul(kGamma, ab)));
+    if (kStep == 3) v = dev::fmul(kKappaL, dev::fadd(v, dev::fmul(kDelta, ab)));
+  } else {
+    if (kStep == 0) v = dev::fsub(dev::fmul(kKappaH, v), dev::fmul(kDelta, ab));
+    if (kStep == 1) v = dev::fsub(dev::fmul(kKappaL, v), dev::fmul(kGamma, ab));
+    if (kStep == 2) v = dev::fsub(v, dev::fmul(kBeta, ab));
+    if (kStep == 3) v = dev::fsub(v, dev::fmul(kAlpha, ab));
+  }
+  s[0] = v;
+}
+
+// The four lifting steps of one line held in registers (positions 0 and L-1 have only one
+// neighbour inside the tile and are never updated; the halo makes them irrelevant).
+template <bool kFwd, int L>
+__device__ __forceinline__ void lift_line(bwc_float (&v)[L]) {
+  // forward: odd, even, odd, even; inverse: even, odd, even, odd
+  constexpr int p0 = kFwd ? 1 : 0, p1 = 1 - p0;
+#pragma unroll
+  for (int i = 1; i < L - 1; ++i)
+    if ((i & 1) == p0) {
+      const bwc_float ab = dev::fadd(v[i - 1], v[i + 1]);
+      v[i] = kFwd ? dev::fadd(v[i], dev::fmul(kAlpha, ab))
+                  : dev::fsub(dev::fmul(kKappaH, v[i]), dev::fmul(kDelta, ab));
+    }
+#pragma unroll
+  for (int i = 1; i < L - 1; ++i)
+    if ((i & 1) == p1) {
+      const bwc_float ab = dev::fadd(v[i - 1], v[i + 1]);
+      v[i] = kFwd ? dev::fadd(v[i], dev::fmul(kBeta, ab))
+                  : dev::fsub(dev::fmul(kKappaL, v[i]), dev::fmul(kGamma, ab));
+    }
+#pragma unroll
+  for (int i = 1; i < L - 1; ++i)
+    if ((i & 1) == p0) {
+      const bwc_float ab = dev::fadd(v[i - 1], v[i + 1]);
+      v[i] = kFwd ? dev::fmul(kKappaH, dev::fadd(v[i], dev::fmul(kGamma, ab)))
+                  : dev::fsub(v[i], dev::fmul(kBeta, ab));
+    }
+#pragma unroll
+  for (int i = 1; i < L - 1; ++i)
+    if ((i & 1) == p1) {
+      const bwc_float ab = dev::fadd(v[i - 1], v[i + 1]);
+      v[i] = kFwd ? dev::fmul(kKappaL, dev::fadd(v[i], dev::fmul(kDelta, ab)))
+                  : dev::fsub(v[i], dev::fmul(kAlpha, ab));
+    }
+}
+
+// shared-memory tile: rows of kLX samples padded to kPX, so that a warp whose lanes each walk
+// their own row touches 32 different bank pairs
+constexpr int kPX = kLX + 1;
+
+__device__ __forceinline__ int tix(int x, int y, int z) { return (z * kLY + y) * kPX + x; }
+
+// the x-rows with y in [y_lo, y_hi) and z in [z_lo, z_hi), one row per thread
+template <bool kFwd>
+__device__ __forceinline__ void lift_x(bwc_float *sm, int y_lo, int y_hi, int z_lo, int z_hi) {
+  static_assert(kLY * kLZ == kFusedThreads, "one x-row per thread");
+  const int y = threadIdx.x % kLY, z = threadIdx.x / kLY;
+  if (y >= y_lo && y < y_hi && z >= z_lo && z < z_hi) {
+    bwc_float v[kLX];
+    bwc_float *row = sm + threadIdx.x * kPX;
+#pragma unroll
+    for (int i = 0; i < kLX; ++i) v[i] = row[i];
+    lift_line<kFwd, kLX>(v);
+#pragma unroll
+    for (int i = 0; i < kLX; ++i) row[i] = v[i];
+  }
+  __syncthreads();
+}
+
+// the y-columns (kAxis 1) or z-columns (kAxis 2) with x in [x_lo, x_hi) and the remaining
+// coordinate (z for y-columns, y for z-columns) in [o_lo, o_hi); lanes walk consecutive x
+template <bool kFwd, int kAxis>
+__device__ __forceinline__ void lift_yz(bwc_float *sm, int x_lo, int x_hi, int o_lo, int o_hi) {
+  constexpr int L = (kAxis == 1) ? kLY : kLZ;
+  constexpr int d = (kAxis == 1) ? kPX : kPX * kLY;
+  const int x = threadIdx.x & 31;
+  if (x >= x_lo && x < x_hi) {
+    for (int o = o_lo + (threadIdx.x >> 5); o < o_hi; o += kFusedThreads / 32) {
+      bwc_float *col = sm + ((kAxis == 1) ? tix(x, 0, o) : tix(x, o, 0));
+      bwc_float v[L];
+#pragma unroll
+      for (int i = 0; i < L; ++i) v[i] = col[i * d];
+      lift_line<kFwd, L>(v);
+#pragma unroll
+      for (int i = 0; i < L; ++i) col[i * d] = v[i];
+    }
+  }
+  __syncthreads();
+}
+
+// asynchronous global -> shared copy of one sample (no register staging, many in flight)
+__device__ __forceinline__ void copy_async(bwc_float *dst_smem, const bwc_float *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+  if (sizeof(bwc_float) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src));
+}
+
+// position of natural index g of an axis of extent e in the de-interleaved layout
+__device__ __forceinline__ uint32_t mallat(uint32_t g, uint32_t e, bool on) {
+  return on ? ((g & 1) ? ((e + 1) >> 1) + (g >> 1) : (g >> 1)) : g;
+}
+
+template <bool kFwd>
+__global__ void __launch_bounds__(kFusedThreads)
+    dwt_level_kernel(const bwc_float *__restrict__ src, bwc_float *__restrict__ dst,
+                     LevelGeom g) {
+  extern __shared__ unsigned char smem_raw[];
+  bwc_float *sm = reinterpret_cast<bwc_float *>(smem_raw);
+  uint32_t b = blockIdx.x;
+  const uint32_t bx = b % g.ntx;
+  b /= g.ntx;
+  const uint32_t by = b % g.nty;
+  b /= g.nty;
+  const uint32_t bz = b % g.ntz;
+  const uint32_t t = b / g.ntz;
+  const int x0 = (int)(bx * g.tx) - (int)g.hx;
+  const int y0 = (int)(by * g.ty) - (int)g.hy;
+  const int z0 = (int)(bz * g.tz) - (int)g.hz;
+  const bool onx = g.hx != 0, ony = g.hy != 0, onz = g.hz != 0;
+  const bwc_float *sbase = src + (uint64_t)t * g.st;
+  bwc_float *dbase = dst + (uint64_t)t * g.st;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // Row offsets, one per thread (kLY * kLZ == kFusedThreads): the source row of each tile row
+  // (reflected on transformed axes, clamped on untransformed ones -- clamped values are never
+  // stored) and the destination row of each interior row (~0 where it lies outside the region).
+  __shared__ uint64_t row_src[kLY * kLZ], row_dst[kLY * kLZ];
+  {
+    const int ly = threadIdx.x % kLY, lz = threadIdx.x / kLY;
+    int gy = y0 + ly, gz = z0 + lz;
+    const bool inside = gy >= 0 && gz >= 0 && gy < (int)g.ey && gz < (int)g.ez &&
+                        ly >= (int)g.hy && ly < (int)(g.hy + g.ty) && lz >= (int)g.hz &&
+                        lz < (int)(g.hz + g.tz);
+    row_dst[threadIdx.x] =
+        inside ? (uint64_t)(kFwd ? mallat((uint32_t)gy, g.ey, ony) : (uint32_t)gy) * g.sy +
+                     (uint64_t)(kFwd ? mallat((uint32_t)gz, g.ez, onz) : (uint32_t)gz) * g.sz
+               : ~0ull;
+    gy = ony ? reflect(gy, (int)g.ey) : min(gy, (int)g.ey - 1);
+    gz = onz ? reflect(gz, (int)g.ez) : min(gz, (int)g.ez - 1);
+    row_src[threadIdx.x] =
+        (uint64_t)(kFwd ? (uint32_t)gy : mallat((uint32_t)gy, g.ey, ony)) * g.sy +
+        (uint64_t)(kFwd ? (uint32_t)gz : mallat((uint32_t)gz, g.ez, onz)) * g.sz;
+  }
+  __syncthreads();
+  // load: one x-row per warp iteration, all rows in flight at once
+  {
+    int gx = x0 + lane;
+    gx = onx ? reflect(gx, (int)g.ex) : min(gx, (int)g.ex - 1);
+    const bwc_float *lsrc = sbase + (kFwd ? (uint32_t)gx : mallat((uint32_t)gx, g.ex, onx));
+    bwc_float *ldst = sm + lane;
+#pragma unroll 8
+    for (int r = warp; r < kLY * kLZ; r += kFusedThreads / 32)
+      copy_async(ldst + r * kPX, lsrc + row_src[r]);
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+  }
+  __syncthreads();
+  // Lift every line along each transformed axis whose samples can reach the stored interior:
+  // forward x on all rows, y on interior x, z on interior x and y; inverse z on all columns, y
+  // on interior z, x on interior y and z.
+  const int ix0 = (int)g.hx, ix1 = (int)(g.hx + g.tx);
+  if (kFwd) {
+    if (onx) lift_x<true>(sm, 0, kLY, 0, kLZ);
+    if (ony) lift_yz<true, 1>(sm, ix0, ix1, 0, kLZ);
+    if (onz) lift_yz<true, 2>(sm, ix0, ix1, (int)g.hy, (int)(g.hy + g.ty));
+  } else {
+    if (onz) lift_yz<false, 2>(sm, 0, kLX, 0, kLY);
+    if (ony) lift_yz<false, 1>(sm, 0, kLX, (int)g.hz, (int)(g.hz + g.tz));
+    if (onx) lift_x<false>(sm, (int)g.hy, (int)(g.hy + g.ty), (int)g.hz, (int)(g.hz + g.tz));
+  }
+  // store the interior
+  {
+    const int lx = ix0 + lane;
+    const uint32_t gx = (uint32_t)(x0 + lx);
+    if (lane < (int)g.tx && gx < g.ex) {
+      bwc_float *sdst = dbase + (kFwd ? mallat(gx, g.ex, onx) : gx);
+      for (int r = warp; r < kLY * kLZ; r += kFusedThreads / 32) {
+        const uint64_t o = row_dst[r];
+        if (o != ~0ull) sdst[o] = sm[r * kPX + lx];
+      }
+    }
   }
 }
 
-void launch_dwt_inverse(bwc_float *work, const FieldDims &dims, const DwtPlan &plan,
-                        cudaStream_t s) {
+// dst = src over the box [0, e0) x [0, e1) x [0, e2) x [0, e3) of the buffer
+__global__ void __launch_bounds__(256) copy_region_kernel(const bwc_float *__restrict__ src,
+                                                          bwc_float *__restrict__ dst,
+                                                          uint32_t e0, uint32_t e1, uint32_t e2,
+                                                          uint64_t rows, uint64_t sy, uint64_t sz,
+                                                          uint64_t st) {
+  for (uint64_t r = blockIdx.x; r < rows; r += gridDim.x) {
+    const uint64_t y = r % e1, z = (r / e1) % e2, t = r / ((uint64_t)e1 * e2);
+    const uint64_t base = y * sy + z * sz + t * st;
+    for (uint32_t x = threadIdx.x; x < e0; x += blockDim.x) dst[base + x] = src[base + x];
+  }
+}
+
+void copy_region(const bwc_float *src, bwc_float *dst, const FieldDims &d, const uint64_t *e,
+                 cudaStream_t s) {
+  const uint64_t rows = e[1] * e[2] * e[3];
+  if (!rows || !e[0]) return;
+  const unsigned grid = (unsigned)std::min<uint64_t>(rows, (uint64_t)dev::kNumSMs * 64);
+  copy_region_kernel<<<grid, 256, 0, s>>>(src, dst, (uint32_t)e[0], (uint32_t)e[1],
+                                          (uint32_t)e[2], rows, d.width, d.width * d.height,
+                                          d.width * d.height * d.depth);
+}
+
+template <bool kFwd>
+void level_pass(const bwc_float *src, bwc_float *dst, const FieldDims &d, const uint64_t *e,
+                uint8_t on, cudaStream_t s) {
+  LevelGeom g;
+  g.ex = (uint32_t)e[0];
+  g.ey = (uint32_t)e[1];
+  g.ez = (uint32_t)e[2];
+  g.hx = (on & 1) ? kH : 0;
+  g.hy = (on & 2) ? kH : 0;
+  g.hz = (on & 4) ? kH : 0;
+  g.tx = kLX - 2 * g.hx;
+  g.ty = kLY - 2 * g.hy;
+  g.tz = kLZ - 2 * g.hz;
+  g.ntx = (g.ex + g.tx - 1) / g.tx;
+  g.nty = (g.ey + g.ty - 1) / g.ty;
+  g.ntz = (g.ez + g.tz - 1) / g.tz;
+  g.sy = d.width;
+  g.sz = d.width * d.height;
+  g.st = d.width * d.height * d.depth;
+  const uint64_t blocks = (uint64_t)g.ntx * g.nty * g.ntz * e[3];
+  const size_t smem = (size_t)kPX * kLY * kLZ * sizeof(bwc_float);
+  auto k = dwt_level_kernel<kFwd>;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k<<<(unsigned)blocks, kFusedThreads, smem, s>>>(src, dst, g);
+}
+
+}  // namespace
+
+// Forward: `temp` holds the normalised field on entry; the coefficients end in `work`.  Even
+// levels go temp -> work and odd levels work -> temp, each level reading one buffer and writing
+// the other.  The high bands a level leaves in temp (odd levels) are copied back to work before
+// the next level overwrites the lows inside them, and after the last level.  The time axis of
+// 4D fields is transformed by a separate in-place pass after the spatial axes of each level.
+void launch_dwt_forward(bwc_float *work, bwc_float *temp, const FieldDims &dims,
+                        const DwtPlan &plan, cudaStream_t s) {
+  const uint64_t full[4] = {dims.width, dims.height, dims.depth, dims.dt};
+  if (plan.levels == 0) {
+    copy_region(temp, work, dims, full, s);
+    return;
+  }
+  for (int l = 0; l < plan.levels; ++l) {
+    const uint64_t *e = plan.ext[l];
+    const bool even = (l % 2) == 0;
+    const bwc_float *src = even ? temp : work;
+    bwc_float *dst = even ? work : temp;
+    if (even && l > 0) copy_region(temp, work, dims, plan.ext[l - 1], s);
+    level_pass<true>(src, dst, dims, e, plan.axis_on[l] & 7, s);
+    if (plan.axis_on[l] & 8) cols_pass<true>(dst, dims, e, 3, s);
+  }
+  if (plan.levels % 2 == 0) copy_region(temp, work, dims, plan.ext[plan.levels - 1], s);
+}
+
+// Inverse: `temp` holds the coefficients on entry (scratch afterwards); the field ends in
+// `work`.  Level l reads temp when l is even and work when l is odd, so the odd levels' inputs
+// (their high bands) are copied to work once at the start; every level's lows come from the
+// level above, written into the buffer it reads.
+void launch_dwt_inverse(bwc_float *work, bwc_float *temp, const FieldDims &dims,
+                        const DwtPlan &plan, cudaStream_t s) {
+  const uint64_t full[4] = {dims.width, dims.height, dims.depth, dims.dt};
+  if (plan.levels == 0) {
+    copy_region(temp, work, dims, full, s);
+    return;
+  }
+  if (plan.levels > 1) copy_region(temp, work, dims, plan.ext[1], s);
   for (int l = plan.levels - 1; l >= 0; --l) {
     const uint64_t *e = plan.ext[l];
-    for (int a = 3; a >= 1; --a)
-      if (plan.axis_on[l] & (1 << a)) cols_pass<false>(work, dims, e, a, s);
-    if (plan.axis_on[l] & 1) rows_pass<false>(work, dims, e, s);
+    const bool even = (l % 2) == 0;
+    bwc_float *src = even ? temp : work;
+    bwc_float *dst = even ? work : temp;
+    if (plan.axis_on[l] & 8) cols_pass<false>(src, dims, e, 3, s);
+    level_pass<false>(src, dst, dims, e, plan.axis_on[l] & 7, s);
   }
 }
 

@@ -60,7 +60,7 @@ void launch_normalize(bwc_float *work, uint64_t n, const uint64_t *minmax_keys, 
 void launch_denormalize(const bwc_float *work, uint64_t n, bwc_float pmin, bwc_float pmax,
                         uint8_t Qm, void *dst, bool dst_double, cudaStream_t s);
 
-// dwt.cu: the multi-level separable 9/7 transform of one parameter, in place.
+// dwt.cu: the multi-level separable 9/7 transform of one parameter.
 // level_ext[l] = extents (x, y, z, t) of the region transformed at level l; axis_on[l] bit a
 // set when axis a is transformed at level l.
 struct DwtPlan {
@@ -68,10 +68,12 @@ struct DwtPlan {
   uint64_t ext[16][4];
   uint8_t axis_on[16];
 };
-void launch_dwt_forward(bwc_float *work, const FieldDims &dims, const DwtPlan &plan,
-                        cudaStream_t s);
-void launch_dwt_inverse(bwc_float *work, const FieldDims &dims, const DwtPlan &plan,
-                        cudaStream_t s);
+// Forward: `temp` holds the normalised field on entry, the coefficients end in `work`;
+// inverse: `temp` holds the coefficients, the field ends in `work`.  `temp` is scratch after.
+void launch_dwt_forward(bwc_float *work, bwc_float *temp, const FieldDims &dims,
+                        const DwtPlan &plan, cudaStream_t s);
+void launch_dwt_inverse(bwc_float *work, bwc_float *temp, const FieldDims &dims,
+                        const DwtPlan &plan, cudaStream_t s);
 
 // t1_encode.cu: context modelling (one CTA per codeblock, max_cols = largest number of stripe
 // columns of a codeblock) followed by MQ coding (one thread per codeblock).
