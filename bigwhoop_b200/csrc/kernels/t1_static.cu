@@ -1,0 +1,167 @@
+// Tier-1 encoding of one codeblock with no memory allocation at all:
+// bwc_b200_t1_encode_codeblock_static.
+//
+// Who needs it: code that must not call cudaMalloc -- a caller working inside a framework whose
+// memory pool owns the device memory, a code path recorded into a stream capture, where an
+// allocation is not allowed, or a latency-bound service that cannot afford the implicit
+// synchronisation of an allocation.  Such a caller owns its inputs and outputs already; what it
+// cannot provide is this library's tier-1 working memory (bit planes, the symbol arena, coder
+// snapshots).  Here that working memory is one fixed static device array, sized for the largest
+// codeblock the entry point accepts; every GPU that loads the library holds it until the
+// process exits.
+//
+// The kernels are the ones bwc_compress runs (t1_model_kernel, t1_mq_kernel through
+// launch_t1_encode); only where their scratch lives differs.
+#include <cstdio>
+#include <mutex>
+
+#include "bwc_b200.h"
+#include "device_common.cuh"
+
+namespace bwcb {
+namespace {
+
+// Largest codeblock: 4096 stripe columns (16384 samples, e.g. 32 x 32 x 16 -- the codeblock of
+// the benchmark workload -- or 64 x 64 x 4).
+constexpr uint32_t kStaticMaxCols = 4096;
+constexpr uint64_t kMaxPlanes = kPrecBit + 1;
+// A stripe column emits at most 10 symbols per bit plane (run mode: 3, then sign and three
+// significance/sign pairs), error resilience 4 per plane, every pass is padded to 16 bytes, and
+// the MQ coder reads up to 256 bytes past the last chunk.
+constexpr uint64_t kArenaBytes =
+    ((uint64_t)kStaticMaxCols * 10 * kMaxPlanes + 4 * kMaxPlanes + 16ull * kMaxPasses + 256 +
+     255) & ~255ull;
+
+constexpr uint64_t round256(uint64_t v) { return (v + 255) & ~255ull; }
+// layout of the static area
+constexpr uint64_t kOffPlanes = 0;
+constexpr uint64_t kOffArena = round256(kOffPlanes + (uint64_t)kStaticMaxCols * kMaxPlanes);
+constexpr uint64_t kOffSnaps = round256(kOffArena + kArenaBytes);
+constexpr uint64_t kOffDmse = round256(kOffSnaps + 16ull * kMaxPasses);
+constexpr uint64_t kOffPcount = round256(kOffDmse + 8ull * kMaxPasses);
+constexpr uint64_t kOffPoff = round256(kOffPcount + 4ull * kMaxPasses);
+constexpr uint64_t kOffUsed = round256(kOffPoff + 8ull * kMaxPasses);   // symbol bump counter
+constexpr uint64_t kOffSlopes = kOffUsed + 8;                            // slope min / max
+constexpr uint64_t kOffFlags = kOffSlopes + 8;                           // codeblock flags
+constexpr uint64_t kOffCb = round256(kOffFlags + 4);
+constexpr uint64_t kOffSb = round256(kOffCb + sizeof(CbDev));
+constexpr uint64_t kStaticBytes = round256(kOffSb + sizeof(SbDev));
+
+// about 2.9 MB in the double build, 1.5 MB in the single build
+static __device__ __align__(256) unsigned char g_t1_static[kStaticBytes];
+
+// device address of g_t1_static, looked up once per device (in host code the array's name is
+// only a host-side stand-in for the symbol)
+constexpr int kMaxDevices = 64;
+std::mutex g_setup_mutex;
+unsigned char *g_static_addr[kMaxDevices] = {};
+
+unsigned char *static_area(int device) {
+  std::lock_guard<std::mutex> lock(g_setup_mutex);
+  if (!g_static_addr[device]) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_t1_static);
+    if (e != cudaSuccess) {
+      fprintf(stderr, "bwc: static tier-1 scratch unavailable on device %d: %s\n", device,
+              cudaGetErrorString(e));
+      return nullptr;
+    }
+    g_static_addr[device] = static_cast<unsigned char *>(p);
+  }
+  return g_static_addr[device];
+}
+
+int reject(const char *why) {
+  fprintf(stderr, "bwc_b200_t1_encode_codeblock_static: %s\n", why);
+  return 1;
+}
+
+}  // namespace
+}  // namespace bwcb
+
+using namespace bwcb;
+
+extern "C" int bwc_b200_t1_encode_codeblock_static(
+    const bwc_float *coeffs, uint64 nX, uint64 nY, uint64 nZ, uint64 nTS, const uint64 *box,
+    bwc_float qt_eff, double gain_step2, uint8 highband, uchar erres, uint8 *K, uint8 *Z,
+    uint32 *L, uint16 *S, uint8 *bytes, uint32 bytes_cap, uint32 *status, void *stream) {
+  if (!coeffs || !box || !K || !Z || !L || !S || !bytes || !status)
+    return reject("a buffer pointer is NULL");
+  if (!nX || !nY || !nZ || !nTS) return reject("field extents must be positive");
+  const uint64 dims[4] = {nX, nY, nZ, nTS};
+  for (int a = 0; a < 4; ++a)
+    if (box[a] >= box[4 + a] || box[4 + a] > dims[a])
+      return reject("codeblock box is empty or outside the field");
+  const uint64 w = box[4] - box[0], h = box[5] - box[1], d = box[6] - box[2], nt = box[7] - box[3];
+  const uint64 ncols = w * ((h + 3) / 4) * d * nt;
+  if (ncols > kStaticMaxCols) {
+    char msg[160];
+    snprintf(msg, sizeof msg,
+             "codeblock has %llu stripe columns; the static working memory holds at most %u "
+             "(16384 samples)", (unsigned long long)ncols, kStaticMaxCols);
+    return reject(msg);
+  }
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kMaxDevices)
+    return reject("no usable current CUDA device");
+  unsigned char *base = static_area(device);
+  if (!base) return 1;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+
+  CbDev cb{};
+  cb.x0 = (uint32_t)box[0];
+  cb.y0 = (uint32_t)box[1];
+  cb.z0 = (uint32_t)box[2];
+  cb.t0 = (uint32_t)box[3];
+  cb.w = (uint32_t)w;
+  cb.h = (uint32_t)h;
+  cb.d = (uint32_t)d;
+  cb.nt = (uint32_t)nt;
+  cb.out_off = 0;
+  cb.scratch_off = 0;
+  cb.out_cap = bytes_cap;
+  cb.sb = 0;
+  SbDev sb{};
+  sb.gain_step2 = gain_step2;
+  sb.qt_eff = qt_eff;
+  sb.Kmax = 0;
+  // significance-context class from the subband's high-pass axes (tier1.c:2416-2446)
+  sb.cls = ((highband & 3) == 1) ? 1u : ((highband & 3) == 3) ? 2u : 0u;
+  const uint32_t slopes_init[2] = {0xFFFF, 0};
+
+  // The static area keeps the previous call's contents: the symbol counter, the slope range
+  // and the flags must start from zero (slope minimum from 0xFFFF); planes, symbol chunks,
+  // snapshots and per-pass records are rewritten before they are read.
+  cudaMemcpyAsync(base + kOffCb, &cb, sizeof cb, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(base + kOffSb, &sb, sizeof sb, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(base + kOffSlopes, slopes_init, sizeof slopes_init, cudaMemcpyHostToDevice, s);
+  cudaMemsetAsync(base + kOffUsed, 0, 8, s);
+  cudaMemsetAsync(base + kOffFlags, 0, 4, s);
+
+  T1EncOut o;
+  o.bytes = bytes;
+  o.K = K;
+  o.Z = Z;
+  o.L = L;
+  o.S = S;
+  o.slopes = reinterpret_cast<uint32_t *>(base + kOffSlopes);
+  o.flags = reinterpret_cast<uint32_t *>(base + kOffFlags);
+  o.planes = base + kOffPlanes;
+  o.snaps = reinterpret_cast<uint64_t *>(base + kOffSnaps);
+  o.dmse = reinterpret_cast<int64_t *>(base + kOffDmse);
+  o.symbols = base + kOffArena;
+  o.sym_cap = kArenaBytes - 256;
+  o.sym_used = reinterpret_cast<unsigned long long *>(base + kOffUsed);
+  o.pass_count = reinterpret_cast<uint32_t *>(base + kOffPcount);
+  o.pass_off = reinterpret_cast<uint64_t *>(base + kOffPoff);
+  FieldDims fd{nX, nY, nZ, nTS};
+  launch_t1_encode(coeffs, fd, reinterpret_cast<const CbDev *>(base + kOffCb), 1,
+                   reinterpret_cast<const SbDev *>(base + kOffSb), erres, o, (uint32_t)ncols, s);
+  cudaMemcpyAsync(status, base + kOffFlags, 4, cudaMemcpyDeviceToDevice, s);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    fprintf(stderr, "bwc_b200_t1_encode_codeblock_static: %s\n", cudaGetErrorString(e));
+    return 1;
+  }
+  return 0;
+}

@@ -96,6 +96,51 @@ size_t bwc_b200_assemble_from_tier1(bwc_codec *const codec, bwc_stream *const st
  * download, [7] total.  Returns the number of entries written (at most n). */
 int    bwc_b200_last_timings(bwc_codec *const codec, double *out_ms, int n);
 
+/* Tier-1 encoding of ONE codeblock without any memory allocation.  No counterpart in the
+ * reference API.
+ *
+ * For callers that cannot call cudaMalloc -- code that gets its device memory from a
+ * framework's pool, code recorded into a stream capture, latency-bound services that cannot
+ * take the synchronisation an allocation implies.  The caller passes device buffers it owns;
+ * the library's own working memory (bit planes, symbol arena, coder snapshots) is one fixed
+ * static device area of about 2.9 MB (double build; 1.5 MB single), held by every GPU that
+ * loads the library until the process exits.
+ *
+ *   coeffs          device pointer: wavelet coefficients of one parameter, nX x nY x nZ x nTS
+ *                   bwc_float values, x fastest (the layout bwc_compress transforms into);
+ *   box             host array: X0, Y0, Z0, TS0, X1, Y1, Z1, TS1 of the codeblock in `coeffs`;
+ *   qt_eff          the subband's effective quantisation step;
+ *   gain_step2      (double)dwt_gain * (double)(qt_step_size * qt_step_size), the distortion
+ *                   weight of the subband;
+ *   highband        the subband's high-pass axis flags (bit 0 x, 1 y, 2 z, 3 t);
+ *   erres           error resilience (segmentation symbols);
+ *   K, Z            device, one byte each: significant bit planes and coding passes;
+ *   L, S            device: MAXIMUM_NO_PASSES truncation lengths and MAXIMUM_NO_PASSES + 1
+ *                   log slopes (only the first Z, resp. Z + 1, are written);
+ *   bytes           device: the codeblock's coded bytes, bytes_cap of room (L[Z-1] are
+ *                   valid; up to 16 zero bytes after them are written too);
+ *   status          device, one uint32: 0, or 1 = bytes_cap too small, 2/4 = see the flags of
+ *                   the stage dump (not expected), 8 = symbol arena full (not possible within
+ *                   the size limit);
+ *   stream          cudaStream_t to run on (NULL = default stream).
+ * Results are identical to what bwc_compress computes for the same codeblock.
+ *
+ * Limit: at most 4096 stripe columns (width x ceil(height / 4) x depth x time steps, e.g. a
+ * 32 x 32 x 16 codeblock); larger ones are rejected with a message on stderr and return 1.
+ * Returns 0 once the work is queued on `stream`, 1 on rejected arguments or a CUDA error.
+ *
+ * The static area is shared by every call on a device and keeps the last call's contents, so
+ * calls that overlap on the GPU (different streams, or host threads without ordering) race
+ * and corrupt each other; order them on one stream.  The first call on a device looks up the
+ * area's device address (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture. */
+int    bwc_b200_t1_encode_codeblock_static(const bwc_float *coeffs, uint64 nX, uint64 nY,
+                                           uint64 nZ, uint64 nTS, const uint64 *box,
+                                           bwc_float qt_eff, double gain_step2, uint8 highband,
+                                           uchar erres, uint8 *K, uint8 *Z, uint32 *L,
+                                           uint16 *S, uint8 *bytes, uint32 bytes_cap,
+                                           uint32 *status, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
