@@ -155,6 +155,8 @@ def load(precision="double"):
         "bwc_b200_parsed_codeblock": (C.c_int, [cp, u8, u64, vp, vp]),
         "bwc_b200_assemble_from_tier1": (C.c_size_t, [cp, vp, vp, vp, vp, vp, vp, vp, vp,
                                                       C.c_uint16, C.c_uint16]),
+        "bwc_b200_compress_batch": (C.c_uint8, [vp, vp, C.c_uint32, vp]),
+        "bwc_b200_last_batch_timings": (C.c_int, [vp, C.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -387,6 +389,34 @@ class Decompressor:
             self.close()
         except Exception:
             pass
+
+
+def compress_batch(compressors):
+    """Compress several prepared `Compressor`s with one bwc_b200_compress_batch call.  All must
+    use the same precision build.  Returns a list with each codestream (bytes) when the
+    compressor writes to host memory, else its length."""
+    if not compressors:
+        return []
+    prec = compressors[0].precision
+    if any(c.precision != prec for c in compressors):
+        raise ValueError("a batch runs in one precision build")
+    L = load(prec)
+    n = len(compressors)
+    codecs = (C.c_void_p * n)(*[C.cast(c.codec, C.c_void_p).value for c in compressors])
+    streams = (C.c_void_p * n)(*[c.stream for c in compressors])
+    sizes = (C.c_size_t * n)()
+    if L.bwc_b200_compress_batch(codecs, streams, n, sizes):
+        raise RuntimeError("bwc_b200_compress_batch failed")
+    out = []
+    for c, sz in zip(compressors, sizes):
+        out.append(bytes(c.out[:sz]) if isinstance(c.out, np.ndarray) else int(sz))
+    return out
+
+
+def batch_timings(precision="double"):
+    out = np.zeros(6)
+    k = load(precision).bwc_b200_last_batch_timings(out.ctypes.data, 6)
+    return out[:k]
 
 
 def decompress_array(codestream, precision="double", layer=0):

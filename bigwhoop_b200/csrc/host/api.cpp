@@ -18,8 +18,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <map>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "../kernels/kernels.hpp"
@@ -131,7 +133,7 @@ struct DeviceState {
   double timings[10] = {};   // stage times (ms); [8] tier-1 symbols coded (millions)
 
   ~DeviceState() {
-    DevBuf *all[] = {&in, &work, &keys, &stats, &cbtab, &sbtab, &bytes, &scratch, &snaps, &dmse,
+    DevBuf *all[] = {&temp, &in, &work, &keys, &stats, &cbtab, &sbtab, &bytes, &scratch, &snaps, &dmse,
                      &K, &Z, &L, &S, &flags, &slopes, &counter, &cs, &blob, &pieces, &outbuf,
                      &mags, &lmax, &symbols, &pcount, &poff, &symused};
     if (stream) cudaStreamSynchronize(stream);
@@ -190,9 +192,11 @@ static DwtPlan make_plan(const bwc_gl_ctrl &c, const Parameter &par) {
   return plan;
 }
 
-static void build_tables(const Parameter &par, bool compress, std::vector<CbDev> &cbs,
-                         std::vector<SbDev> &sbs, uint64_t *bytes_total, uint64_t *scratch_total,
-                         uint32_t *max_cols) {
+// Codeblock and subband tables of one parameter whose working buffer has the extents `dims`
+// (codeblocks address it from element 0, slope range slot 0).
+static void build_tables(const Parameter &par, const FieldDims &dims, uchar erres, bool compress,
+                         std::vector<CbDev> &cbs, std::vector<SbDev> &sbs, uint64_t *bytes_total,
+                         uint64_t *scratch_total, uint32_t *max_cols) {
   sbs.clear();
   for (const Subband &s : par.subbands) {
     SbDev d;
@@ -202,6 +206,8 @@ static void build_tables(const Parameter &par, bool compress, std::vector<CbDev>
     d.qt_eff = s.qt_eff;
     d.Kmax = s.Kmax;
     d.cls = sig_class(s.highband);
+    d.erres = erres ? 1u : 0u;
+    d.pad = 0;
     sbs.push_back(d);
   }
   cbs.clear();
@@ -218,6 +224,12 @@ static void build_tables(const Parameter &par, bool compress, std::vector<CbDev>
     d.d = (uint32_t)(cb.box.Z1 - cb.box.Z0);
     d.nt = (uint32_t)(cb.box.TS1 - cb.box.TS0);
     d.sb = cb.subband;
+    d.base = 0;
+    d.sy = dims.width;
+    d.sz = dims.width * dims.height;
+    d.st = dims.width * dims.height * dims.depth;
+    d.slot = 0;
+    d.pad = 0;
     const uint64_t nsamp = (uint64_t)d.w * d.h * d.d * d.nt;
     const uint32_t ncols = d.w * ((d.h + 3) / 4) * d.d * d.nt;
     mc = std::max(mc, ncols);
@@ -290,7 +302,7 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
   for (int p = 0; p < info.nPar; ++p) {
     uint64_t bt, st;
     uint32_t mc;
-    build_tables(tile.params[p], true, cbs[p], sbs[p], &bt, &st, &mc);
+    build_tables(tile.params[p], dims, c.error_resilience, true, cbs[p], sbs[p], &bt, &st, &mc);
     max_cols = std::max(max_cols, mc);
     cb_base[p + 1] = cb_base[p] + cbs[p].size();
     byte_base[p + 1] = byte_base[p] + bt;
@@ -382,9 +394,8 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
       o.sym_cap = dv->symbols.cap - 256;   // slack for the MQ kernel's read-ahead
       cudaMemsetAsync(dv->symused.p, 0, 8, s);
       cudaMemsetAsync(o.flags, 0, cbs[p].size() * 4, s);
-      launch_t1_encode(dv->work.as<bwc_float>(), dims, dv->cbtab.as<CbDev>() + cb_base[p],
-                       (uint32_t)cbs[p].size(), dv->sbtab.as<SbDev>(), c.error_resilience, o,
-                       max_cols, s);
+      launch_t1_encode(dv->work.as<bwc_float>(), dv->cbtab.as<CbDev>() + cb_base[p],
+                       (uint32_t)cbs[p].size(), dv->sbtab.as<SbDev>(), o, max_cols, s);
       unsigned long long used = 0;
       cudaMemcpyAsync(&used, dv->symused.p, 8, cudaMemcpyDeviceToHost, s);
       if (!cuda_ok(cudaStreamSynchronize(s), "tier-1 encoding")) return 0;
@@ -567,7 +578,7 @@ static uchar decompress_impl(bwc_codec *codec, bwc_stream *stream) {
     std::vector<SbDev> sbs;
     uint64_t bt, st;
     uint32_t mc;
-    build_tables(par, false, cbs, sbs, &bt, &st, &mc);
+    build_tables(par, dims, c.error_resilience, false, cbs, sbs, &bt, &st, &mc);
     const uint64_t ncb = cbs.size();
     std::vector<uint8_t> hK(ncb), hZ(ncb);
     std::vector<uint32_t> hLmax(ncb);
@@ -618,7 +629,7 @@ static uchar decompress_impl(bwc_codec *codec, bwc_stream *stream) {
     cudaEventRecord(a, s);
     cudaMemsetAsync(dv->temp.p, 0, n * sizeof(bwc_float), s);
     const int grid = t1_grid(nullptr, smem);
-    launch_t1_decode_ex(dv->temp.as<bwc_float>(), dims, dv->cbtab.as<CbDev>(), (uint32_t)ncb,
+    launch_t1_decode_ex(dv->temp.as<bwc_float>(), dv->cbtab.as<CbDev>(), (uint32_t)ncb,
                         dv->sbtab.as<SbDev>(), dv->bytes.as<uint8_t>(), dv->K.as<uint8_t>(),
                         dv->Z.as<uint8_t>(), dv->lmax.as<uint32_t>(), c.error_resilience,
                         dv->mags.as<bwc_raw>(), dv->flags.as<uint32_t>(), state_cap,
@@ -658,6 +669,376 @@ static uchar decompress_impl(bwc_codec *codec, bwc_stream *stream) {
   dv->timings[6] = dl;
   dv->timings[7] = up + t_norm + t_dwt + t_t1 + dl;
   dv->ddump_set = false;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Batched compression: many independently configured codecs in one pass over the device.
+//
+// Every field keeps its own codec (geometry, rates, decomposition, input dtype), so its
+// codestream is the one bwc_compress would write; only the execution changes:
+//   * each (field, parameter) unit gets its own region of a batch working buffer; fill,
+//     normalisation and the transform of the units run on several streams at once;
+//   * tier-1 codes the codeblocks of ALL fields in one launch of each kernel (per field, tier-1
+//     time is set by its longest codeblock, so separate calls would pay that chain per field);
+//   * tier-2 runs for the fields in parallel host threads;
+//   * one gather kernel assembles every codestream.
+// One batch runs at a time per device (the batch buffers are shared); the call is serialised.
+namespace {
+
+struct BatchState {
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> join;
+  cudaEvent_t ev[6] = {};
+  DevBuf in, work, temp, keys, stats, cbtab, sbtab, bytes, scratch, snaps, dmse, K, Z, L, S,
+      flags, slopes, pcount, poff, symbols, symused, blob, pieces, cs;
+  double timings[8] = {};
+};
+
+constexpr int kBatchStreams = 8;
+std::mutex g_batch_mutex;
+BatchState *g_batch[64] = {};
+
+BatchState *batch_state() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  if (!g_batch[dev]) {
+    BatchState *b = new (std::nothrow) BatchState();
+    if (!b) return nullptr;
+    b->device = dev;
+    if (!cuda_ok(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "stream")) {
+      delete b;
+      return nullptr;
+    }
+    b->side.resize(kBatchStreams);
+    b->join.resize(kBatchStreams + 1);
+    for (auto &x : b->side) cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking);
+    for (auto &e : b->join) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    for (auto &e : b->ev) cudaEventCreate(&e);
+    g_batch[dev] = b;
+  }
+  return g_batch[dev];
+}
+
+struct BatchUnit {
+  uint32_t field;
+  int param;
+  uint64_t n;          // values
+  uint64_t work_off;   // element offset in the batch working buffers
+  const uint8_t *src;  // device address of the unit's input values
+  bool src_double;
+  FieldDims dims;
+  DwtPlan plan;
+  uint8_t Qm;
+  uint64_t cb_first, cb_count;
+};
+
+}  // namespace
+
+static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *streams,
+                                 uint32_t nf, size_t *sizes) {
+  std::lock_guard<std::mutex> lock(g_batch_mutex);
+  BatchState *bs = batch_state();
+  if (!bs) return 1;
+  cudaStream_t s = bs->stream;
+  for (uint32_t i = 0; i < nf; ++i) {
+    sizes[i] = 0;
+    if (!codecs[i] || !streams[i] || !codecs[i]->tile || codecs[i]->tile->tiles.empty()) {
+      warn("o##########################################################o\n"
+           "| ERROR: bwc_create_compression has not been called        |\n"
+           "o##########################################################o\n");
+      return 1;
+    }
+  }
+  cudaEventRecord(bs->ev[0], s);
+  // ---- units, inputs, tables
+  std::vector<BatchUnit> units;
+  std::vector<uint64_t> in_off(nf, ~0ull), in_bytes(nf, 0);
+  uint64_t work_total = 0, in_total = 0;
+  for (uint32_t i = 0; i < nf; ++i) {
+    bwc_codec *codec = codecs[i];
+    const bwc_gl_inf &info = codec->info;
+    Tile &tile = codec->tile->tiles[0];
+    const uint64_t n = tile.box.size();
+    const size_t dsz = (info.data_prec == bwc_precision_double) ? 8 : 4;
+    in_bytes[i] = info.nX * info.nY * info.nZ * info.nTS * (uint64_t)info.nPar * dsz;
+    if (!is_device_pointer(streams[i]->inp)) {
+      in_off[i] = in_total;
+      in_total += (in_bytes[i] + 255) & ~255ull;
+    }
+    for (int p = 0; p < info.nPar; ++p) {
+      BatchUnit u{};
+      u.field = i;
+      u.param = p;
+      u.n = n;
+      u.work_off = work_total;
+      work_total += (n + 31) & ~31ull;
+      u.src_double = dsz == 8;
+      u.dims = FieldDims{tile.box.nx(), tile.box.ny(), tile.box.nz(), tile.box.nt()};
+      u.plan = make_plan(codec->control, tile.params[p]);
+      u.Qm = codec->control.Qm;
+      units.push_back(u);
+    }
+  }
+  std::vector<CbDev> allcb;
+  std::vector<SbDev> allsb;
+  uint64_t bytes_total = 0, scratch_total = 0, total_samples = 0;
+  uint32_t max_cols = 0;
+  for (BatchUnit &u : units) {
+    Tile &tile = codecs[u.field]->tile->tiles[0];
+    std::vector<CbDev> cbs;
+    std::vector<SbDev> sbs;
+    uint64_t bt, st;
+    uint32_t mc;
+    build_tables(tile.params[u.param], u.dims, codecs[u.field]->control.error_resilience, true,
+                 cbs, sbs, &bt, &st, &mc);
+    max_cols = std::max(max_cols, mc);
+    u.cb_first = allcb.size();
+    u.cb_count = cbs.size();
+    for (CbDev &d : cbs) {
+      d.base = u.work_off;
+      d.out_off += bytes_total;
+      d.scratch_off += scratch_total;
+      d.sb += (uint32_t)allsb.size();
+      d.slot = u.field;
+      total_samples += (uint64_t)d.w * ((d.h + 3) / 4) * 4 * d.d * d.nt;
+      allcb.push_back(d);
+    }
+    allsb.insert(allsb.end(), sbs.begin(), sbs.end());
+    bytes_total += bt;
+    scratch_total += st;
+  }
+  const uint64_t ncb = allcb.size(), nu = units.size();
+  if (t1_model_smem(max_cols) > 200 * 1024) {
+    warn("o##########################################################o\n"
+         "| ERROR: codeblocks above 2^18 samples are not supported   |\n"
+         "o##########################################################o\n");
+    return 1;
+  }
+  if (!bs->in.ensure(in_total) || !bs->work.ensure(work_total * sizeof(bwc_float)) ||
+      !bs->temp.ensure(work_total * sizeof(bwc_float)) || !bs->keys.ensure(16 * nu) ||
+      !bs->stats.ensure(4 * sizeof(bwc_float) * nu) || !bs->cbtab.ensure(sizeof(CbDev) * ncb) ||
+      !bs->sbtab.ensure(sizeof(SbDev) * allsb.size()) || !bs->bytes.ensure(bytes_total) ||
+      !bs->scratch.ensure(scratch_total) || !bs->snaps.ensure(ncb * kMaxPasses * 16) ||
+      !bs->dmse.ensure(ncb * kMaxPasses * 8) || !bs->K.ensure(ncb) || !bs->Z.ensure(ncb) ||
+      !bs->L.ensure(ncb * kMaxPasses * 4) || !bs->S.ensure(ncb * (kMaxPasses + 1) * 2) ||
+      !bs->flags.ensure(ncb * 4) || !bs->slopes.ensure(8 * nf) ||
+      !bs->pcount.ensure(ncb * kMaxPasses * 4) || !bs->poff.ensure(ncb * kMaxPasses * 8) ||
+      !bs->symused.ensure(8))
+    return 1;
+  for (uint32_t i = 0; i < nf; ++i)
+    if (in_off[i] != ~0ull)
+      cudaMemcpyAsync(bs->in.as<uint8_t>() + in_off[i], streams[i]->inp, in_bytes[i],
+                      cudaMemcpyHostToDevice, s);
+  for (BatchUnit &u : units) {
+    const bwc_codec *codec = codecs[u.field];
+    const size_t dsz = u.src_double ? 8 : 4;
+    const uint8_t *base = (in_off[u.field] != ~0ull) ? bs->in.as<uint8_t>() + in_off[u.field]
+                                                     : (const uint8_t *)streams[u.field]->inp;
+    u.src = base + (uint64_t)u.param * u.n * dsz;
+    (void)codec;
+  }
+  cudaMemcpyAsync(bs->cbtab.p, allcb.data(), sizeof(CbDev) * ncb, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(bs->sbtab.p, allsb.data(), sizeof(SbDev) * allsb.size(), cudaMemcpyHostToDevice,
+                  s);
+  {
+    std::vector<uint32_t> init(2 * nf);
+    for (uint32_t i = 0; i < nf; ++i) {
+      init[2 * i] = 0xFFFF;
+      init[2 * i + 1] = 0;
+    }
+    cudaMemcpyAsync(bs->slopes.p, init.data(), 8 * nf, cudaMemcpyHostToDevice, s);
+    std::vector<uint64_t> keys(2 * nu);
+    for (uint64_t u = 0; u < nu; ++u) {
+      keys[2 * u] = ~0ull;
+      keys[2 * u + 1] = 0;
+    }
+    cudaMemcpyAsync(bs->keys.p, keys.data(), 16 * nu, cudaMemcpyHostToDevice, s);
+    if (!cuda_ok(cudaStreamSynchronize(s), "batch set-up")) return 1;   // host vectors die here
+  }
+  cudaEventRecord(bs->ev[1], s);
+
+  // ---- fill, normalise and transform every unit, spread over the side streams
+  cudaEventRecord(bs->join[kBatchStreams], s);
+  for (int k = 0; k < kBatchStreams; ++k) cudaStreamWaitEvent(bs->side[k], bs->join[kBatchStreams], 0);
+  for (uint64_t ui = 0; ui < nu; ++ui) {
+    const BatchUnit &u = units[ui];
+    cudaStream_t ss = bs->side[ui % kBatchStreams];
+    bwc_float *temp = bs->temp.as<bwc_float>() + u.work_off;
+    bwc_float *work = bs->work.as<bwc_float>() + u.work_off;
+    launch_fill_minmax(u.src, u.src_double, u.n, temp, bs->keys.as<uint64_t>() + 2 * ui, ss);
+    launch_normalize(temp, u.n, bs->keys.as<uint64_t>() + 2 * ui, u.Qm,
+                     bs->stats.as<bwc_float>() + 4 * ui, ss);
+    launch_dwt_forward(work, temp, u.dims, u.plan, ss);
+  }
+  for (int k = 0; k < kBatchStreams; ++k) {
+    cudaEventRecord(bs->join[k], bs->side[k]);
+    cudaStreamWaitEvent(s, bs->join[k], 0);
+  }
+  cudaEventRecord(bs->ev[2], s);
+
+  // ---- tier-1 over all codeblocks (grown and repeated if the symbol arena was too small)
+  uint64_t arena = std::max<uint64_t>(1 << 20, total_samples * (kPrecBit + 1) * 9 / 8);
+  T1EncOut o;
+  o.bytes = bs->bytes.as<uint8_t>();
+  o.K = bs->K.as<uint8_t>();
+  o.Z = bs->Z.as<uint8_t>();
+  o.L = bs->L.as<uint32_t>();
+  o.S = bs->S.as<uint16_t>();
+  o.slopes = bs->slopes.as<uint32_t>();
+  o.flags = bs->flags.as<uint32_t>();
+  o.planes = bs->scratch.as<uint8_t>();
+  o.snaps = bs->snaps.as<uint64_t>();
+  o.dmse = bs->dmse.as<int64_t>();
+  o.pass_count = bs->pcount.as<uint32_t>();
+  o.pass_off = bs->poff.as<uint64_t>();
+  o.sym_used = bs->symused.as<unsigned long long>();
+  for (int attempt = 0;; ++attempt) {
+    if (!bs->symbols.ensure(arena + 256)) return 1;
+    o.symbols = bs->symbols.as<uint8_t>();
+    o.sym_cap = bs->symbols.cap - 256;
+    cudaMemsetAsync(bs->symused.p, 0, 8, s);
+    cudaMemsetAsync(bs->flags.p, 0, ncb * 4, s);
+    launch_t1_encode(bs->work.as<bwc_float>(), bs->cbtab.as<CbDev>(), (uint32_t)ncb,
+                     bs->sbtab.as<SbDev>(), o, max_cols, s);
+    unsigned long long used = 0;
+    cudaMemcpyAsync(&used, bs->symused.p, 8, cudaMemcpyDeviceToHost, s);
+    if (!cuda_ok(cudaStreamSynchronize(s), "batch tier-1 encoding")) return 1;
+    if (used <= o.sym_cap) break;
+    if (attempt >= 3) {
+      warn("o##########################################################o\n"
+           "| ERROR: tier-1 symbol arena exhausted                     |\n"
+           "o##########################################################o\n");
+      return 1;
+    }
+    arena = used + (used >> 3) + (1 << 20);
+  }
+  cudaEventRecord(bs->ev[3], s);
+  std::vector<uint8_t> hK(ncb), hZ(ncb);
+  std::vector<uint32_t> hL(ncb * kMaxPasses), hflags(ncb), hslopes(2 * nf);
+  std::vector<uint16_t> hS(ncb * (kMaxPasses + 1));
+  std::vector<bwc_float> hstats(4 * nu);
+  cudaMemcpyAsync(hK.data(), bs->K.p, ncb, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hZ.data(), bs->Z.p, ncb, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hL.data(), bs->L.p, ncb * kMaxPasses * 4, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hS.data(), bs->S.p, ncb * (kMaxPasses + 1) * 2, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hflags.data(), bs->flags.p, ncb * 4, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hslopes.data(), bs->slopes.p, 8 * nf, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hstats.data(), bs->stats.p, 4 * sizeof(bwc_float) * nu, cudaMemcpyDeviceToHost,
+                  s);
+  if (!cuda_ok(cudaStreamSynchronize(s), "batch tier-1 download")) return 1;
+  for (uint64_t c = 0; c < ncb; ++c)
+    if (hflags[c] & 1u) {
+      warn("o##########################################################o\n"
+           "| ERROR: tier-1 output exceeded its codeblock buffer       |\n"
+           "o##########################################################o\n");
+      return 1;
+    }
+  const auto h0 = std::chrono::steady_clock::now();
+
+  // ---- tier-2 and layout per field, in parallel host threads
+  std::vector<std::vector<uint8_t>> blobs(nf);
+  std::vector<std::vector<GatherPiece>> fpieces(nf);
+  std::vector<uint64_t> totals(nf, 0);
+  std::vector<uint64_t> first_unit(nf + 1, 0);
+  for (uint64_t ui = 0; ui < nu; ++ui) first_unit[units[ui].field + 1] = ui + 1;
+  for (uint32_t i = 0; i < nf; ++i) first_unit[i + 1] = std::max(first_unit[i + 1], first_unit[i]);
+  std::atomic<uint32_t> next{0};
+  std::atomic<int> failed{0};
+  auto worker = [&]() {
+    for (;;) {
+      const uint32_t i = next.fetch_add(1);
+      if (i >= nf) return;
+      bwc_codec *codec = codecs[i];
+      Tile &tile = codec->tile->tiles[0];
+      for (uint64_t ui = first_unit[i]; ui < first_unit[i + 1]; ++ui) {
+        const BatchUnit &u = units[ui];
+        Parameter &par = tile.params[u.param];
+        par.pmin = hstats[4 * ui + 0];
+        par.pmax = hstats[4 * ui + 1];
+        par.alpha = hstats[4 * ui + 2];
+        par.beta = hstats[4 * ui + 3];
+        for (uint64_t j = 0; j < u.cb_count; ++j) {
+          const uint64_t g = u.cb_first + j;
+          Codeblock &cb = par.codeblocks[j];
+          CodedBlock &e = cb.enc;
+          e.K = hK[g];
+          e.Z = hZ[g];
+          e.Kmsbs = e.K ? (uint8_t)(par.subbands[cb.subband].Kmax - e.K) : 0;
+          for (int z = 0; z < e.Z; ++z) e.L[z] = hL[g * kMaxPasses + z];
+          for (int z = 0; z <= e.Z; ++z) e.S[z] = hS[g * (kMaxPasses + 1) + z];
+          cb.data_off = allcb[g].out_off;
+          cb.data_cap = allcb[g].out_cap;
+        }
+      }
+      tile.slope_min = (uint16_t)hslopes[2 * i];
+      tile.slope_max = (uint16_t)hslopes[2 * i + 1];
+      if (t2_encode(codec, tile)) {
+        failed = 1;
+        continue;
+      }
+      totals[i] = layout_codestream(codec, streams[i], blobs[i], fpieces[i]);
+      if (!totals[i]) failed = 1;
+    }
+  };
+  {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned nt = std::min<unsigned>(hw, nf);
+    std::vector<std::thread> pool;
+    for (unsigned t = 1; t < nt; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto &t : pool) t.join();
+  }
+  if (failed) return 1;
+  const auto h1 = std::chrono::steady_clock::now();
+
+  // ---- one gather for every codestream, then each to its stream->out
+  std::vector<uint8_t> blob;
+  std::vector<GatherPiece> pieces;
+  std::vector<uint64_t> cs_off(nf);
+  uint64_t cs_total = 0;
+  for (uint32_t i = 0; i < nf; ++i) {
+    const uint64_t boff = blob.size();
+    blob.insert(blob.end(), blobs[i].begin(), blobs[i].end());
+    cs_off[i] = cs_total;
+    for (GatherPiece pc : fpieces[i]) {
+      if (pc.from_blob) pc.src += boff;
+      pc.dst += cs_off[i];
+      pieces.push_back(pc);
+    }
+    cs_total += (totals[i] + 255) & ~255ull;
+  }
+  cudaEventRecord(bs->ev[4], s);
+  if (!bs->blob.ensure(blob.size()) || !bs->pieces.ensure(pieces.size() * sizeof(GatherPiece)) ||
+      !bs->cs.ensure(cs_total))
+    return 1;
+  cudaMemcpyAsync(bs->blob.p, blob.data(), blob.size(), cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(bs->pieces.p, pieces.data(), pieces.size() * sizeof(GatherPiece),
+                  cudaMemcpyHostToDevice, s);
+  launch_gather(bs->cs.as<uint8_t>(), bs->blob.as<uint8_t>(), bs->bytes.as<uint8_t>(),
+                bs->pieces.as<GatherPiece>(), pieces.size(), s);
+  for (uint32_t i = 0; i < nf; ++i) {
+    const bool out_dev = is_device_pointer(streams[i]->out);
+    cudaMemcpyAsync(streams[i]->out, bs->cs.as<uint8_t>() + cs_off[i], totals[i],
+                    out_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s);
+  }
+  cudaEventRecord(bs->ev[5], s);
+  if (!cuda_ok(cudaStreamSynchronize(s), "batch codestream assembly")) return 1;
+  float t[5] = {0, 0, 0, 0, 0};
+  cudaEventElapsedTime(&t[0], bs->ev[0], bs->ev[1]);
+  cudaEventElapsedTime(&t[1], bs->ev[1], bs->ev[2]);
+  cudaEventElapsedTime(&t[2], bs->ev[2], bs->ev[3]);
+  cudaEventElapsedTime(&t[3], bs->ev[4], bs->ev[5]);
+  bs->timings[0] = t[0];   // set-up and uploads
+  bs->timings[1] = t[1];   // fill, normalise, transform
+  bs->timings[2] = t[2];   // tier-1
+  bs->timings[3] = std::chrono::duration<double, std::milli>(h1 - h0).count();   // tier-2
+  bs->timings[4] = t[3];   // gather and outputs
+  cudaEventElapsedTime(&t[4], bs->ev[0], bs->ev[5]);
+  bs->timings[5] = t[4];   // whole call
+  for (uint32_t i = 0; i < nf; ++i) sizes[i] = totals[i];
   return 0;
 }
 
@@ -705,5 +1086,20 @@ extern "C" int bwc_b200_last_timings(bwc_codec *const codec, double *out_ms, int
   if (!codec || !codec->tile || !codec->tile->dev) return 0;
   const int k = std::min(n, 9);
   for (int i = 0; i < k; ++i) out_ms[i] = codec->tile->dev->timings[i];
+  return k;
+}
+
+extern "C" uchar bwc_b200_compress_batch(bwc_codec *const *codecs, bwc_stream *const *streams,
+                                         uint32 n, size_t *sizes) {
+  if (!codecs || !streams || !sizes || n == 0) return 1;
+  return compress_batch_impl(codecs, streams, n, sizes);
+}
+
+extern "C" int bwc_b200_last_batch_timings(double *out_ms, int n) {
+  std::lock_guard<std::mutex> lock(g_batch_mutex);
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || !g_batch[dev]) return 0;
+  const int k = std::min(n, 6);
+  for (int i = 0; i < k; ++i) out_ms[i] = g_batch[dev]->timings[i];
   return k;
 }

@@ -18,6 +18,10 @@ struct CbDev {
                              // decompress: element offset of its magnitudes
   uint32_t out_cap;          // compress: capacity of the coded-byte region
   uint32_t sb;               // index into the SbDev table
+  uint64_t base;             // element offset of the codeblock's field in the working buffer
+  uint64_t sy, sz, st;       // that field's strides along y, z and t (elements)
+  uint32_t slot;             // which slope-range pair (min, max) the codeblock updates
+  uint32_t pad;
 };
 
 // One subband.
@@ -26,6 +30,8 @@ struct SbDev {
   bwc_float qt_eff;    // qt_effective_step_size
   uint32_t Kmax;
   uint32_t cls;        // significance-context class: 0 low-pass, 1 high-pass, 2 diagonal
+  uint32_t erres;      // error resilience of the field (segmentation symbols after each plane)
+  uint32_t pad;
 };
 
 // Outputs and scratch of the tier-1 encoder.
@@ -35,7 +41,8 @@ struct T1EncOut {
   uint8_t *Z;            // [ncb]
   uint32_t *L;           // [ncb * kMaxPasses] truncation lengths
   uint16_t *S;           // [ncb * (kMaxPasses + 1)] log slopes
-  uint32_t *slopes;      // [2]: min over non-zero slopes, max (atomics; init 0xFFFF / 0)
+  uint32_t *slopes;      // [2 * slots]: per slot min over non-zero slopes, max (atomics;
+                         //   init 0xFFFF / 0); CbDev::slot selects the pair
   uint32_t *flags;       // [ncb]: 1 coded-byte overflow, 2 hull stack underflow,
                          //        4 unsettled truncation scan, 8 symbol arena full
   uint8_t *planes;       // scratch: bit planes, CbDev::scratch_off
@@ -78,13 +85,13 @@ void launch_dwt_inverse(bwc_float *work, bwc_float *temp, const FieldDims &dims,
 // t1_encode.cu: context modelling (one CTA per codeblock, max_cols = largest number of stripe
 // columns of a codeblock) followed by MQ coding (one thread per codeblock).
 size_t t1_model_smem(uint32_t max_cols);
-void launch_t1_encode(const bwc_float *work, const FieldDims &dims, const CbDev *cbs,
-                      uint32_t ncb, const SbDev *sbs, uchar erres, const T1EncOut &out,
-                      uint32_t max_cols, cudaStream_t s);
+// Each codeblock addresses its samples as work[base + x + y*sy + z*sz + t*st].
+void launch_t1_encode(const bwc_float *work, const CbDev *cbs, uint32_t ncb, const SbDev *sbs,
+                      const T1EncOut &out, uint32_t max_cols, cudaStream_t s);
 
 // t1_decode.cu: decodes Z[c] passes of codeblock c from data + out_off (Lmax[c] bytes) and
 // writes the dequantised samples into the (zeroed) working buffer.
-void launch_t1_decode_ex(bwc_float *work, const FieldDims &dims, const CbDev *cbs, uint32_t ncb,
+void launch_t1_decode_ex(bwc_float *work, const CbDev *cbs, uint32_t ncb,
                          const SbDev *sbs, const uint8_t *data, const uint8_t *K,
                          const uint8_t *Z, const uint32_t *Lmax, uchar erres, bwc_raw *mags,
                          uint32_t *flags, uint32_t state_cap, uint16_t *gstate,

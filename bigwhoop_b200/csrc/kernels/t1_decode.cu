@@ -257,7 +257,7 @@ __device__ void dec_cu(MqDec &d, uint8_t *ctx, uint16_t *state, bwc_raw *mag, co
 }
 
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
-    t1_decode_kernel(bwc_float *__restrict__ work, FieldDims dims, const CbDev *__restrict__ cbs,
+    t1_decode_kernel(bwc_float *__restrict__ work, const CbDev *__restrict__ cbs,
                      uint32_t ncb, const SbDev *__restrict__ sbs, const uint8_t *__restrict__ data,
                      const uint8_t *__restrict__ Kin, const uint8_t *__restrict__ Zin,
                      const uint32_t *__restrict__ Lmax, uint32_t erres, bwc_raw *mags,
@@ -345,8 +345,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     __syncwarp();
     const int bitplane = s_bitplane[wib], cpass = s_pass[wib];
     // ---- dequantise into the working buffer ---------------------------------------------------
-    const uint64_t sy = dims.width, sz = dims.width * dims.height,
-                   st_ = dims.width * dims.height * dims.depth;
+    const uint64_t sy = cb.sy, sz = cb.sz, st_ = cb.st;
     for (uint32_t q = lane; q < g.ncols * 4; q += 32) {
       const uint32_t col = q >> 2, row = q & 3;
       const bwc_raw m = mag[q];
@@ -364,7 +363,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
       f = dev::fadd(f, (bwc_float)off);
       f = dev::fmul(f, sb.qt_eff);
       bwc_raw r = dev::as_raw(f) | (xib ? kSignMask : (bwc_raw)0);
-      work[(cb.x0 + x) + (uint64_t)(cb.y0 + y) * sy + (uint64_t)(cb.z0 + z) * sz +
+      work[cb.base + (cb.x0 + x) + (uint64_t)(cb.y0 + y) * sy + (uint64_t)(cb.z0 + z) * sz +
            (uint64_t)(cb.t0 + t) * st_] = dev::as_float(r);
     }
     __syncwarp();
@@ -373,14 +372,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 
 }  // namespace
 
-void launch_t1_decode_ex(bwc_float *work, const FieldDims &dims, const CbDev *cbs, uint32_t ncb,
+void launch_t1_decode_ex(bwc_float *work, const CbDev *cbs, uint32_t ncb,
                          const SbDev *sbs, const uint8_t *data, const uint8_t *K,
                          const uint8_t *Z, const uint32_t *Lmax, uchar erres, bwc_raw *mags,
                          uint32_t *flags, uint32_t state_cap, uint16_t *gstate,
                          uint32_t *work_counter, int grid, cudaStream_t s) {
   const size_t smem = 32 * kWarpsPerBlock + (size_t)state_cap * sizeof(uint16_t) * kWarpsPerBlock;
   cudaFuncSetAttribute(t1_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  t1_decode_kernel<<<grid, kWarpsPerBlock * 32, smem, s>>>(work, dims, cbs, ncb, sbs, data, K, Z,
+  t1_decode_kernel<<<grid, kWarpsPerBlock * 32, smem, s>>>(work, cbs, ncb, sbs, data, K, Z,
                                                             Lmax, erres, mags, flags, state_cap,
                                                             gstate, work_counter);
 }

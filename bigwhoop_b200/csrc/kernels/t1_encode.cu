@@ -334,9 +334,9 @@ __device__ __forceinline__ int64_t block_sum64(int64_t v, int64_t *wsum) {
 // ---- kernel 1: quantisation + context modelling ------------------------------------------------
 
 __global__ void __launch_bounds__(kModelThreads)
-    t1_model_kernel(const bwc_float *__restrict__ work, FieldDims dims,
+    t1_model_kernel(const bwc_float *__restrict__ work,
                     const CbDev *__restrict__ cbs, uint32_t ncb, const SbDev *__restrict__ sbs,
-                    uint32_t erres, T1EncOut out) {
+                    T1EncOut out) {
   extern __shared__ uint8_t smem[];
   __shared__ uint32_t s_wsum[kModelThreads / 32];
   __shared__ int64_t s_wsum64[kModelThreads / 32];
@@ -352,15 +352,14 @@ __global__ void __launch_bounds__(kModelThreads)
   uint8_t *planes = out.planes + cb.scratch_off;
 
   // ---- quantise -------------------------------------------------------------------------------
-  const uint64_t sy = dims.width, sz = dims.width * dims.height,
-                 st_ = dims.width * dims.height * dims.depth;
+  const uint64_t sy = cb.sy, sz = cb.sz, st_ = cb.st;
   auto sample = [&](uint32_t col, int row, bool *valid) -> uint64_t {
     const uint32_t x = col % g.W, sr = col / g.W;
     const uint32_t j = sr % g.nstripes, sl = sr / g.nstripes;
     const uint32_t y = 4 * j + row;
     *valid = y < g.H;
     const uint32_t z = sl % cb.d, t = sl / cb.d;
-    return (uint64_t)(cb.x0 + x) + (uint64_t)(cb.y0 + y) * sy + (uint64_t)(cb.z0 + z) * sz +
+    return cb.base + (uint64_t)(cb.x0 + x) + (uint64_t)(cb.y0 + y) * sy + (uint64_t)(cb.z0 + z) * sz +
            (uint64_t)(cb.t0 + t) * st_;
   };
   auto quant = [&](uint64_t idx, uint32_t *sign) -> bwc_raw {
@@ -547,7 +546,7 @@ __global__ void __launch_bounds__(kModelThreads)
           cu_symbols<CountSink, false>(lo[col] & 0xF, lo[col] >> 4, hi[col] & 0xF, plane[col], n,
                                        lmin, full, sb.cls, cnt, nullptr, planes, g.ncols, col, b);
         }
-        const uint32_t extra = (erres && tid == kModelThreads - 1) ? 4u : 0u;
+        const uint32_t extra = (sb.erres && tid == kModelThreads - 1) ? 4u : 0u;
         uint32_t total;
         const uint32_t off = block_exclusive_scan(cnt.n + extra, &total, s_wsum);
         uint8_t *chunk = reserve(total);
@@ -899,8 +898,8 @@ __global__ void __launch_bounds__(kMqThreads) t1_mq_kernel(const CbDev *__restri
     }
   }
   if (Lout[Z - 1] > 0) {
-    atomicMin(&out.slopes[0], smin);
-    atomicMax(&out.slopes[1], smax);
+    atomicMin(&out.slopes[2 * cb.slot], smin);
+    atomicMax(&out.slopes[2 * cb.slot + 1], smax);
   }
   out.flags[c] |= bo.flags;
 }
@@ -921,13 +920,12 @@ uint32_t mq_lanes_per_warp(uint32_t ncb) {
   return lanes;
 }
 
-void launch_t1_encode(const bwc_float *work, const FieldDims &dims, const CbDev *cbs, uint32_t ncb,
-                      const SbDev *sbs, uchar erres, const T1EncOut &out, uint32_t max_cols,
-                      cudaStream_t s) {
+void launch_t1_encode(const bwc_float *work, const CbDev *cbs, uint32_t ncb, const SbDev *sbs,
+                      const T1EncOut &out, uint32_t max_cols, cudaStream_t s) {
   if (!ncb) return;
   const size_t smem = t1_model_smem(max_cols);
   cudaFuncSetAttribute(t1_model_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  t1_model_kernel<<<ncb, kModelThreads, smem, s>>>(work, dims, cbs, ncb, sbs, erres, out);
+  t1_model_kernel<<<ncb, kModelThreads, smem, s>>>(work, cbs, ncb, sbs, out);
   const uint32_t lanes = mq_lanes_per_warp(ncb);
   t1_mq_kernel<<<(ncb + lanes - 1) / lanes, kMqThreads, 0, s>>>(cbs, ncb, sbs, out, lanes);
 }

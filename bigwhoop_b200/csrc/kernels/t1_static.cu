@@ -121,12 +121,18 @@ extern "C" int bwc_b200_t1_encode_codeblock_static(
   cb.scratch_off = 0;
   cb.out_cap = bytes_cap;
   cb.sb = 0;
+  cb.base = 0;
+  cb.sy = nX;
+  cb.sz = nX * nY;
+  cb.st = nX * nY * nZ;
+  cb.slot = 0;
   SbDev sb{};
   sb.gain_step2 = gain_step2;
   sb.qt_eff = qt_eff;
   sb.Kmax = 0;
   // significance-context class from the subband's high-pass axes (tier1.c:2416-2446)
   sb.cls = ((highband & 3) == 1) ? 1u : ((highband & 3) == 3) ? 2u : 0u;
+  sb.erres = erres ? 1u : 0u;
   const uint32_t slopes_init[2] = {0xFFFF, 0};
 
   // The static area keeps the previous call's contents: the symbol counter, the slope range
@@ -154,9 +160,8 @@ extern "C" int bwc_b200_t1_encode_codeblock_static(
   o.sym_used = reinterpret_cast<unsigned long long *>(base + kOffUsed);
   o.pass_count = reinterpret_cast<uint32_t *>(base + kOffPcount);
   o.pass_off = reinterpret_cast<uint64_t *>(base + kOffPoff);
-  FieldDims fd{nX, nY, nZ, nTS};
-  launch_t1_encode(coeffs, fd, reinterpret_cast<const CbDev *>(base + kOffCb), 1,
-                   reinterpret_cast<const SbDev *>(base + kOffSb), erres, o, (uint32_t)ncols, s);
+  launch_t1_encode(coeffs, reinterpret_cast<const CbDev *>(base + kOffCb), 1,
+                   reinterpret_cast<const SbDev *>(base + kOffSb), o, (uint32_t)ncols, s);
   cudaMemcpyAsync(status, base + kOffFlags, 4, cudaMemcpyDeviceToDevice, s);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {

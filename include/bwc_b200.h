@@ -96,6 +96,21 @@ size_t bwc_b200_assemble_from_tier1(bwc_codec *const codec, bwc_stream *const st
  * download, [7] total.  Returns the number of entries written (at most n). */
 int    bwc_b200_last_timings(bwc_codec *const codec, double *out_ms, int n);
 
+/* Batched compression of n independently configured codecs (each set up with
+ * bwc_create_compression as for bwc_compress, with its own stream).  No counterpart in the
+ * reference API.  Every codestream is byte-identical to what bwc_compress would produce for that
+ * codec; sizes[i] receives its length (0 on failure).  The fields' transforms run concurrently,
+ * tier-1 codes all their codeblocks in one pass, tier-2 runs in parallel host threads and one
+ * device gather assembles every codestream.  Returns 0 on success, 1 on failure.  One batch runs
+ * at a time per device (calls are serialised). */
+uchar  bwc_b200_compress_batch(bwc_codec *const *codecs, bwc_stream *const *streams, uint32 n,
+                               size_t *sizes);
+
+/* Stage times (ms) of the last batch on the current device: [0] set-up and uploads,
+ * [1] fill/normalise/transform, [2] tier-1, [3] tier-2 (host), [4] gather and outputs,
+ * [5] whole call.  Returns the number of entries written (at most n). */
+int    bwc_b200_last_batch_timings(double *out_ms, int n);
+
 /* Tier-1 encoding of ONE codeblock without any memory allocation.  No counterpart in the
  * reference API.
  *
