@@ -920,6 +920,9 @@ uint32_t mq_lanes_per_warp(uint32_t ncb) {
   return lanes;
 }
 
+// Context modelling, then MQ coding, on `s`.  (Running the modelling of later codeblocks
+// concurrently with the MQ coding of earlier ones was measured slower: the issue-bound modelling
+// warps lengthen the latency-bound MQ chains, and the longest chain sets the time.)
 void launch_t1_encode(const bwc_float *work, const CbDev *cbs, uint32_t ncb, const SbDev *sbs,
                       const T1EncOut &out, uint32_t max_cols, cudaStream_t s) {
   if (!ncb) return;
