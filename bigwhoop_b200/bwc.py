@@ -157,6 +157,13 @@ def load(precision="double"):
                                                       C.c_uint16, C.c_uint16]),
         "bwc_b200_compress_batch": (C.c_uint8, [vp, vp, C.c_uint32, vp]),
         "bwc_b200_last_batch_timings": (C.c_int, [vp, C.c_int]),
+        "bwc_b200_set_rate_model": (C.c_int, [vp]),
+        "bwc_b200_rate_features": (C.c_int, [cp, u8, vp]),
+        "bwc_b200_rate_stats": (C.c_int, [cp, u8, vp]),
+        "bwc_b200_mlp_forward": (C.c_int, [vp, vp, C.c_uint32, vp]),
+        "bwc_b200_mlp_gradient": (C.c_int, [vp, vp, vp, C.c_uint32, vp, vp]),
+        "bwc_b200_mlp_train": (C.c_int, [vp, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32,
+                                         C.c_float, u64, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -36,6 +36,8 @@ constexpr bwc_raw kExponentMask = 0x7FF0000000000000ull;
 constexpr bwc_float kFltMax = 1.7976931348623157e+308;
 #endif
 constexpr int kMaxPasses = MAXIMUM_NO_PASSES;
+constexpr int kRateFeatures = 34;   // inputs of the rate-control warm start (tier2.cpp)
+constexpr int kRateStats = 6;
 
 // dimension flags of a subband's high-pass axes (macros.h:66-70)
 constexpr uint8_t kDimX = 1, kDimY = 2, kDimZ = 4, kDimTS = 8;
@@ -159,6 +161,9 @@ struct Tile {
   uint16_t slope_min = 0xFFFF, slope_max = 0;
   std::vector<Parameter> params;
   std::vector<Packet *> sequence;
+  // rate control of the last compression, per quality layer
+  std::vector<float> rc_features;   // kRateFeatures per layer (the warm start's inputs)
+  std::vector<double> rc_stats;     // kRateStats per layer, see tier2.cpp
 };
 
 struct DeviceState;   // CUDA resources (api.cpp)

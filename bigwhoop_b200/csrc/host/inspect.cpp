@@ -87,3 +87,20 @@ extern "C" size_t bwc_b200_assemble_from_tier1(bwc_codec *const codec, bwc_strea
     std::memcpy(out + pc.dst, (pc.from_blob ? blob.data() : bytes) + pc.src, pc.size);
   return total;
 }
+
+extern "C" int bwc_b200_rate_features(bwc_codec *const codec, uint8 const layer, float *out) {
+  if (!codec || !codec->tile || codec->tile->tiles.empty() || !out) return 1;
+  const Tile &tile = codec->tile->tiles[0];
+  if ((size_t)(layer + 1) * kRateFeatures > tile.rc_features.size()) return 1;
+  std::memcpy(out, tile.rc_features.data() + (size_t)layer * kRateFeatures,
+              kRateFeatures * sizeof(float));
+  return 0;
+}
+
+extern "C" int bwc_b200_rate_stats(bwc_codec *const codec, uint8 const layer, double *out) {
+  if (!codec || !codec->tile || codec->tile->tiles.empty() || !out) return 1;
+  const Tile &tile = codec->tile->tiles[0];
+  if ((size_t)(layer + 1) * kRateStats > tile.rc_stats.size()) return 1;
+  std::memcpy(out, tile.rc_stats.data() + (size_t)layer * kRateStats, kRateStats * sizeof(double));
+  return 0;
+}

@@ -6,11 +6,15 @@
 // (tier2.c:896-1079, :434-711).  The probe results feed a trajectory-dependent search (exact
 // exits on equality, the `tmp` fallback), so the same arithmetic -- including its quirks, such
 // as adding L[0] for a codeblock whose previous layer stopped after one pass -- is kept here.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <thread>
+#include <vector>
 
 #include "common.hpp"
+#include "../kernels/kernels.hpp"
 
 namespace bwcb {
 
@@ -386,6 +390,76 @@ int64_t probe_layer(const Probe &pr, uint16_t threshold) {
 
 }  // namespace
 
+// ---- rate-control warm start ---------------------------------------------------------------
+// The reference's per-layer bisection (tier2.c:1115-1254) is a chain of dependent probes, each
+// a full truncation-and-header estimate.  Its outcome depends on the exact sequence of probes,
+// so the search itself is kept: the same probes, compared the same way, in the same order.
+// What a predicted final threshold changes is WHEN the probes are evaluated: from the
+// prediction the whole probe path is simulated (assuming the size falls as the threshold
+// rises) and evaluated at once, in parallel host threads; the exact bisection then replays over
+// those results, and only when its path leaves the predicted one is a new round needed (again
+// speculated from the prediction).  The selected slope, and so every output byte, is the
+// plain search's; what the prediction saves is rounds of dependent probes.
+//
+// Features of one layer (kRateFeatures values): a 32-bin histogram (fractions) of the
+// codeblocks' non-zero pass slopes S[1..Z] over the 16-bit log range, log(bits per value of the
+// layer) / 4 and (log(values) - 14) / 4.  The network predicts the final slope / 65536.
+
+namespace {
+
+void rate_features(const Tile &tile, float bpv, float *out) {
+  double hist[32] = {};
+  double total = 0;
+  for (const Parameter &par : tile.params)
+    for (const Codeblock &cb : par.codeblocks)
+      for (int z = 1; z <= cb.enc.Z; ++z)
+        if (cb.enc.S[z]) {
+          hist[cb.enc.S[z] >> 11] += 1;
+          total += 1;
+        }
+  for (int i = 0; i < 32; ++i) out[i] = total > 0 ? (float)(hist[i] / total) : 0.f;
+  uint64_t values = tile.box.size() * tile.params.size();
+  out[32] = (float)(std::log((double)std::max(bpv, 1e-6f)) / 4.0);
+  out[33] = (float)((std::log((double)std::max<uint64_t>(values, 1)) - 14.0) / 4.0);
+}
+
+// One bisection step of tier2.c:1115-1254; returns true when the search is over.
+struct Search {
+  uint16_t smin, smax, tmp, slope;
+  int64_t est;
+  bool done() const { return smin >= smax; }
+  uint16_t next() const { return (uint16_t)((smax + smin) >> 1); }
+  void step(uint16_t s, int64_t e, int64_t target) {
+    slope = s;
+    est = e;
+    if (e > target) {
+      if (smin == s) smax = s;
+      smin = s;
+    } else if (e < target) {
+      if (smax == s) smin = s;
+      smax = s;
+      tmp = s;
+    } else {
+      smax = s;
+      smin = s;
+    }
+  }
+};
+
+// the probe slopes the search would take if its estimate exceeded the target exactly below
+// `pred` (the predicted final slope)
+std::vector<uint16_t> predicted_path(Search st, uint16_t pred, int64_t target) {
+  std::vector<uint16_t> out;
+  while (!st.done() && out.size() < 64) {
+    const uint16_t s = st.next();
+    out.push_back(s);
+    st.step(s, (s < pred) ? target + 1 : target - 1, target);
+  }
+  return out;
+}
+
+}  // namespace
+
 // create_quality_layers (tier2.c:1115-1254)
 static uchar create_quality_layers(bwc_codec *codec, Tile &tile) {
   const bwc_gl_ctrl &c = codec->control;
@@ -398,45 +472,88 @@ static uchar create_quality_layers(bwc_codec *codec, Tile &tile) {
   static const bool check = getenv("BWC_B200_CHECK_PROBES") != nullptr;
   Probe probe;
   build_records(tile, probe);
+  // features and, when a model is set, the predicted final slope of every layer
+  tile.rc_features.assign((size_t)c.nLayers * kRateFeatures, 0.f);
+  tile.rc_stats.assign((size_t)c.nLayers * kRateStats, 0.0);
+  for (uint8_t l = 0; l < c.nLayers; ++l)
+    rate_features(tile, c.bitrate[l], tile.rc_features.data() + (size_t)l * kRateFeatures);
+  std::vector<float> pred(c.nLayers, -1.f);
+  const bool have_pred =
+      !check && c.nLayers <= 64 && mlp_predict(tile.rc_features.data(), c.nLayers, pred.data());
+  uint64_t ncb_total = 0;
+  for (const Parameter &par : tile.params) ncb_total += par.codeblocks.size();
+  const bool parallel = have_pred && ncb_total >= 256;
   for (uint8_t l = 0; l < c.nLayers; ++l) {
     uint16_t slope;
+    int probes = 0, rounds = 0;
+    uint16_t pslope = 0;
     target = (int64_t)ceilf(c.bitrate[l] * (float)tile_size / 8.0f);
     if ((float)target > 0.0f) {
-      uint16_t smin = tile.slope_min, smax = tile.slope_max;
-      uint16_t tmp = smin;
-      slope = smin;
+      Search st{tile.slope_min, tile.slope_max, tile.slope_min, tile.slope_min, 0};
       build_layer(tile, l, probe);
-      while (smin < smax) {
-        slope = (uint16_t)((smax + smin) >> 1);
-        est = probe_layer(probe, slope);
+      if (have_pred) {
+        const double p = std::min(std::max((double)pred[l], 0.0), 1.0) * 65536.0;
+        pslope = (uint16_t)std::min(65535.0, std::floor(p));
+      }
+      std::vector<std::pair<uint16_t, int64_t>> known;   // evaluated probes of this layer
+      auto lookup = [&](uint16_t s, int64_t *e) {
+        for (auto &kv : known)
+          if (kv.first == s) {
+            *e = kv.second;
+            return true;
+          }
+        return false;
+      };
+      while (!st.done()) {
+        const uint16_t s = st.next();
+        int64_t e;
+        if (!lookup(s, &e)) {
+          // a new round: this probe, plus the rest of the predicted path
+          std::vector<uint16_t> todo{s};
+          if (have_pred) {
+            todo = predicted_path(st, pslope, target - est_tile - (int64_t)header_size);
+            if (todo.empty() || todo[0] != s) todo.insert(todo.begin(), s);
+          }
+          std::vector<int64_t> res(todo.size());
+          if (parallel && todo.size() > 1) {
+            std::vector<std::thread> th;
+            for (size_t k = 1; k < todo.size(); ++k)
+              th.emplace_back([&, k]() { res[k] = probe_layer(probe, todo[k]); });
+            res[0] = probe_layer(probe, todo[0]);
+            for (auto &t : th) t.join();
+          } else {
+            for (size_t k = 0; k < todo.size(); ++k) res[k] = probe_layer(probe, todo[k]);
+          }
+          for (size_t k = 0; k < todo.size(); ++k) known.emplace_back(todo[k], res[k]);
+          ++rounds;
+          e = res[0];
+        }
         if (check) {
-          const int64_t slow = create_quality_layer(codec, tile, slope, l, 1);
-          if (slow != est) {
+          const int64_t slow = create_quality_layer(codec, tile, s, l, 1);
+          if (slow != e) {
             fprintf(stderr, "bwc: rate-control probe mismatch (layer %d, slope %u: %lld vs %lld)\n",
-                    l, slope, (long long)est, (long long)slow);
+                    l, s, (long long)e, (long long)slow);
             return 1;
           }
         }
-        if (est >= 0)
-          est += est_tile + (int64_t)header_size;
-        else
-          return 1;
-        if (est > target) {
-          if (smin == slope) smax = slope;
-          smin = slope;
-        } else if (est < target) {
-          if (smax == slope) smin = slope;
-          smax = slope;
-          tmp = slope;
-        } else {
-          smax = slope;
-          smin = slope;
-        }
+        if (e < 0) return 1;
+        ++probes;
+        st.step(s, e + est_tile + (int64_t)header_size, target);
       }
-      if (est > target) slope = std::max(tmp, tile.slope_min);
+      slope = st.slope;
+      est = st.est;
+      if (probes == 0) slope = tile.slope_min;
+      if (est > target && probes > 0) slope = std::max(st.tmp, tile.slope_min);
     } else {
       slope = 0;
     }
+    double *rs = tile.rc_stats.data() + (size_t)l * kRateStats;
+    rs[0] = slope;
+    rs[1] = probes;
+    rs[2] = rounds;
+    rs[3] = have_pred ? (double)pslope : -1.0;
+    rs[4] = tile.slope_min;
+    rs[5] = tile.slope_max;
     est = create_quality_layer(codec, tile, slope, l, 0);
     if (est >= 0)
       est_tile += est + (int64_t)header_size;

@@ -97,6 +97,13 @@ void launch_t1_decode_ex(bwc_float *work, const CbDev *cbs, uint32_t ncb,
                          uint32_t *flags, uint32_t state_cap, uint16_t *gstate,
                          uint32_t *work_counter, int grid, cudaStream_t s);
 
+// mlp.cu: the rate-control warm start's network (34 -> 64 -> 64 -> 1, FP32).
+constexpr int kMlpInputs = kRateFeatures;
+constexpr int kMlpParams = 64 * kMlpInputs + 64 + 64 * 64 + 64 + 64 + 1;
+// predictions for n (<= 64) feature rows with the model set by bwc_b200_set_rate_model;
+// false when no model is set
+bool mlp_predict(const float *features, int n, float *out);
+
 // gather.cu: dst[p.dst .. +size) = (p.from_blob ? blob : dev)[p.src .. +size)
 void launch_gather(uint8_t *dst, const uint8_t *blob, const uint8_t *dev,
                    const GatherPiece *pieces, uint64_t npieces, cudaStream_t s);

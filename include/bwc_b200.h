@@ -111,6 +111,42 @@ uchar  bwc_b200_compress_batch(bwc_codec *const *codecs, bwc_stream *const *stre
  * [5] whole call.  Returns the number of entries written (at most n). */
 int    bwc_b200_last_batch_timings(double *out_ms, int n);
 
+/* Rate-control warm start.  No counterpart in the reference API.
+ *
+ * The reference's rate control bisects, per quality layer, over a 16-bit log-slope threshold;
+ * every probe depends on the previous one.  With a model set, the library predicts each layer's
+ * final threshold with a small network (34 -> 64 -> 64 -> 1, ReLU, FP32; hand-written CUDA
+ * kernels), evaluates the whole probe path that prediction implies at once (in parallel host
+ * threads) and replays the exact bisection over those results; a path that leaves the predicted
+ * one costs another round.  The probes, their order and the selected thresholds are the plain
+ * search's, so the codestream is byte-identical with or without a model.
+ *
+ * Network parameters: BWC_B200_MLP_PARAMS floats, W1[64][34], b1[64], W2[64][64], b2[64],
+ * W3[64], b3.  Inputs (bwc_b200_rate_features): a 32-bin histogram of the codeblocks' non-zero
+ * pass slopes (bins of 2048), log(layer bits per value) / 4, (log(values) - 14) / 4.  Output:
+ * final threshold / 65536.
+ *
+ * set_rate_model     : copies the parameters (NULL: plain bisection again); process-wide.
+ * rate_features      : the 34 inputs of `layer` in the last compression of `codec`.
+ * rate_stats         : of that layer: final threshold, probes, rounds of dependent probes,
+ *                      predicted threshold (-1 without a model), slope range min and max.
+ * mlp_forward        : y[n] = network(X[n][34]) (host arrays; runs on the current device).
+ * mlp_gradient       : gradient of mean((y - t)^2) over the n rows, and that loss.
+ * mlp_train          : `epochs` passes of Adam (learning rate lr, minibatches of `batch` rows
+ *                      drawn in a seeded order) starting from and updating `params`; the mean
+ *                      minibatch loss of every epoch goes to loss_per_epoch (may be NULL).
+ * All return 0 on success. */
+#define BWC_B200_MLP_PARAMS 6465
+int    bwc_b200_set_rate_model(const float *params);
+int    bwc_b200_rate_features(bwc_codec *const codec, uint8 const layer, float *out34);
+int    bwc_b200_rate_stats(bwc_codec *const codec, uint8 const layer, double *out6);
+int    bwc_b200_mlp_forward(const float *params, const float *X, uint32 n, float *y);
+int    bwc_b200_mlp_gradient(const float *params, const float *X, const float *t, uint32 n,
+                             float *grad, float *loss);
+int    bwc_b200_mlp_train(float *params, const float *X, const float *t, uint32 n,
+                          uint32 epochs, uint32 batch, float lr, uint64 seed,
+                          float *loss_per_epoch);
+
 /* Tier-1 encoding of ONE codeblock without any memory allocation.  No counterpart in the
  * reference API.
  *
