@@ -26,9 +26,35 @@ PRECISIONS = {"double": [], "single": ["-DBWC_SINGLE_PRECISION"]}
 
 
 def _sources():
-    host = sorted(glob.glob(os.path.join(CSRC, "host", "*.cpp")))
+    host = sorted(glob.glob(os.path.join(CSRC, "host", "*.cpp"))) + [_rate_model_source()]
     dev = sorted(glob.glob(os.path.join(CSRC, "kernels", "*.cu")))
     return host, dev
+
+
+MODEL = os.path.join(HERE, "data", "pcrd_mlp.npy")
+
+
+def _rate_model_source():
+    """Generated C++ source holding the trained rate-control model (data/pcrd_mlp.npy, made by
+    bigwhoop_b200/ratemodel.py) as the library's built-in warm-start model; a library built
+    without the file has none."""
+    out = os.path.join(LIB, "gen", "rate_model_data.cpp")
+    os.makedirs(os.path.dirname(out), exist_ok=True)
+    if os.path.exists(MODEL):
+        import numpy as np
+        w = np.load(MODEL).astype(np.float32).ravel()
+        body = ",\n".join(", ".join(f"{float(v)!r}f" if np.isfinite(v) else "0.0f" for v in w[i:i + 8])
+                           for i in range(0, w.size, 8))
+        text = ("// generated by bigwhoop_b200/build.py from data/pcrd_mlp.npy\n"
+                "namespace bwcb {\n"
+                f"extern const float kBuiltinRateModel[{w.size}] = {{\n{body}\n}};\n"
+                f"extern const int kBuiltinRateModelSize = {w.size};\n}}\n")
+    else:
+        text = ("namespace bwcb {\nextern const float kBuiltinRateModel[1] = {0.0f};\n"
+                "extern const int kBuiltinRateModelSize = 0;\n}\n")
+    if not os.path.exists(out) or open(out).read() != text:
+        open(out, "w").write(text)
+    return out
 
 
 def _headers():

@@ -17,6 +17,10 @@
 #include "device_common.cuh"
 
 namespace bwcb {
+
+extern const float kBuiltinRateModel[];
+extern const int kBuiltinRateModelSize;
+
 namespace {
 
 constexpr int kIn = kMlpInputs, kHid = 64;
@@ -155,10 +159,21 @@ void gradient_on_device(Scratch &w, int n, cudaStream_t s) {
   mlp_reduce_kernel<<<(kMlpParams + 255) / 256, 256, 0, s>>>(w.G, n, w.grad, w.Y, w.T, w.loss);
 }
 
-// model for rate-control warm starts, per device
+// model for rate-control warm starts: the built-in one (compiled from data/pcrd_mlp.npy) until
+// bwc_b200_set_rate_model replaces or disables it
 std::mutex g_model_mutex;
+bool g_model_init = false;
 bool g_model_set = false;
 std::vector<float> g_model;
+
+void init_model_locked() {
+  if (g_model_init) return;
+  g_model_init = true;
+  if (kBuiltinRateModelSize == kMlpParams) {
+    g_model.assign(kBuiltinRateModel, kBuiltinRateModel + kMlpParams);
+    g_model_set = true;
+  }
+}
 float *g_model_dev[64] = {};
 float *g_io_dev[64] = {};
 cudaStream_t g_model_stream[64] = {};
@@ -167,6 +182,7 @@ cudaStream_t g_model_stream[64] = {};
 
 bool mlp_predict(const float *features, int n, float *out) {
   std::lock_guard<std::mutex> lock(g_model_mutex);
+  init_model_locked();
   if (!g_model_set || n <= 0 || n > 64) return false;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
@@ -262,6 +278,7 @@ extern "C" int bwc_b200_mlp_train(float *params, const float *X, const float *t,
 
 extern "C" int bwc_b200_set_rate_model(const float *params) {
   std::lock_guard<std::mutex> lock(g_model_mutex);
+  g_model_init = true;
   if (!params) {
     g_model_set = false;
     return 0;

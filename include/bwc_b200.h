@@ -126,7 +126,9 @@ int    bwc_b200_last_batch_timings(double *out_ms, int n);
  * pass slopes (bins of 2048), log(layer bits per value) / 4, (log(values) - 14) / 4.  Output:
  * final threshold / 65536.
  *
- * set_rate_model     : copies the parameters (NULL: plain bisection again); process-wide.
+ * set_rate_model     : copies the parameters (NULL: plain bisection); process-wide.  Until it
+ *                      is called, the library uses its built-in model (trained by
+ *                      bigwhoop_b200/ratemodel.py on 2000 synthetic fields).
  * rate_features      : the 34 inputs of `layer` in the last compression of `codec`.
  * rate_stats         : of that layer: final threshold, probes, rounds of dependent probes,
  *                      predicted threshold (-1 without a model), slope range min and max.

@@ -4,7 +4,7 @@
   within 1e-4 relative to the largest gradient entry);
 * training with the CUDA kernels lowers the loss;
 * codestreams are byte-identical with and without a model, and with the trained model the
-  rate control needs fewer rounds of dependent probes than the plain bisection's probe count.
+  rate control needs fewer rounds of dependent probes than the plain bisection.
 """
 import os
 
@@ -74,8 +74,9 @@ def test_warm_start_keeps_bytes_and_saves_rounds(gpu):
         assert cs_warm == cs_plain
         assert np.array_equal(st_warm[:, 0], st_plain[:, 0])     # same final thresholds
         assert np.array_equal(st_warm[:, 1], st_plain[:, 1])     # same probes
-        assert np.all(st_plain[:, 2] == st_plain[:, 1])          # plain: one probe per round
+        # plain: one new probe per round (a slope the search revisits is not evaluated again)
+        assert np.all(st_plain[:, 2] <= st_plain[:, 1])
         assert np.all(st_warm[:, 3] >= 0)                        # a prediction was made
-        probes += st_plain[:, 1].sum()
+        probes += st_plain[:, 2].sum()
         rounds += st_warm[:, 2].sum()
     assert rounds < probes, (rounds, probes)
