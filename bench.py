@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
     ap.add_argument("--size", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the batched-vs-plain comparison on the 64-field uneven batch")
     return ap.parse_args()
 
 
@@ -234,7 +236,7 @@ def run_reference(a):
 def run_ours(a):
     import torch
     ws, rank, local = dist_setup(a)
-    from bigwhoop_b200 import bwc
+    from bigwhoop_b200 import bwc, ratemodel
     prec = "double" if a.dtype == "f64" else "single"
     # FP64 fields are coded by the double build (the reference's default); FP32 by the single
     field = make_field(a, "cuda").contiguous()
@@ -267,9 +269,11 @@ def run_ours(a):
         torch.cuda.synchronize()
         dt = ev0.elapsed_time(ev1) * 1e-3
         tm = c.timings()
+        rc = np.array([ratemodel.stats(c, l) for l in range(len(RATES.split(",")))])
         c.close()
         if n == 0:
             raise RuntimeError("bwc_compress failed")
+        one.rate_stats = rc
         return dt, int(n), tm
 
     for _ in range(a.warmup):
@@ -284,6 +288,13 @@ def run_ours(a):
     for _ in range(max(1, a.steps)):
         dt, ncs_h, _ = one(False)
         e2e_times.append(max_over_ranks(ws, dt))
+    rate_warm = one.rate_stats
+    # the same compression with the plain bisection (warm start off), for its tier-2 time
+    ratemodel.set_model(None, prec)
+    _, ncs_plain, tm_plain = one(True)
+    rate_plain = one.rate_stats
+    cs_plain = bytes(dev_out[:ncs_plain].cpu().numpy())
+    ratemodel.load_default(prec)
     t = float(np.mean(times))
     te = float(np.mean(e2e_times))
     stage = np.mean(np.array(stage), axis=0)
@@ -312,9 +323,11 @@ def run_ours(a):
     rng = float(orig.max() - orig.min())
     psnr = 20 * np.log10(rng / (2 * np.sqrt(mse))) if mse > 0 else float("inf")
 
-    # kernels per compression: fill+min/max, normalise, one DWT pass per (level, axis),
-    # tier-1 context modelling + MQ coding, codestream gather
-    launches = 2 + DECOMP[0] * 3 + 2 + 1
+    # kernels per compression: fill+min/max, normalise, one fused DWT pass per level and the
+    # region copies between the ping-pong buffers (before every even level but the first, and
+    # after an even number of levels), tier-1 context modelling + MQ coding, codestream gather
+    L = DECOMP[0]
+    launches = 2 + L + len(range(2, L, 2)) + (1 if L % 2 == 0 else 0) + 2 + 1
     line = None
     if rank == 0:
         total_bytes = nbytes * ws
@@ -365,7 +378,16 @@ def run_ours(a):
                         "device_and_host_codestreams_equal": cs == cs_dev},
             "clocks": clocks.summary(),
             "gpu_launches": launches,
+            "rate_control": {
+                "warm_start": "built-in model (bigwhoop_b200/data/pcrd_mlp.npy)",
+                "dependent_probe_rounds_per_layer": [int(v) for v in rate_warm[:, 2]],
+                "plain_bisection_probes_per_layer": [int(v) for v in rate_plain[:, 1]],
+                "tier2_host_ms_warm": round(float(stage[5]), 3),
+                "tier2_host_ms_plain": round(float(tm_plain[5]), 3),
+                "codestreams_equal": cs_plain == cs_dev},
         }
+        if not a.no_batch and ws == 1:
+            line["batch"] = batch_compare(prec)
         if not a.no_cpu_baseline and ws == 1:
             line["cpu_baseline"] = cpu_baseline(host_in.numpy(), a)
         print(json.dumps(line), flush=True)
@@ -373,6 +395,77 @@ def run_ours(a):
         import torch.distributed as dist
         dist.destroy_process_group()
     return 0
+
+
+def batch_compare(prec):
+    """The uneven batch: 64 fields (seed 2, extents U[33, 300], FP32/FP64, rates 0.25-4 bpv,
+    2-4 levels, 32x32x16 codeblocks) from host memory, compressed by 64 plain bwc_compress calls
+    (plain bisection) and by one bwc_b200_compress_batch (warm start on), both end to end."""
+    import torch
+    from bigwhoop_b200 import bwc, fields, ratemodel
+    desc = fields.uneven_batch(seed=2, n_fields=64)
+    fs = []
+    for d in desc:
+        f = fields.shock_field(d["shape"], d["seed"], dtype=d["dtype"], slope=d["slope"], device="cuda")
+        fs.append(f.cpu().numpy())
+    torch.cuda.synchronize()
+    total = sum(f.nbytes for f in fs)
+
+    def comp(f, d):
+        lv = d["levels"]
+        return bwc.Compressor(f, precision=prec, decomp=(lv, lv, lv, 0), codeblocks=(5, 5, 4, 0),
+                              rate=str(d["rate"]))
+
+    def plain():
+        ratemodel.set_model(None, prec)
+        bwc.reset_gain_state(prec)
+        out = []
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record()
+        for f, d in zip(fs, desc):
+            c = comp(f, d)
+            try:
+                out.append(c.compress())
+            finally:
+                c.close()
+        ev1.record()
+        torch.cuda.synchronize()
+        dt = ev0.elapsed_time(ev1) * 1e-3
+        ratemodel.load_default(prec)
+        return dt, out
+
+    def batched():
+        bwc.reset_gain_state(prec)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record()
+        comps = [comp(f, d) for f, d in zip(fs, desc)]
+        try:
+            out = bwc.compress_batch(comps)
+        finally:
+            for c in comps:
+                c.close()
+        ev1.record()
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1) * 1e-3, out
+
+    batched()   # warm-up
+    tb, outb = min((batched() for _ in range(2)), key=lambda r: r[0])
+    tp, outp = plain()
+    tim = bwc.batch_timings(prec)
+    return {"workload": "uneven batch: 64 fields, seed 2, extents U[33,300], FP32/FP64, rates "
+                        "{0.25..4} bpv, 2-4 levels, cb 32x32x16 (codec precision %s)" % prec,
+            "input_bytes": total, "timing": "CUDA events around codec set-up and compression of "
+            "all 64 fields (each call returns with its codestream); inputs and codestreams in "
+            "host memory",
+            "batched_warm_GBps": total / tb / 1e9, "plain_per_field_GBps": total / tp / 1e9,
+            "speedup": tp / tb, "codestreams_equal": outb == outp,
+            "batched_stages_ms": {"setup_uploads": round(float(tim[0]), 1),
+                                  "transform": round(float(tim[1]), 1),
+                                  "tier1": round(float(tim[2]), 1),
+                                  "tier2_host": round(float(tim[3]), 1),
+                                  "gather_outputs": round(float(tim[4]), 1)}}
 
 
 def main():

@@ -948,6 +948,7 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
   std::atomic<uint32_t> next{0};
   std::atomic<int> failed{0};
   auto worker = [&]() {
+    t_rate_control_in_parallel_fields = true;
     for (;;) {
       const uint32_t i = next.fetch_add(1);
       if (i >= nf) return;
@@ -989,6 +990,7 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
     std::vector<std::thread> pool;
     for (unsigned t = 1; t < nt; ++t) pool.emplace_back(worker);
     worker();
+    t_rate_control_in_parallel_fields = false;
     for (auto &t : pool) t.join();
   }
   if (failed) return 1;

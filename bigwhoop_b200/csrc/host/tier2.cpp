@@ -460,6 +460,10 @@ std::vector<uint16_t> predicted_path(Search st, uint16_t pred, int64_t target) {
 
 }  // namespace
 
+// Set by the batch driver in its worker threads: the fields already run in parallel there, so
+// the speculative probes of one field are not spread over further threads.
+thread_local bool t_rate_control_in_parallel_fields = false;
+
 // create_quality_layers (tier2.c:1115-1254)
 static uchar create_quality_layers(bwc_codec *codec, Tile &tile) {
   const bwc_gl_ctrl &c = codec->control;
@@ -482,7 +486,9 @@ static uchar create_quality_layers(bwc_codec *codec, Tile &tile) {
       !check && c.nLayers <= 64 && mlp_predict(tile.rc_features.data(), c.nLayers, pred.data());
   uint64_t ncb_total = 0;
   for (const Parameter &par : tile.params) ncb_total += par.codeblocks.size();
-  const bool parallel = have_pred && ncb_total >= 256;
+  // with no spare threads the prediction is recorded but probes are evaluated on demand
+  const bool speculate = have_pred && !t_rate_control_in_parallel_fields;
+  const bool parallel = speculate && ncb_total >= 256;
   for (uint8_t l = 0; l < c.nLayers; ++l) {
     uint16_t slope;
     int probes = 0, rounds = 0;
@@ -510,7 +516,7 @@ static uchar create_quality_layers(bwc_codec *codec, Tile &tile) {
         if (!lookup(s, &e)) {
           // a new round: this probe, plus the rest of the predicted path
           std::vector<uint16_t> todo{s};
-          if (have_pred) {
+          if (speculate) {
             todo = predicted_path(st, pslope, target - est_tile - (int64_t)header_size);
             if (todo.empty() || todo[0] != s) todo.insert(todo.begin(), s);
           }
