@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the batched-vs-plain comparison on the 64-field uneven batch")
+    ap.add_argument("--config", default="single", choices=["single", "combined4d"],
+                    help="combined4d: the 384^3 x 8 FP64 advected time series instead")
     return ap.parse_args()
 
 
@@ -468,10 +470,115 @@ def batch_compare(prec):
                                   "gather_outputs": round(float(tim[4]), 1)}}
 
 
+def run_combined4d(a):
+    """The combined large 4D workload: a 384^3 x 8 FP64 spectral field advected by 1.5 cells per
+    step with fresh noise (seed 3), 3 spatial and 2 temporal decomposition levels, codeblocks
+    32x32x8x2, 6 quality layers 0.25 ... 8 bpv.  Compressed from host memory through the batched
+    path with the warm start and through the plain bwc_compress call without it (same bytes),
+    then decompressed in full; PSNR and max-abs error against the original.  The reference CPU
+    library runs on a bounded sample (the first 2 time steps of a central 192^3 window)."""
+    import torch
+    from bigwhoop_b200 import bwc, fields, ratemodel
+    from oracle import ref
+    rates = "0.25,0.5,1,2,4,8"
+    kw = dict(precision="double", decomp=(3, 3, 3, 2), codeblocks=(5, 5, 3, 1), rate=rates)
+    f = fields.advected_field((8, 384, 384, 384), 3, device="cuda")
+    host = f.cpu().pin_memory()
+    del f
+    torch.cuda.empty_cache()
+    arr = host.numpy()
+    nbytes = arr.nbytes
+    out = torch.empty(nbytes + (1 << 20), dtype=torch.uint8).pin_memory()
+
+    def timed(fn):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record()
+        r = fn()
+        ev1.record()
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1) * 1e-3, r
+
+    def batched():
+        bwc.reset_gain_state()
+        c = bwc.Compressor(arr, out=out.numpy(), **kw)
+        try:
+            cs = bwc.compress_batch([c])[0]   # bytes: the output buffer is host memory
+            st = [ratemodel.stats(c, l) for l in range(6)]
+        finally:
+            c.close()
+        return cs, st
+
+    def plain():
+        ratemodel.set_model(None)
+        bwc.reset_gain_state()
+        c = bwc.Compressor(arr, out=out.numpy(), **kw)
+        try:
+            cs = c.compress()
+            st = [ratemodel.stats(c, l) for l in range(6)]
+        finally:
+            c.close()
+            ratemodel.load_default()
+        return cs, st
+
+    timed(batched)   # warm-up
+    tb, (cs_b, st_b) = timed(batched)
+    tp, (cs_p, st_p) = timed(plain)
+    dec = torch.empty(arr.shape, dtype=torch.float64).pin_memory()
+
+    def decompress():
+        d = bwc.Decompressor(cs_b, out=dec.data_ptr())
+        try:
+            d.decompress()
+        finally:
+            d.close()
+
+    td, _ = timed(decompress)
+    err = np.abs(dec.numpy() - arr)
+    mse = float(np.mean(err ** 2))
+    rng_ = float(arr.max() - arr.min())
+    # reference CPU library on a bounded sample
+    sub = np.ascontiguousarray(arr[:2, 96:288, 96:288, 96:288])
+    threads = os.cpu_count()
+    ref.set_threads(threads)
+    ref.reset_gain_lut()
+    rc = ref.RefCompressor(sub, decomp=(3, 3, 3, 1), cb=(5, 5, 3, 1), rate=rates)
+    t0 = time.perf_counter()
+    rc.compress()
+    tr = time.perf_counter() - t0
+    rc.close()
+    line = {"metric": METRIC, "value": nbytes / tb / 1e9, "unit": "GB/s", "n_gpus": 1,
+            "steps": 1, "warmup": 1, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "combined 4D: 384^3 x 8 FP64 advected spectral field (1.5 "
+                                   "cells/step, noise 1e-5, seed 3), decomp 3 spatial + 2 "
+                                   "temporal, cb 32x32x8x2, layers " + rates + " bpv",
+                       "input_bytes": nbytes},
+            "e2e": {"value": nbytes / tb / 1e9, "unit": "GB/s", "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": len(cs_b)},
+            "path": "bwc_b200_compress_batch with the warm start, host buffers",
+            "plain_path_GBps": nbytes / tp / 1e9, "codestreams_equal": cs_b == cs_p,
+            "decompress_GBps": nbytes / td / 1e9,
+            "quality": {"psnr_db": 20 * np.log10(rng_ / (2 * np.sqrt(mse))) if mse > 0 else None,
+                        "max_abs_err": float(err.max()), "codestream_bytes": len(cs_b),
+                        "bpv": len(cs_b) * 8 / arr.size},
+            "rate_control": {"rounds_per_layer_warm": [int(v[2]) for v in st_b],
+                             "probes_per_layer_plain": [int(v[1]) for v in st_p]},
+            "cpu_baseline": {"value": sub.nbytes / tr / 1e9, "unit": "GB/s", "cores": threads,
+                             "kind": "reference",
+                             "sample": "time steps 0-1 of the central 192^3 window (113 MiB), "
+                                       "temporal decomposition 1 level (2 steps), same other "
+                                       "settings"}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         return run_reference(a)
+    if a.config == "combined4d":
+        return run_combined4d(a)
     return run_ours(a)
 
 

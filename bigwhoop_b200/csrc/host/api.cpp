@@ -948,7 +948,7 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
   std::atomic<uint32_t> next{0};
   std::atomic<int> failed{0};
   auto worker = [&]() {
-    t_rate_control_in_parallel_fields = true;
+    t_rate_control_in_parallel_fields = nf > 1;   // a lone field may spread its probes
     for (;;) {
       const uint32_t i = next.fetch_add(1);
       if (i >= nf) return;

@@ -95,6 +95,30 @@ def _eval_torch(shape, k, phase, amp, device):
     return f
 
 
+def advected_field(shape, seed, *, shift=1.5, n_modes=256, slope=-11.0 / 6.0, kmin=1.0,
+                   kmax=16.0, noise=1e-5, dtype=np.float64, device="cuda"):
+    """Time series (nTS, nZ, nY, nX) of a 3D spectral field advected along x by `shift` cells
+    per step (a phase shift of every mode), each step with fresh Gaussian noise of relative
+    standard deviation `noise`.  Evaluated with torch on `device`."""
+    import torch
+    nt, spatial = int(shape[0]), tuple(int(v) for v in shape[1:])
+    rng = np.random.default_rng(seed)
+    k, phase, amp = _mode_params(rng, n_modes, 3, kmin, kmax, slope)
+    noise_seed = int(rng.integers(0, 2**63 - 1))
+    g = torch.Generator(device=device).manual_seed(noise_seed)
+    out = torch.empty((nt,) + spatial, dtype=_torch_dtype(dtype), device=device)
+    nx = spatial[2]
+    for t in range(nt):
+        # f(x - shift * t): every mode's phase moves by -2 pi k_x shift t / nx
+        ph = phase - 2.0 * math.pi * k[:, 0] * shift * t / nx
+        f = _eval_torch(spatial, k, ph, amp, device)
+        if noise:
+            f += torch.randn(f.shape, generator=g, device=device, dtype=f.dtype) * (noise * f.std())
+        out[t] = f.to(out.dtype)
+        del f
+    return out
+
+
 def add_shocks(f, seed, n_fronts=8, width=2.0, rel_amp=1.0):
     """Add ``n_fronts`` tanh fronts of the given width (cells) across random planes (numpy)."""
     rng = np.random.default_rng(seed)
