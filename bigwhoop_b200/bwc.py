@@ -158,6 +158,7 @@ def load(precision="double"):
         "bwc_b200_compress_batch": (C.c_uint8, [vp, vp, C.c_uint32, vp]),
         "bwc_b200_last_batch_timings": (C.c_int, [vp, C.c_int]),
         "bwc_b200_set_rate_model": (C.c_int, [vp]),
+        "bwc_b200_mq_lanes": (C.c_int, [C.c_uint32]),
         "bwc_b200_rate_features": (C.c_int, [cp, u8, vp]),
         "bwc_b200_rate_stats": (C.c_int, [cp, u8, vp]),
         "bwc_b200_mlp_forward": (C.c_int, [vp, vp, C.c_uint32, vp]),

@@ -34,8 +34,14 @@
 // Stripe-column state (shared memory, one byte each): lo = significance | sign << 4 (read by
 // neighbours), hi = visited-in-significance-pass | refined << 4 (owner only).  Bit planes: one
 // byte per stripe column per plane, the column's four bits in the low nibble, row 0 at bit 3.
+#include <algorithm>
 #include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <string>
 
+#include "bwc_b200.h"
 #include "device_common.cuh"
 #include "t1_tables.cuh"
 
@@ -833,28 +839,26 @@ __global__ void __launch_bounds__(kMqThreads) t1_mq_kernel(const CbDev *__restri
                                           (uint32_t)((s0 >> 40) & 0xFF), Ls, bo.out, bo.cap, &bad);
   }
   if (bad) bo.flags |= 4u;
-  // convex hull (scratch: distortions overwrite dmse, slopes and hull stack the snapshots)
-  double *mse_d = reinterpret_cast<double *>(dmse);
+  // convex hull (scratch: slopes and hull stack overwrite the snapshots; dmse stays as it is,
+  // so the kernel can run again on the same symbol streams)
   double *lambda = reinterpret_cast<double *>(snaps);
   uint8_t *hull = reinterpret_cast<uint8_t *>(snaps + kMaxPasses + 1);
-  double scale = sb.gain_step2;
-  scale = dev::fmul(scale, ldexp(1.0, 2 * K));
-  scale = dev::fdiv(scale, 65536.0);
-  {
-    int j = 0;
-    for (int b = K - 1; b >= 0; --b) {
-      for (int kind = (b == K - 1) ? 2 : 0; kind < 3; ++kind, ++j)
-        mse_d[j] = dev::fmul(__ll2double_rn(dmse[j]), scale);
-      scale = dev::fmul(scale, 0.25);
-    }
-  }
+  double scale0 = sb.gain_step2;
+  scale0 = dev::fmul(scale0, ldexp(1.0, 2 * K));
+  scale0 = dev::fdiv(scale0, 65536.0);
+  // distortion decrease of pass q in the reference's weighting: the weight is scale0 for the
+  // first plane and a quarter less per plane below (exact: powers of two, no subnormals);
+  // pass 0 codes plane K-1, passes 1-3 plane K-2, and so on
+  auto mse_of = [&](int q) -> double {
+    return dev::fmul(__ll2double_rn(dmse[q]), ldexp(scale0, -2 * ((q + 2) / 3)));
+  };
   for (int i = 0; i <= Z; ++i) lambda[i] = 0.0;
   for (int i = 0; i < Z; ++i) hull[i] = 0;
   lambda[0] = 18446744073709551616.0;
   int h = 0, hlast = 0;
   for (int i = 0; i < Z; ++i) {
     double dD = 0.0;
-    for (int q = hlast; q <= i; ++q) dD = dev::fadd(dD, mse_d[q]);
+    for (int q = hlast; q <= i; ++q) dD = dev::fadd(dD, mse_of(q));
     uint64_t dL = (hlast > 0) ? (uint64_t)Lout[i] - Lout[hlast - 1] : (uint64_t)Lout[i];
     if (dD > 0) {
       while (dD >= dev::fmul(lambda[hlast], __ull2double_rn(dL))) {
@@ -867,7 +871,7 @@ __global__ void __launch_bounds__(kMqThreads) t1_mq_kernel(const CbDev *__restri
         h--;
         hlast = hull[h];
         dD = 0.0;
-        for (int q = hlast; q <= i; ++q) dD = dev::fadd(dD, mse_d[q]);
+        for (int q = hlast; q <= i; ++q) dD = dev::fadd(dD, mse_of(q));
         dL = (hlast > 0) ? (uint64_t)Lout[i] - Lout[hlast - 1] : (uint64_t)Lout[i];
       }
       h++;
@@ -920,6 +924,49 @@ uint32_t mq_lanes_per_warp(uint32_t ncb) {
   return lanes;
 }
 
+// ---- autotuner: codeblocks per MQ warp ------------------------------------------------------
+// mq_lanes_per_warp is a rule measured on one B200 workload.  The first time a GPU model sees a
+// codeblock-count class (the count's bit length) it times the MQ kernel with the candidate lane
+// counts around the rule's -- on the real symbol streams; the kernel reads only the streams and
+// the model kernel's per-pass records and rewrites all of its outputs, so every run produces the
+// same results -- and keeps the fastest for that class.  Results live for the process and, with
+// BWC_B200_TUNE_FILE set, in that file (one "gpu-name class lanes" line each), so later
+// processes start tuned.  BWC_B200_AUTOTUNE=0 keeps the rule.
+namespace {
+
+std::mutex g_tune_mutex;
+std::map<std::string, uint32_t> g_tuned;   // "gpu-name/class" -> lanes
+bool g_tune_loaded = false;
+
+std::string tune_key(uint32_t ncb) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceProp prop;
+  std::string name = "gpu";
+  if (cudaGetDeviceProperties(&prop, dev) == cudaSuccess) name = prop.name;
+  for (char &ch : name)
+    if (ch == ' ') ch = '_';
+  int cls = 0;
+  while ((ncb >> cls) > 1) ++cls;
+  return name + "/" + std::to_string(cls);
+}
+
+void load_tune_file_locked() {
+  if (g_tune_loaded) return;
+  g_tune_loaded = true;
+  const char *path = getenv("BWC_B200_TUNE_FILE");
+  if (!path) return;
+  FILE *f = fopen(path, "r");
+  if (!f) return;
+  char key[256];
+  unsigned lanes = 0;
+  while (fscanf(f, "%255s %u", key, &lanes) == 2)
+    if (lanes >= 1 && lanes <= 32) g_tuned[key] = lanes;
+  fclose(f);
+}
+
+}  // namespace
+
 // Context modelling, then MQ coding, on `s`.  (Running the modelling of later codeblocks
 // concurrently with the MQ coding of earlier ones was measured slower: the issue-bound modelling
 // warps lengthen the latency-bound MQ chains, and the longest chain sets the time.)
@@ -929,8 +976,58 @@ void launch_t1_encode(const bwc_float *work, const CbDev *cbs, uint32_t ncb, con
   const size_t smem = t1_model_smem(max_cols);
   cudaFuncSetAttribute(t1_model_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   t1_model_kernel<<<ncb, kModelThreads, smem, s>>>(work, cbs, ncb, sbs, out);
-  const uint32_t lanes = mq_lanes_per_warp(ncb);
+  const uint32_t rule = mq_lanes_per_warp(ncb);
+  uint32_t lanes = rule;
+  bool tune = false;
+  std::string key;
+  const char *at = getenv("BWC_B200_AUTOTUNE");
+  if (ncb >= 64 && !(at && at[0] == '0')) {
+    key = tune_key(ncb);
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    load_tune_file_locked();
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end())
+      lanes = it->second;
+    else
+      tune = true;
+  }
   t1_mq_kernel<<<(ncb + lanes - 1) / lanes, kMqThreads, 0, s>>>(cbs, ncb, sbs, out, lanes);
+  if (!tune) return;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  uint32_t best_lanes = rule;
+  for (uint32_t cand = std::max(1u, rule / 4); cand <= std::min(32u, rule * 4); cand *= 2) {
+    cudaEventRecord(e0, s);
+    t1_mq_kernel<<<(ncb + cand - 1) / cand, kMqThreads, 0, s>>>(cbs, ncb, sbs, out, cand);
+    cudaEventRecord(e1, s);
+    if (cudaEventSynchronize(e1) != cudaSuccess) break;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best) {
+      best = ms;
+      best_lanes = cand;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  g_tuned[key] = best_lanes;
+  if (const char *path = getenv("BWC_B200_TUNE_FILE")) {
+    if (FILE *f = fopen(path, "a")) {
+      fprintf(f, "%s %u\n", key.c_str(), best_lanes);
+      fclose(f);
+    }
+  }
+}
+
+extern "C" int bwc_b200_mq_lanes(uint32 ncb) {
+  if (!ncb) return 0;
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  load_tune_file_locked();
+  auto it = g_tuned.find(tune_key(ncb));
+  return (int)(it != g_tuned.end() ? it->second : mq_lanes_per_warp(ncb));
 }
 
 }  // namespace bwcb

@@ -111,6 +111,12 @@ uchar  bwc_b200_compress_batch(bwc_codec *const *codecs, bwc_stream *const *stre
  * [5] whole call.  Returns the number of entries written (at most n). */
 int    bwc_b200_last_batch_timings(double *out_ms, int n);
 
+/* Codeblocks per warp the MQ coder uses for a launch of `ncb` codeblocks on the current GPU:
+ * the autotuned value when this GPU model has tuned that size class (its first tier-1 launch of
+ * the class times the candidates; BWC_B200_TUNE_FILE persists results, BWC_B200_AUTOTUNE=0
+ * disables tuning), else the built-in rule.  No counterpart in the reference API. */
+int    bwc_b200_mq_lanes(uint32 ncb);
+
 /* Rate-control warm start.  No counterpart in the reference API.
  *
  * The reference's rate control bisects, per quality layer, over a 16-bit log-slope threshold;
