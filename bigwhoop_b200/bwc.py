@@ -422,8 +422,10 @@ def compress_batch(compressors):
 
 
 def batch_timings(precision="double"):
-    out = np.zeros(6)
-    k = load(precision).bwc_b200_last_batch_timings(out.ctypes.data, 6)
+    """[0] set-up/uploads, [1] transforms, [2] tier-1, [3] tier-2, [4] gather/outputs, [5] call
+    (ms); [6] graphs captured and [7] graph launches so far."""
+    out = np.zeros(8)
+    k = load(precision).bwc_b200_last_batch_timings(out.ctypes.data, 8)
     return out[:k]
 
 

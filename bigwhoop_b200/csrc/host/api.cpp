@@ -21,6 +21,7 @@
 #include <atomic>
 #include <map>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -695,6 +696,10 @@ struct BatchState {
   DevBuf in, work, temp, keys, stats, cbtab, sbtab, bytes, scratch, snaps, dmse, K, Z, L, S,
       flags, slopes, pcount, poff, symbols, symused, blob, pieces, cs;
   double timings[8] = {};
+  // instantiated graphs of the fill/normalise/transform phase, by batch signature (geometry,
+  // sources and buffer addresses); the few most recent are kept
+  std::vector<std::pair<std::string, cudaGraphExec_t>> graphs;
+  uint64_t graph_launches = 0, graph_captures = 0;
 };
 
 constexpr int kBatchStreams = 8;
@@ -860,22 +865,68 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
   }
   cudaEventRecord(bs->ev[1], s);
 
-  // ---- fill, normalise and transform every unit, spread over the side streams
-  cudaEventRecord(bs->join[kBatchStreams], s);
-  for (int k = 0; k < kBatchStreams; ++k) cudaStreamWaitEvent(bs->side[k], bs->join[kBatchStreams], 0);
-  for (uint64_t ui = 0; ui < nu; ++ui) {
-    const BatchUnit &u = units[ui];
-    cudaStream_t ss = bs->side[ui % kBatchStreams];
-    bwc_float *temp = bs->temp.as<bwc_float>() + u.work_off;
-    bwc_float *work = bs->work.as<bwc_float>() + u.work_off;
-    launch_fill_minmax(u.src, u.src_double, u.n, temp, bs->keys.as<uint64_t>() + 2 * ui, ss);
-    launch_normalize(temp, u.n, bs->keys.as<uint64_t>() + 2 * ui, u.Qm,
-                     bs->stats.as<bwc_float>() + 4 * ui, ss);
-    launch_dwt_forward(work, temp, u.dims, u.plan, ss);
+  // ---- fill, normalise and transform every unit, spread over the side streams: captured once
+  // into a CUDA graph per batch signature and replayed
+  auto enqueue_transforms = [&]() {
+    cudaEventRecord(bs->join[kBatchStreams], s);
+    for (int k = 0; k < kBatchStreams; ++k)
+      cudaStreamWaitEvent(bs->side[k], bs->join[kBatchStreams], 0);
+    for (uint64_t ui = 0; ui < nu; ++ui) {
+      const BatchUnit &u = units[ui];
+      cudaStream_t ss = bs->side[ui % kBatchStreams];
+      bwc_float *temp = bs->temp.as<bwc_float>() + u.work_off;
+      bwc_float *work = bs->work.as<bwc_float>() + u.work_off;
+      launch_fill_minmax(u.src, u.src_double, u.n, temp, bs->keys.as<uint64_t>() + 2 * ui, ss);
+      launch_normalize(temp, u.n, bs->keys.as<uint64_t>() + 2 * ui, u.Qm,
+                       bs->stats.as<bwc_float>() + 4 * ui, ss);
+      launch_dwt_forward(work, temp, u.dims, u.plan, ss);
+    }
+    for (int k = 0; k < kBatchStreams; ++k) {
+      cudaEventRecord(bs->join[k], bs->side[k]);
+      cudaStreamWaitEvent(s, bs->join[k], 0);
+    }
+  };
+  std::string sig;
+  {
+    char buf[160];
+    snprintf(buf, sizeof buf, "%p %p %p %p|", bs->work.p, bs->temp.p, bs->keys.p, bs->stats.p);
+    sig = buf;
+    for (const BatchUnit &u : units) {
+      snprintf(buf, sizeof buf, "%p %d %llu %llu %llu %llu %llu %d %u|", (const void *)u.src,
+               (int)u.src_double, (unsigned long long)u.n, (unsigned long long)u.work_off,
+               (unsigned long long)u.dims.width, (unsigned long long)u.dims.height,
+               (unsigned long long)(u.dims.depth * 65536 + u.dims.dt), u.plan.levels, u.Qm);
+      sig += buf;
+      for (int l = 0; l < u.plan.levels; ++l) sig += std::to_string(u.plan.axis_on[l]);
+    }
   }
-  for (int k = 0; k < kBatchStreams; ++k) {
-    cudaEventRecord(bs->join[k], bs->side[k]);
-    cudaStreamWaitEvent(s, bs->join[k], 0);
+  cudaGraphExec_t exec = nullptr;
+  for (auto &g : bs->graphs)
+    if (g.first == sig) exec = g.second;
+  if (!exec) {
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      enqueue_transforms();
+      if (cudaStreamEndCapture(s, &graph) == cudaSuccess && graph &&
+          cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+        bs->graphs.emplace_back(sig, exec);
+        ++bs->graph_captures;
+        if (bs->graphs.size() > 8) {
+          cudaGraphExecDestroy(bs->graphs.front().second);
+          bs->graphs.erase(bs->graphs.begin());
+        }
+      } else {
+        exec = nullptr;
+      }
+      if (graph) cudaGraphDestroy(graph);
+    }
+    cudaGetLastError();
+  }
+  if (exec) {
+    if (!cuda_ok(cudaGraphLaunch(exec, s), "batch transform graph")) return 1;
+    ++bs->graph_launches;
+  } else {
+    enqueue_transforms();   // capture unavailable: the same launches, directly
   }
   cudaEventRecord(bs->ev[2], s);
 
@@ -1101,7 +1152,9 @@ extern "C" int bwc_b200_last_batch_timings(double *out_ms, int n) {
   std::lock_guard<std::mutex> lock(g_batch_mutex);
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || !g_batch[dev]) return 0;
-  const int k = std::min(n, 6);
+  const int k = std::min(n, 8);
+  g_batch[dev]->timings[6] = (double)g_batch[dev]->graph_captures;
+  g_batch[dev]->timings[7] = (double)g_batch[dev]->graph_launches;
   for (int i = 0; i < k; ++i) out_ms[i] = g_batch[dev]->timings[i];
   return k;
 }

@@ -108,7 +108,9 @@ uchar  bwc_b200_compress_batch(bwc_codec *const *codecs, bwc_stream *const *stre
 
 /* Stage times (ms) of the last batch on the current device: [0] set-up and uploads,
  * [1] fill/normalise/transform, [2] tier-1, [3] tier-2 (host), [4] gather and outputs,
- * [5] whole call.  Returns the number of entries written (at most n). */
+ * [5] whole call; then the counts [6] of CUDA graphs captured and [7] of graph launches so far
+ * (the fill/normalise/transform phase runs as a graph, captured once per batch signature).
+ * Returns the number of entries written (at most n). */
 int    bwc_b200_last_batch_timings(double *out_ms, int n);
 
 /* Codeblocks per warp the MQ coder uses for a launch of `ncb` codeblocks on the current GPU:

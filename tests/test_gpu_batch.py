@@ -46,6 +46,7 @@ def test_batch_equals_per_field_calls(gpu, repeat):
             plain.append(c.compress())
         finally:
             c.close()
+    counts = []
     for _ in range(repeat):
         bwc.reset_gain_state()
         comps = [_compressor(f, sp) for f, sp in zip(fs, SPECS)]
@@ -57,7 +58,11 @@ def test_batch_equals_per_field_calls(gpu, repeat):
         for i, (a, b) in enumerate(zip(plain, batch)):
             assert a == b, i
         t = bwc.batch_timings()
-        assert len(t) == 6 and t[5] > 0
+        assert len(t) == 8 and t[5] > 0
+        counts.append((t[6], t[7]))
+    if repeat == 2:
+        # the same batch again replays the captured transform graph
+        assert counts[1][0] == counts[0][0] and counts[1][1] == counts[0][1] + 1
 
 
 def test_batch_with_device_buffers(gpu):
