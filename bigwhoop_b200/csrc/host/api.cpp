@@ -127,14 +127,15 @@ struct DeviceState {
   cudaEvent_t ev[8] = {};
   DevBuf temp;     // second field-sized buffer: the transform reads one and writes the other
   DevBuf in, work, keys, stats, cbtab, sbtab, bytes, scratch, snaps, dmse, K, Z, L, S, flags,
-      slopes, counter, cs, blob, pieces, outbuf, mags, lmax, symbols, pcount, poff, symused;
+      slopes, counter, cs, blob, pieces, outbuf, mags, lmax, symbols, pcount, poff, symused,
+      order, queue;
   bool dump_set = false, ddump_set = false;
   bwc_b200_stage_dump dump{};
   bwc_b200_decode_dump ddump{};
   double timings[10] = {};   // stage times (ms); [8] tier-1 symbols coded (millions)
 
   ~DeviceState() {
-    DevBuf *all[] = {&temp, &in, &work, &keys, &stats, &cbtab, &sbtab, &bytes, &scratch, &snaps, &dmse,
+    DevBuf *all[] = {&order, &queue, &temp, &in, &work, &keys, &stats, &cbtab, &sbtab, &bytes, &scratch, &snaps, &dmse,
                      &K, &Z, &L, &S, &flags, &slopes, &counter, &cs, &blob, &pieces, &outbuf,
                      &mags, &lmax, &symbols, &pcount, &poff, &symused};
     if (stream) cudaStreamSynchronize(stream);
@@ -254,6 +255,22 @@ static void build_tables(const Parameter &par, const FieldDims &dims, uchar erre
   *max_cols = mc;
 }
 
+// Codeblock indices [0, count) of cbs[first ...] sorted by expected tier-1 work (stripe columns x
+// the subband's Kmax), largest first; ties keep tier-1 order.
+static std::vector<uint32_t> work_order(const std::vector<CbDev> &cbs, const std::vector<SbDev> &sbs,
+                                        size_t first, size_t count) {
+  std::vector<uint32_t> order(count);
+  std::vector<uint64_t> cost(count);
+  for (size_t i = 0; i < count; ++i) {
+    const CbDev &d = cbs[first + i];
+    order[i] = (uint32_t)i;
+    cost[i] = (uint64_t)d.w * ((d.h + 3) / 4) * d.d * d.nt * (sbs[d.sb].Kmax + 1);
+  }
+  std::stable_sort(order.begin(), order.end(),
+                   [&](uint32_t a, uint32_t b) { return cost[a] > cost[b]; });
+  return order;
+}
+
 static int t1_grid(const void *kernel_unused, size_t smem_per_block) {
   (void)kernel_unused;
   int dev = 0, sms = 148, smem_max = 227 * 1024;
@@ -356,8 +373,17 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
     total_samples += (uint64_t)allcb[i].w * ((allcb[i].h + 3) / 4) * 4 * allcb[i].d * allcb[i].nt;
   uint64_t arena = std::max<uint64_t>(1 << 20, total_samples * (kPrecBit + 1) * 9 / 8);
   if (!dv->pcount.ensure(ncb * kMaxPasses * 4) || !dv->poff.ensure(ncb * kMaxPasses * 8) ||
-      !dv->symused.ensure(8))
+      !dv->symused.ensure(8) || !dv->order.ensure(ncb * 4) || !dv->queue.ensure(4))
     return 0;
+  {
+    std::vector<uint32_t> order;
+    for (int p = 0; p < info.nPar; ++p) {
+      const std::vector<uint32_t> o = work_order(allcb, allsb, cb_base[p], cbs[p].size());
+      order.insert(order.end(), o.begin(), o.end());
+    }
+    cudaMemcpyAsync(dv->order.p, order.data(), ncb * 4, cudaMemcpyHostToDevice, s);
+    if (!cuda_ok(cudaStreamSynchronize(s), "tier-1 order")) return 0;
+  }
   float t_norm = 0, t_dwt = 0, t_t1 = 0;
   for (int p = 0; p < info.nPar; ++p) {
     cudaEvent_t a, b2, c2, d2;
@@ -396,7 +422,8 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
       cudaMemsetAsync(dv->symused.p, 0, 8, s);
       cudaMemsetAsync(o.flags, 0, cbs[p].size() * 4, s);
       launch_t1_encode(dv->work.as<bwc_float>(), dv->cbtab.as<CbDev>() + cb_base[p],
-                       (uint32_t)cbs[p].size(), dv->sbtab.as<SbDev>(), o, max_cols, s);
+                       (uint32_t)cbs[p].size(), dv->sbtab.as<SbDev>(), o, max_cols, s,
+                       dv->order.as<uint32_t>() + cb_base[p], dv->queue.as<uint32_t>());
       unsigned long long used = 0;
       cudaMemcpyAsync(&used, dv->symused.p, 8, cudaMemcpyDeviceToHost, s);
       if (!cuda_ok(cudaStreamSynchronize(s), "tier-1 encoding")) return 0;
@@ -694,7 +721,7 @@ struct BatchState {
   std::vector<cudaEvent_t> join;
   cudaEvent_t ev[6] = {};
   DevBuf in, work, temp, keys, stats, cbtab, sbtab, bytes, scratch, snaps, dmse, K, Z, L, S,
-      flags, slopes, pcount, poff, symbols, symused, blob, pieces, cs;
+      flags, slopes, pcount, poff, symbols, symused, blob, pieces, cs, order, queue;
   double timings[8] = {};
   // instantiated graphs of the fill/normalise/transform phase, by batch signature (geometry,
   // sources and buffer addresses); the few most recent are kept
@@ -831,8 +858,9 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
       !bs->L.ensure(ncb * kMaxPasses * 4) || !bs->S.ensure(ncb * (kMaxPasses + 1) * 2) ||
       !bs->flags.ensure(ncb * 4) || !bs->slopes.ensure(8 * nf) ||
       !bs->pcount.ensure(ncb * kMaxPasses * 4) || !bs->poff.ensure(ncb * kMaxPasses * 8) ||
-      !bs->symused.ensure(8))
+      !bs->symused.ensure(8) || !bs->order.ensure(ncb * 4) || !bs->queue.ensure(4))
     return 1;
+  const std::vector<uint32_t> order = work_order(allcb, allsb, 0, ncb);
   for (uint32_t i = 0; i < nf; ++i)
     if (in_off[i] != ~0ull)
       cudaMemcpyAsync(bs->in.as<uint8_t>() + in_off[i], streams[i]->inp, in_bytes[i],
@@ -848,6 +876,7 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
   cudaMemcpyAsync(bs->cbtab.p, allcb.data(), sizeof(CbDev) * ncb, cudaMemcpyHostToDevice, s);
   cudaMemcpyAsync(bs->sbtab.p, allsb.data(), sizeof(SbDev) * allsb.size(), cudaMemcpyHostToDevice,
                   s);
+  cudaMemcpyAsync(bs->order.p, order.data(), ncb * 4, cudaMemcpyHostToDevice, s);
   {
     std::vector<uint32_t> init(2 * nf);
     for (uint32_t i = 0; i < nf; ++i) {
@@ -953,7 +982,8 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
     cudaMemsetAsync(bs->symused.p, 0, 8, s);
     cudaMemsetAsync(bs->flags.p, 0, ncb * 4, s);
     launch_t1_encode(bs->work.as<bwc_float>(), bs->cbtab.as<CbDev>(), (uint32_t)ncb,
-                     bs->sbtab.as<SbDev>(), o, max_cols, s);
+                     bs->sbtab.as<SbDev>(), o, max_cols, s, bs->order.as<uint32_t>(),
+                     bs->queue.as<uint32_t>());
     unsigned long long used = 0;
     cudaMemcpyAsync(&used, bs->symused.p, 8, cudaMemcpyDeviceToHost, s);
     if (!cuda_ok(cudaStreamSynchronize(s), "batch tier-1 encoding")) return 1;

@@ -85,9 +85,13 @@ void launch_dwt_inverse(bwc_float *work, bwc_float *temp, const FieldDims &dims,
 // t1_encode.cu: context modelling (one CTA per codeblock, max_cols = largest number of stripe
 // columns of a codeblock) followed by MQ coding (one thread per codeblock).
 size_t t1_model_smem(uint32_t max_cols);
-// Each codeblock addresses its samples as work[base + x + y*sy + z*sz + t*st].
+// Each codeblock addresses its samples as work[base + x + y*sy + z*sz + t*st].  `order`
+// (optional, device) lists the codeblocks largest first: the MQ kernel's lanes take them in
+// that order, and with `queue` (a device counter, zeroed here) the modelling kernel runs
+// persistent and takes codeblocks from that work queue.
 void launch_t1_encode(const bwc_float *work, const CbDev *cbs, uint32_t ncb, const SbDev *sbs,
-                      const T1EncOut &out, uint32_t max_cols, cudaStream_t s);
+                      const T1EncOut &out, uint32_t max_cols, cudaStream_t s,
+                      const uint32_t *order = nullptr, uint32_t *queue = nullptr);
 
 // t1_decode.cu: decodes Z[c] passes of codeblock c from data + out_off (Lmax[c] bytes) and
 // writes the dequantised samples into the (zeroed) working buffer.

@@ -339,17 +339,17 @@ __device__ __forceinline__ int64_t block_sum64(int64_t v, int64_t *wsum) {
 
 // ---- kernel 1: quantisation + context modelling ------------------------------------------------
 
-__global__ void __launch_bounds__(kModelThreads)
-    t1_model_kernel(const bwc_float *__restrict__ work,
-                    const CbDev *__restrict__ cbs, uint32_t ncb, const SbDev *__restrict__ sbs,
-                    T1EncOut out) {
+// quantisation and context modelling of codeblock c by the whole CTA (every thread calls it,
+// every return is taken by all threads together)
+__device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ work,
+                                                const CbDev *__restrict__ cbs,
+                                                const SbDev *__restrict__ sbs,
+                                                const T1EncOut &out, const uint32_t c) {
   extern __shared__ uint8_t smem[];
   __shared__ uint32_t s_wsum[kModelThreads / 32];
   __shared__ int64_t s_wsum64[kModelThreads / 32];
   __shared__ uint32_t s_K, s_ok;
   __shared__ uint64_t s_base;
-  const uint32_t c = blockIdx.x;
-  if (c >= ncb) return;
   const int tid = threadIdx.x;
   const CbDev cb = cbs[c];
   const SbDev sb = sbs[cb.sb];
@@ -588,6 +588,29 @@ __global__ void __launch_bounds__(kModelThreads)
   }
 }
 
+// Kernel 1.  Without a queue, CTA i models codeblock order[i] (or i).  With a queue it is
+// persistent: every CTA takes the next position of the device work queue (an atomic counter
+// over `order`, largest codeblocks first) until the list is exhausted.
+__global__ void __launch_bounds__(kModelThreads)
+    t1_model_kernel(const bwc_float *__restrict__ work, const CbDev *__restrict__ cbs,
+                    uint32_t ncb, const SbDev *__restrict__ sbs, T1EncOut out,
+                    const uint32_t *__restrict__ order, uint32_t *queue) {
+  if (!queue) {
+    if (blockIdx.x < ncb) model_codeblock(work, cbs, sbs, out, order ? order[blockIdx.x] : blockIdx.x);
+    return;
+  }
+  __shared__ uint32_t s_next;
+  for (;;) {
+    if (threadIdx.x == 0) s_next = atomicAdd(queue, 1u);
+    __syncthreads();
+    const uint32_t i = s_next;
+    __syncthreads();   // every thread has read s_next before it is overwritten
+    if (i >= ncb) return;
+    model_codeblock(work, cbs, sbs, out, order ? order[i] : i);
+    __syncthreads();
+  }
+}
+
 // ---- kernel 2: MQ coding, truncation lengths, convex hull ------------------------------------
 
 // MQ encoder state (mq.c:68-110)
@@ -713,7 +736,8 @@ __device__ uint16_t slope2log(double lambda) {
 __global__ void __launch_bounds__(kMqThreads) t1_mq_kernel(const CbDev *__restrict__ cbs,
                                                            uint32_t ncb,
                                                            const SbDev *__restrict__ sbs,
-                                                           T1EncOut out, uint32_t lanes) {
+                                                           T1EncOut out, uint32_t lanes,
+                                                           const uint32_t *__restrict__ order) {
   __shared__ uint32_t tbl[94];
   // context states, [context][thread]: every lane of a warp hits its own bank
   __shared__ uint32_t ctx_all[dev::kCtxTotal][kMqThreads];
@@ -723,7 +747,8 @@ __global__ void __launch_bounds__(kMqThreads) t1_mq_kernel(const CbDev *__restri
   // without a codeblock to code (beyond `lanes`, or past the last codeblock) take part with Z = 0.  A codeblock whose symbol stream did not
   // fit the arena is skipped: the host retries with a larger one.
   const bool lane_used = threadIdx.x < lanes;
-  const uint32_t c = blockIdx.x * lanes + (lane_used ? threadIdx.x : 0u);
+  const uint32_t slot = blockIdx.x * lanes + (lane_used ? threadIdx.x : 0u);
+  const uint32_t c = (slot < ncb) ? (order ? order[slot] : slot) : ncb;
   const uint32_t cc = (c < ncb) ? c : 0u;
   const int K = (lane_used && c < ncb) ? out.K[c] : 0;
   const bool live = (K != 0) && !(out.flags[cc] & 8u);
@@ -971,11 +996,22 @@ void load_tune_file_locked() {
 // concurrently with the MQ coding of earlier ones was measured slower: the issue-bound modelling
 // warps lengthen the latency-bound MQ chains, and the longest chain sets the time.)
 void launch_t1_encode(const bwc_float *work, const CbDev *cbs, uint32_t ncb, const SbDev *sbs,
-                      const T1EncOut &out, uint32_t max_cols, cudaStream_t s) {
+                      const T1EncOut &out, uint32_t max_cols, cudaStream_t s,
+                      const uint32_t *order, uint32_t *queue) {
   if (!ncb) return;
   const size_t smem = t1_model_smem(max_cols);
   cudaFuncSetAttribute(t1_model_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  t1_model_kernel<<<ncb, kModelThreads, smem, s>>>(work, cbs, ncb, sbs, out);
+  unsigned grid = ncb;
+  if (queue) {
+    // persistent: as many CTAs as fit on the GPU at once
+    int dev = 0, sms = dev::kNumSMs, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, t1_model_kernel, kModelThreads, smem);
+    grid = std::min<unsigned>(ncb, (unsigned)std::max(1, sms * std::max(1, per_sm)));
+    cudaMemsetAsync(queue, 0, sizeof(uint32_t), s);
+  }
+  t1_model_kernel<<<grid, kModelThreads, smem, s>>>(work, cbs, ncb, sbs, out, order, queue);
   const uint32_t rule = mq_lanes_per_warp(ncb);
   uint32_t lanes = rule;
   bool tune = false;
@@ -991,7 +1027,7 @@ void launch_t1_encode(const bwc_float *work, const CbDev *cbs, uint32_t ncb, con
     else
       tune = true;
   }
-  t1_mq_kernel<<<(ncb + lanes - 1) / lanes, kMqThreads, 0, s>>>(cbs, ncb, sbs, out, lanes);
+  t1_mq_kernel<<<(ncb + lanes - 1) / lanes, kMqThreads, 0, s>>>(cbs, ncb, sbs, out, lanes, order);
   if (!tune) return;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
@@ -1000,7 +1036,7 @@ void launch_t1_encode(const bwc_float *work, const CbDev *cbs, uint32_t ncb, con
   uint32_t best_lanes = rule;
   for (uint32_t cand = std::max(1u, rule / 4); cand <= std::min(32u, rule * 4); cand *= 2) {
     cudaEventRecord(e0, s);
-    t1_mq_kernel<<<(ncb + cand - 1) / cand, kMqThreads, 0, s>>>(cbs, ncb, sbs, out, cand);
+    t1_mq_kernel<<<(ncb + cand - 1) / cand, kMqThreads, 0, s>>>(cbs, ncb, sbs, out, cand, order);
     cudaEventRecord(e1, s);
     if (cudaEventSynchronize(e1) != cudaSuccess) break;
     float ms = 0;
