@@ -159,6 +159,7 @@ def load(precision="double"):
         "bwc_b200_last_batch_timings": (C.c_int, [vp, C.c_int]),
         "bwc_b200_set_rate_model": (C.c_int, [vp]),
         "bwc_b200_mq_lanes": (C.c_int, [C.c_uint32]),
+        "bwc_b200_set_transform_tuning": (None, [C.c_int, C.c_int]),
         "bwc_b200_rate_features": (C.c_int, [cp, u8, vp]),
         "bwc_b200_rate_stats": (C.c_int, [cp, u8, vp]),
         "bwc_b200_mlp_forward": (C.c_int, [vp, vp, C.c_uint32, vp]),
@@ -230,6 +231,13 @@ def create_decompression(codec, stream, layer, precision="double"):
 
 def decompress(codec, stream, precision="double"):
     return load(precision).bwc_decompress(codec, stream)
+
+
+def set_transform_tuning(mode=1, zlen=0, precision="double"):
+    """Forward transform path for levels that transform x, y and z: 0 = 3D tile kernel only,
+    1 = z-streaming kernel where x, y >= 48 and z >= 16 (default), 2 = z-streaming kernel
+    wherever x, y, z >= 8; ``zlen`` > 0 fixes its z-chunk length.  Coefficients are identical."""
+    load(precision).bwc_b200_set_transform_tuning(int(mode), int(zlen))
 
 
 def reset_gain_state(precision="double"):

@@ -119,6 +119,14 @@ int    bwc_b200_last_batch_timings(double *out_ms, int n);
  * disables tuning), else the built-in rule.  No counterpart in the reference API. */
 int    bwc_b200_mq_lanes(uint32 ncb);
 
+/* Forward transform path for the levels that transform x, y and z: mode 0 = the 3D tile kernel
+ * only, 1 (default) = the z-streaming kernel where x and y span at least 48 samples and z at
+ * least 16, 2 = the z-streaming kernel wherever x, y and z span at least 8.  zlen > 0 fixes the
+ * streaming kernel's chunk length along z (rounded up to even), 0 = by rule.  Process-wide; set
+ * it between calls.  Both paths give bit-identical coefficients.  No counterpart in the
+ * reference API. */
+void   bwc_b200_set_transform_tuning(int mode, int zlen);
+
 /* Rate-control warm start.  No counterpart in the reference API.
  *
  * The reference's rate control bisects, per quality layer, over a 16-bit log-slope threshold;
