@@ -233,11 +233,11 @@ def decompress(codec, stream, precision="double"):
     return load(precision).bwc_decompress(codec, stream)
 
 
-def set_transform_tuning(mode=1, zlen=0, precision="double"):
+def set_transform_tuning(mode=1, ctas=0, precision="double"):
     """Forward transform path for levels that transform x, y and z: 0 = 3D tile kernel only,
-    1 = z-streaming kernel where x, y >= 48 and z >= 16 (default), 2 = z-streaming kernel
-    wherever x, y, z >= 8; ``zlen`` > 0 fixes its z-chunk length.  Coefficients are identical."""
-    load(precision).bwc_b200_set_transform_tuning(int(mode), int(zlen))
+    1 = z-streaming kernel where it pays (default), 2 = z-streaming kernel wherever x, y, z >= 8;
+    ``ctas`` > 0 fixes the streaming kernel's grid.  Coefficients are identical."""
+    load(precision).bwc_b200_set_transform_tuning(int(mode), int(ctas))
 
 
 def reset_gain_state(precision="double"):

@@ -365,36 +365,42 @@ __global__ void __launch_bounds__(kFusedThreads)
 }
 
 // ---- z-streaming forward pass of one level -------------------------------------------------
-// For levels that transform x, y and z.  A CTA owns a 64 x 64 tile of (x, y) -- a 56 x 56
-// interior plus a 4-sample reflected halo on each side -- and a chunk of z, and streams through
-// the chunk's planes (and 4 reflected or neighbouring planes before and after it) one at a time:
+// For levels that transform x, y and z.  The level is cut into 64 x 64 tiles of (x, y) -- a
+// 56 x 56 interior plus a 4-sample reflected halo on each side -- times pairs of z-planes; each
+// CTA (one per SM) takes an equal share of those (tile, plane pair) units and streams through
+// them, a contiguous run of planes of one tile at a time (with 4 reflected or neighbouring planes
+// before the run and 3 to 4 after it).  Per plane:
 //   x: the tile's rows come from global memory straight into registers, one plane ahead of use;
-//      a warp holds a row as 32 (even, odd) pairs and lifts it with its neighbours fetched by
+//      a warp holds a row as 32 (even, odd) pairs and lifts it with neighbours fetched by
 //      shuffle; the row goes to a shared-memory plane split by row parity (rows of kZP samples);
-//   y: the same warp-wide lifting on columns, each lane now holding a (even row, odd row) pair
-//      of two adjacent columns, read and written back as 16-byte words;
+//   y: the same warp-wide lifting on columns, each lane holding an (even row, odd row) pair of
+//      two adjacent columns, read and written back as 16-byte words;
 //   z: every lane keeps, for each of its points, a window of four planes in registers.  When an
 //      even plane j has arrived, the lifting steps advance at planes j-1, j-2, j-3 and j-4 (the
-//      only steps whose neighbours are complete), after which plane j-4 (low) and j-3 (high) are
-//      final and stored de-interleaved.
+//      only steps whose neighbours are complete), after which planes j-4 (low) and j-3 (high)
+//      are final and stored de-interleaved.
+// The three passes are software-pipelined over a ring of four plane slots: step s lifts plane s
+// along x, plane s-1 along y and (s-2 even) planes s-3, s-2 along z, then one barrier.
 // The arithmetic of every sample is the line lifting of dwt_level_kernel -- the same operands in
 // the same order, rounded the same way -- only the z steps are scheduled as the planes arrive.
 // Shuffles at the warp's ends read the lane's own value: those samples are halo, and a 4-sample
-// halo keeps the interior exact, as for the tile kernel.  Global traffic per plane: one read of
-// the tile (neighbouring tiles' halos mostly hit L2), one write of the interior.
+// halo keeps the interior exact, as for the tile kernel.  Samples a run reads before its first
+// plane (a ring slot or window left by the previous run, or zeros) reach no stored sample.
 constexpr int kZT = 64, kZH = 4, kZI = kZT - 2 * kZH;  // tile extent, halo, interior (x and y)
 constexpr int kZThreads = 512;                           // 16 warps
 constexpr int kZP = kZT + 2;                             // row pitch of a parity plane
-constexpr int kZRing = 3;                                // tile planes held in shared memory
-constexpr size_t kZSmem = (size_t)kZRing * 2 * (kZT / 2) * kZP * sizeof(bwc_float);
+constexpr int kZRing = 4;                                // tile planes held in shared memory
+constexpr int kZPar = (kZT / 2) * kZP, kZSlot = 2 * kZPar;
+constexpr size_t kZSmem = (size_t)kZRing * kZSlot * sizeof(bwc_float);
 
 struct StreamGeom {
   uint32_t ex, ey, ez;        // region extents
   uint32_t lx, ly, lz;        // low-band sizes, (e + 1) / 2
-  uint32_t ntx, nty, nch;     // tiles along x and y, chunks along z
-  uint32_t zlen;              // chunk length (even)
+  uint32_t ntx, nty, npairs;  // tiles along x and y, plane pairs along z
   uint32_t vec;               // rows start on pair boundaries: pair loads allowed
-  uint64_t sy, sz, st;        // buffer strides
+  uint32_t sy, sz;            // buffer strides within a time slice (< 2^31 samples)
+  uint64_t st;                // time-slice stride
+  uint64_t units;             // ntx * nty * time slices * npairs
 };
 
 template <typename T>
@@ -446,164 +452,167 @@ __global__ void __launch_bounds__(kZThreads, 1)
     dwt_stream_fwd_kernel(const bwc_float *__restrict__ src, bwc_float *__restrict__ dst,
                           StreamGeom g) {
   extern __shared__ unsigned char smem_raw[];
-  // ring[slot][parity][row / 2][kZP]
+  // ring[slot][row parity][row / 2][kZP]
   bwc_float *ring = reinterpret_cast<bwc_float *>(smem_raw);
-  constexpr int kSlot = 2 * (kZT / 2) * kZP, kPar = (kZT / 2) * kZP;
-  uint32_t b = blockIdx.x;
-  const uint32_t bx = b % g.ntx;
-  b /= g.ntx;
-  const uint32_t by = b % g.nty;
-  b /= g.nty;
-  const uint32_t bc = b % g.nch;
-  const uint32_t t = b / g.nch;
-  const int x0 = (int)(bx * kZI) - kZH, y0 = (int)(by * kZI) - kZH;   // both even
-  const int zc0 = (int)(bc * g.zlen);
-  const int zc1 = min(zc0 + (int)g.zlen, (int)g.ez);
-  const int jlast = (zc1 + 3) & ~1;   // smallest even plane index >= zc1 + 2
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const bwc_float *sbase = src + (uint64_t)t * g.st;
-  bwc_float *dbase = dst + (uint64_t)t * g.st;
-
-  // zero the ring: the first z step reads a plane slot nothing has written yet
-  for (int i = threadIdx.x; i < kZRing * kSlot; i += kZThreads) ring[i] = (bwc_float)0;
-
-  // this thread's rows (x pass and z pass): r = warp + 16 k, source rows reflected
-  int gy[4];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) gy[k] = reflect(y0 + warp + 16 * k, (int)g.ey);
-  const int xo = x0 + 2 * lane;
-  const bool xin = x0 >= 0 && x0 + kZT <= (int)g.ex;
-  const bool vec = xin && g.vec;
-  const int xa = xin ? xo : reflect(xo, (int)g.ex);
-  const int xb = xin ? xo + 1 : reflect(xo + 1, (int)g.ex);
-
-  auto load_plane = [&](int j, bwc_float (&e)[4], bwc_float (&o)[4]) {
-    const bwc_float *p = sbase + (uint64_t)reflect(j, (int)g.ez) * g.sz;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const bwc_float *row = p + (uint64_t)gy[k] * g.sy;
-      if (vec) {
-        const pair_t v = __ldg(reinterpret_cast<const pair_t *>(row + xa));
-        e[k] = v.x;
-        o[k] = v.y;
-      } else {
-        e[k] = __ldg(row + xa);
-        o[k] = __ldg(row + xb);
-      }
-    }
-  };
-  auto slot_of = [](int j) { return (j + 6) % kZRing; };
-
-  // x pass of one plane: lift the four rows, write them to the plane's ring slot
-  auto x_pass = [&](bwc_float (&e)[4], bwc_float (&o)[4], int slot) {
-    lift_pairs_fwd<4>(e, o);
-    bwc_float *pl = ring + slot * kSlot + (warp & 1) * kPar + (warp >> 1) * kZP + 2 * lane;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      pair_t v;
-      v.x = e[k];
-      v.y = o[k];
-      *reinterpret_cast<pair_t *>(pl + 8 * k * kZP) = v;   // row warp + 16 k
-    }
-  };
-  // y pass: column pairs p = warp and warp + 16, lane = row pair
-  auto y_pass = [&](int slot) {
-    bwc_float *ev = ring + slot * kSlot + lane * kZP + 2 * warp;
-    bwc_float *od = ev + kPar;
-    bwc_float e[4], o[4];
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const pair_t a = *reinterpret_cast<const pair_t *>(ev + 32 * q);
-      const pair_t c = *reinterpret_cast<const pair_t *>(od + 32 * q);
-      e[2 * q] = a.x;
-      e[2 * q + 1] = a.y;
-      o[2 * q] = c.x;
-      o[2 * q + 1] = c.y;
-    }
-    lift_pairs_fwd<4>(e, o);
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      pair_t a, c;
-      a.x = e[2 * q];
-      a.y = e[2 * q + 1];
-      c.x = o[2 * q];
-      c.y = o[2 * q + 1];
-      *reinterpret_cast<pair_t *>(ev + 32 * q) = a;
-      *reinterpret_cast<pair_t *>(od + 32 * q) = c;
-    }
-  };
+  for (int i = threadIdx.x; i < kZRing * kZSlot; i += kZThreads) ring[i] = (bwc_float)0;
+  // this thread's place in a slot: x and z passes (row warp + 16 k, lane's x pair), y pass
+  // (column pairs warp and warp + 16, lane's row pair)
+  const int xoff = (warp & 1) * kZPar + (warp >> 1) * kZP + 2 * lane;
+  const int yoff = lane * kZP + 2 * warp;
+  const int klo = (warp < kZH) ? 1 : 0, khi = (warp >= 16 - kZH) ? 3 : 4;   // interior rows
 
   // z window per point (row k, x parity i): w5 = plane j-5 after step 3, w4 = j-4 after step 2,
-  // w3 = j-3 after step 1, w2 = j-2 as transformed along x and y
+  // w3 = j-3 after step 1, w2 = j-2 as lifted along x and y
   bwc_float w5[4][2], w4[4][2], w3[4][2], w2[4][2];
 #pragma unroll
   for (int k = 0; k < 4; ++k)
 #pragma unroll
     for (int i = 0; i < 2; ++i) w5[k][i] = w4[k][i] = w3[k][i] = w2[k][i] = (bwc_float)0;
-  const int klo = (warp < kZH) ? 1 : 0, khi = (warp >= 16 - kZH) ? 3 : 4;   // interior rows
-  const uint32_t xe = (uint32_t)xo;   // even x of this lane (valid when stored)
-  const bool lane_in = lane >= kZH / 2 && lane < 32 - kZH / 2 && xo >= 0;
+  __syncthreads();   // ring zeroed
 
-  auto z_pass = [&](int j) {
-    const bwc_float *pe = ring + slot_of(j) * kSlot + (warp & 1) * kPar + (warp >> 1) * kZP + 2 * lane;
-    const bwc_float *po = ring + slot_of(j - 1) * kSlot + (warp & 1) * kPar + (warp >> 1) * kZP + 2 * lane;
-    const int ze = j - 4, zo = j - 3;
-    const bool st_e = ze >= zc0 && ze < zc1, st_o = zo >= zc0 && zo < zc1;
-    const uint64_t de = (uint64_t)(ze >= 0 ? ze / 2 : 0) * g.sz;
-    const uint64_t dz = (uint64_t)(g.lz + (zo >= 0 ? zo / 2 : 0)) * g.sz;
+  const uint64_t ubeg = (uint64_t)blockIdx.x * g.units / gridDim.x;
+  const uint64_t uend = (uint64_t)(blockIdx.x + 1) * g.units / gridDim.x;
+  for (uint64_t u = ubeg; u < uend;) {
+    // the run: tile `tile`, plane pairs [p0, p1)
+    const uint64_t tile = u / g.npairs;
+    const uint32_t p0 = (uint32_t)(u % g.npairs);
+    const uint64_t left = uend - u;
+    const uint32_t p1 = (left < (uint64_t)(g.npairs - p0)) ? p0 + (uint32_t)left : g.npairs;
+    u += p1 - p0;
+    const uint32_t bx = (uint32_t)(tile % g.ntx);
+    const uint32_t by = (uint32_t)((tile / g.ntx) % g.nty);
+    const uint64_t t = tile / ((uint64_t)g.ntx * g.nty);
+    const int x0 = (int)(bx * kZI) - kZH, y0 = (int)(by * kZI) - kZH;   // both even
+    const int zc0 = 2 * (int)p0, zc1 = min(2 * (int)p1, (int)g.ez);
+    const int jfirst = zc0 - kZH, jlast = (zc1 + 3) & ~1;   // first / last plane fed (even)
+    const bwc_float *sbase = src + t * g.st;
+    bwc_float *dbase = dst + t * g.st;
+
+    // source offsets of this thread's rows, reflected; destination rows (~0u: not stored)
+    const int xo = x0 + 2 * lane;
+    const bool xin = x0 >= 0 && x0 + kZT <= (int)g.ex;
+    const bool vec = xin && g.vec;
+    const int xa = xin ? xo : reflect(xo, (int)g.ex);
+    const int xb = xin ? xo + 1 : reflect(xo + 1, (int)g.ex);
+    uint32_t lrow[4], srow[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      if (k < klo || k >= khi) continue;
-      const pair_t n0 = *reinterpret_cast<const pair_t *>(pe + 8 * k * kZP);
-      const pair_t n1v = *reinterpret_cast<const pair_t *>(po + 8 * k * kZP);
-      bwc_float out_e[2], out_o[2];
-#pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const bwc_float v0 = i ? n0.y : n0.x;
-        bwc_float v1 = i ? n1v.y : n1v.x;
-        v1 = dev::fadd(v1, dev::fmul(kAlpha, dev::fadd(w2[k][i], v0)));
-        w2[k][i] = dev::fadd(w2[k][i], dev::fmul(kBeta, dev::fadd(w3[k][i], v1)));
-        w3[k][i] = dev::fmul(kKappaH,
-                             dev::fadd(w3[k][i], dev::fmul(kGamma, dev::fadd(w4[k][i], w2[k][i]))));
-        w4[k][i] = dev::fmul(kKappaL,
-                             dev::fadd(w4[k][i], dev::fmul(kDelta, dev::fadd(w5[k][i], w3[k][i]))));
-        out_e[i] = w4[k][i];
-        out_o[i] = w3[k][i];
-        w5[k][i] = w3[k][i];
-        w4[k][i] = w2[k][i];
-        w3[k][i] = v1;
-        w2[k][i] = v0;
-      }
       const int y = y0 + warp + 16 * k;
-      if (lane_in && y < (int)g.ey) {
-        const uint32_t yp = (y & 1) ? g.ly + (uint32_t)y / 2 : (uint32_t)y / 2;
-        bwc_float *row = dbase + (uint64_t)yp * g.sy;
-        const uint32_t xl = xe / 2, xh = g.lx + xe / 2;
-        if (st_e) {
-          if (xe < g.ex) row[de + xl] = out_e[0];
-          if (xe + 1 < g.ex) row[de + xh] = out_e[1];
-        }
-        if (st_o) {
-          if (xe < g.ex) row[dz + xl] = out_o[0];
-          if (xe + 1 < g.ex) row[dz + xh] = out_o[1];
+      lrow[k] = (uint32_t)reflect(y, (int)g.ey) * g.sy;
+      const uint32_t yp = (y & 1) ? g.ly + (uint32_t)y / 2 : (uint32_t)y / 2;
+      srow[k] = (k >= klo && k < khi && y < (int)g.ey) ? yp * g.sy : ~0u;
+    }
+    const uint32_t xe = (uint32_t)xo;
+    const bool lane_in = lane >= kZH / 2 && lane < 32 - kZH / 2;
+    const bool st_l = lane_in && xe < g.ex, st_h = lane_in && xe + 1 < g.ex;
+    const uint32_t xl = xe / 2, xh = g.lx + xe / 2;
+
+    auto load_plane = [&](int j, bwc_float (&e)[4], bwc_float (&o)[4]) {
+      const bwc_float *p = sbase + (uint64_t)((uint32_t)reflect(j, (int)g.ez) * g.sz);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const bwc_float *row = p + lrow[k];
+        if (vec) {
+          const pair_t v = __ldg(reinterpret_cast<const pair_t *>(row + xa));
+          e[k] = v.x;
+          o[k] = v.y;
+        } else {
+          e[k] = __ldg(row + xa);
+          o[k] = __ldg(row + xb);
         }
       }
-    }
-  };
+    };
+    auto x_pass = [&](bwc_float (&e)[4], bwc_float (&o)[4], bwc_float *slot) {
+      lift_pairs_fwd<4>(e, o);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        pair_t v;
+        v.x = e[k];
+        v.y = o[k];
+        *reinterpret_cast<pair_t *>(slot + xoff + 8 * k * kZP) = v;   // row warp + 16 k
+      }
+    };
+    auto y_pass = [&](bwc_float *slot) {
+      bwc_float *ev = slot + yoff;
+      bwc_float *od = ev + kZPar;
+      bwc_float e[4], o[4];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const pair_t a = *reinterpret_cast<const pair_t *>(ev + 32 * q);
+        const pair_t c = *reinterpret_cast<const pair_t *>(od + 32 * q);
+        e[2 * q] = a.x;
+        e[2 * q + 1] = a.y;
+        o[2 * q] = c.x;
+        o[2 * q + 1] = c.y;
+      }
+      lift_pairs_fwd<4>(e, o);
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        pair_t a, c;
+        a.x = e[2 * q];
+        a.y = e[2 * q + 1];
+        c.x = o[2 * q];
+        c.y = o[2 * q + 1];
+        *reinterpret_cast<pair_t *>(ev + 32 * q) = a;
+        *reinterpret_cast<pair_t *>(od + 32 * q) = c;
+      }
+    };
+    // z pass at even plane j: planes j-1 (odd) and j (even) enter the window
+    auto z_pass = [&](int j, const bwc_float *slot_o, const bwc_float *slot_e) {
+      const int ze = j - 4, zo = j - 3;
+      const bool st_e = ze >= zc0 && ze < zc1, st_o = zo >= zc0 && zo < zc1;
+      const uint32_t de = (uint32_t)(ze >> 1) * g.sz;
+      const uint32_t dz = (g.lz + (uint32_t)(zo >> 1)) * g.sz;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (k < klo || k >= khi) continue;
+        const pair_t n0 = *reinterpret_cast<const pair_t *>(slot_e + xoff + 8 * k * kZP);
+        const pair_t n1 = *reinterpret_cast<const pair_t *>(slot_o + xoff + 8 * k * kZP);
+        bwc_float out_e[2], out_o[2];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const bwc_float v0 = i ? n0.y : n0.x;
+          bwc_float v1 = i ? n1.y : n1.x;
+          v1 = dev::fadd(v1, dev::fmul(kAlpha, dev::fadd(w2[k][i], v0)));
+          w2[k][i] = dev::fadd(w2[k][i], dev::fmul(kBeta, dev::fadd(w3[k][i], v1)));
+          w3[k][i] = dev::fmul(
+              kKappaH, dev::fadd(w3[k][i], dev::fmul(kGamma, dev::fadd(w4[k][i], w2[k][i]))));
+          w4[k][i] = dev::fmul(
+              kKappaL, dev::fadd(w4[k][i], dev::fmul(kDelta, dev::fadd(w5[k][i], w3[k][i]))));
+          out_e[i] = w4[k][i];
+          out_o[i] = w3[k][i];
+          w5[k][i] = w3[k][i];
+          w4[k][i] = w2[k][i];
+          w3[k][i] = v1;
+          w2[k][i] = v0;
+        }
+        if (srow[k] != ~0u) {
+          if (st_e) {
+            if (st_l) dbase[de + srow[k] + xl] = out_e[0];
+            if (st_h) dbase[de + srow[k] + xh] = out_e[1];
+          }
+          if (st_o) {
+            if (st_l) dbase[dz + srow[k] + xl] = out_o[0];
+            if (st_h) dbase[dz + srow[k] + xh] = out_o[1];
+          }
+        }
+      }
+    };
 
-  // One register plane: plane j + 1 is requested as soon as the x pass has consumed plane j, so
-  // its loads are in flight during the y and z passes of plane j.
-  bwc_float pe_[4], po_[4];
-  load_plane(zc0 - kZH, pe_, po_);
-  __syncthreads();   // ring zeroed
-  for (int j = zc0 - kZH; j <= jlast; ++j) {
-    const int slot = slot_of(j);
-    x_pass(pe_, po_, slot);
-    if (j < jlast) load_plane(j + 1, pe_, po_);
-    __syncthreads();
-    y_pass(slot);
-    __syncthreads();
-    if ((j & 1) == 0) z_pass(j);
+    // one register plane: plane s + 1 is requested as soon as the x pass has consumed plane s
+    bwc_float pe_[4], po_[4];
+    load_plane(jfirst, pe_, po_);
+    for (int s = jfirst; s <= jlast + 2; ++s) {
+      if (s <= jlast) {
+        x_pass(pe_, po_, ring + (s & 3) * kZSlot);
+        if (s < jlast) load_plane(s + 1, pe_, po_);
+      }
+      if (s - 1 >= jfirst && s - 1 <= jlast) y_pass(ring + ((s - 1) & 3) * kZSlot);
+      if (s - 2 >= jfirst && ((s - 2) & 1) == 0)
+        z_pass(s - 2, ring + ((s - 3) & 3) * kZSlot, ring + ((s - 2) & 3) * kZSlot);
+      __syncthreads();
+    }
   }
 }
 
@@ -631,31 +640,25 @@ void copy_region(const bwc_float *src, bwc_float *dst, const FieldDims &d, const
 }
 
 // Transform path selection (bwc_b200_set_transform_tuning): 0 = tile kernel only, 1 = the
-// z-streaming kernel where x and y span at least 48 samples and z 16, 2 = the z-streaming kernel
-// wherever x, y and z are transformed and span at least 8.  zlen 0 = chunk length by rule.
+// z-streaming kernel where x and y span at least 48 samples and the level gives every SM at
+// least 8 plane pairs, 2 = the z-streaming kernel wherever x, y and z are transformed and span
+// at least 8.  `ctas` > 0 fixes the streaming kernel's grid, 0 = one CTA per SM.
 int g_transform_mode = 1;
-int g_transform_zlen = 0;
+int g_transform_ctas = 0;
 
-// chunk length along z: enough (tile, chunk) CTAs for about four waves of one CTA per SM,
-// chunks of at least 16 planes (each chunk re-reads 7 to 8 planes around it)
-uint32_t stream_zlen(uint64_t items_xy, uint32_t ez) {
-  uint32_t zlen;
-  if (g_transform_zlen > 0) {
-    zlen = (uint32_t)g_transform_zlen;
-  } else {
-    const uint64_t want = 4ull * dev::kNumSMs;
-    const uint64_t nch = std::max<uint64_t>(1, (want + items_xy - 1) / items_xy);
-    zlen = (uint32_t)std::max<uint64_t>(16, (ez + nch - 1) / nch);
-  }
-  zlen = std::min<uint32_t>(zlen, ez);
-  return std::max<uint32_t>(2, (zlen + 1) & ~1u);
+int sm_count() {
+  int dev = 0, n = 0;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+    n = dev::kNumSMs;
+  return n;
 }
 
 bool stream_pass(const bwc_float *src, bwc_float *dst, const FieldDims &d, const uint64_t *e,
                  uint8_t on, cudaStream_t s) {
   if (g_transform_mode == 0 || (on & 7) != 7) return false;
-  const uint64_t mxy = (g_transform_mode == 2) ? 8 : 48, mz = (g_transform_mode == 2) ? 8 : 16;
-  if (e[0] < mxy || e[1] < mxy || e[2] < mz) return false;
+  if (e[0] < 8 || e[1] < 8 || e[2] < 8) return false;
+  if (d.width * d.height * d.depth >= (1ull << 31)) return false;   // 32-bit slice offsets
   StreamGeom g;
   g.ex = (uint32_t)e[0];
   g.ey = (uint32_t)e[1];
@@ -665,16 +668,19 @@ bool stream_pass(const bwc_float *src, bwc_float *dst, const FieldDims &d, const
   g.lz = (g.ez + 1) >> 1;
   g.ntx = (g.ex + kZI - 1) / kZI;
   g.nty = (g.ey + kZI - 1) / kZI;
-  g.zlen = stream_zlen((uint64_t)g.ntx * g.nty * e[3], g.ez);
-  g.nch = (g.ez + g.zlen - 1) / g.zlen;
+  g.npairs = (g.ez + 1) / 2;
+  g.units = (uint64_t)g.ntx * g.nty * e[3] * g.npairs;
   g.vec = (d.width % 2) == 0;
-  g.sy = d.width;
-  g.sz = d.width * d.height;
+  g.sy = (uint32_t)d.width;
+  g.sz = (uint32_t)(d.width * d.height);
   g.st = d.width * d.height * d.depth;
-  const uint64_t blocks = (uint64_t)g.ntx * g.nty * g.nch * e[3];
+  static const int sms = sm_count();
+  const uint64_t grid =
+      std::min<uint64_t>(g.units, g_transform_ctas > 0 ? (uint64_t)g_transform_ctas : (uint64_t)sms);
+  if (g_transform_mode == 1 && (e[0] < 48 || e[1] < 48 || g.units < 8 * grid)) return false;
   cudaFuncSetAttribute(dwt_stream_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)kZSmem);
-  dwt_stream_fwd_kernel<<<(unsigned)blocks, kZThreads, kZSmem, s>>>(src, dst, g);
+  dwt_stream_fwd_kernel<<<(unsigned)grid, kZThreads, kZSmem, s>>>(src, dst, g);
   return true;
 }
 
@@ -755,7 +761,7 @@ void launch_dwt_inverse(bwc_float *work, bwc_float *temp, const FieldDims &dims,
 
 }  // namespace bwcb
 
-extern "C" void bwc_b200_set_transform_tuning(int mode, int zlen) {
+extern "C" void bwc_b200_set_transform_tuning(int mode, int ctas) {
   bwcb::g_transform_mode = (mode < 0 || mode > 2) ? 1 : mode;
-  bwcb::g_transform_zlen = zlen > 0 ? zlen : 0;
+  bwcb::g_transform_ctas = ctas > 0 ? ctas : 0;
 }

@@ -120,12 +120,12 @@ int    bwc_b200_last_batch_timings(double *out_ms, int n);
 int    bwc_b200_mq_lanes(uint32 ncb);
 
 /* Forward transform path for the levels that transform x, y and z: mode 0 = the 3D tile kernel
- * only, 1 (default) = the z-streaming kernel where x and y span at least 48 samples and z at
- * least 16, 2 = the z-streaming kernel wherever x, y and z span at least 8.  zlen > 0 fixes the
- * streaming kernel's chunk length along z (rounded up to even), 0 = by rule.  Process-wide; set
- * it between calls.  Both paths give bit-identical coefficients.  No counterpart in the
- * reference API. */
-void   bwc_b200_set_transform_tuning(int mode, int zlen);
+ * only, 1 (default) = the z-streaming kernel where x and y span at least 48 samples and the
+ * level gives every SM at least 8 plane pairs, 2 = the z-streaming kernel wherever x, y and z
+ * span at least 8.  ctas > 0 fixes the streaming kernel's grid (its CTAs split the level's
+ * (tile, plane pair) units evenly), 0 = one CTA per SM.  Process-wide; set it between calls.
+ * All settings give bit-identical coefficients.  No counterpart in the reference API. */
+void   bwc_b200_set_transform_tuning(int mode, int ctas);
 
 /* Rate-control warm start.  No counterpart in the reference API.
  *

@@ -1,6 +1,7 @@
-"""Forward transform paths against the reference: the z-streaming level kernel (every chunk
-length, odd and even row widths, partial edge tiles, 4D fields, both precisions) and the 3D tile
-kernel must give the reference's coefficients bit for bit, and so the same codestream."""
+"""Forward transform paths against the reference: the z-streaming level kernel (grids from one
+CTA, whose runs cross tiles and time slices, to one per SM; odd and even row widths, partial
+edge tiles, 4D fields, both precisions) and the 3D tile kernel must give the reference's
+coefficients bit for bit, and so the same codestream."""
 import numpy as np
 import pytest
 
@@ -22,7 +23,7 @@ CASES = [
     ("4d", (8, 20, 24, 30), np.float64, "double", (2, 2, 2, 1), (3, 3, 3, 1), "0.25,8"),
     ("4d_single", (6, 12, 16, 18), np.float32, "single", (1, 2, 2, 1), (3, 3, 3, 1), "1,4"),
 ]
-TUNINGS = [(0, 0), (2, 0), (2, 8), (2, 10), (1, 0), (1, 16)]
+TUNINGS = [(0, 0), (2, 0), (2, 1), (2, 7), (2, 50), (1, 0)]   # (mode, CTAs)
 
 
 @pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
