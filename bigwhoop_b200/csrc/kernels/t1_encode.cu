@@ -743,9 +743,8 @@ __global__ void __launch_bounds__(kMqThreads) t1_mq_kernel(const CbDev *__restri
   __shared__ uint32_t ctx_all[dev::kCtxTotal][kMqThreads];
   for (int i = threadIdx.x; i < 94; i += blockDim.x) tbl[i] = dev::c_mq_states[i];
   __syncthreads();
-  // Every lane of the warp stays in the coding loop below (it synchronises warp-wide); lanes
-  // without a codeblock to code (beyond `lanes`, or past the last codeblock) take part with Z = 0.  A codeblock whose symbol stream did not
-  // fit the arena is skipped: the host retries with a larger one.
+  // Lanes beyond `lanes`, past the last codeblock, or whose symbol stream did not fit the arena
+  // (the host retries those with a larger one) have nothing to code.
   const bool lane_used = threadIdx.x < lanes;
   const uint32_t slot = blockIdx.x * lanes + (lane_used ? threadIdx.x : 0u);
   const uint32_t c = (slot < ncb) ? (order ? order[slot] : slot) : ncb;
@@ -770,8 +769,6 @@ __global__ void __launch_bounds__(kMqThreads) t1_mq_kernel(const CbDev *__restri
                    ((uint64_t)(uint8_t)e.t << 32) | (uint64_t)(uint32_t)e.C;
     snaps[2 * p + 1] = (uint64_t)(int64_t)e.L;
   };
-  int p = -1;
-  uint32_t rem = 0;
   // symbols of the current pass, four per word, the next word already in flight
   const uint32_t *src = nullptr;
   uint32_t w0 = 0, w1 = 0;
@@ -792,62 +789,55 @@ __global__ void __launch_bounds__(kMqThreads) t1_mq_kernel(const CbDev *__restri
     --kk;
     return v;
   };
-  bool active = true;
-  uint32_t sym = 0, k = 0, ent = 0;
-  // One flat loop over the codeblock's symbols, kept converged across the warp's 32 codeblocks:
-  // the coding step is predicated, byte transfers run under warp-uniform tests, pass ends (rare,
-  // per lane) are the only divergent branch.  The next symbol's context is fetched while the
-  // current symbol is coded; a context the current symbol just changed overrides it.
-  while (__any_sync(0xffffffffu, active)) {
-    if (active && rem == 0) {
-      if (p >= 0) snapshot(p);
-      for (++p; p < Z && pcount[p] == 0; ++p) snapshot(p);
-      if (p >= Z) {
-        active = false;
-      } else {
-        rem = pcount[p];
-        start_pass(out.symbols + poff[p]);
-        sym = next_symbol();
-        k = sym >> 1;
-        ent = ctx[k * kMqThreads];
+  if (!live) return;
+  // Each lane codes its codeblock on its own: passes in order, the state snapshot at the end of
+  // each.  Per symbol (mq_bit_encode, mq.c:478-556): the common case -- the more probable symbol
+  // with the interval staying >= 0x8000 -- is a subtraction and an addition; the rest updates
+  // the context's state, renormalises, and transfers a byte each time the counter runs out.  The
+  // next symbol's context entry is read while the current symbol is coded; a context the
+  // current symbol just changed overrides it.
+  for (int p = 0; p < Z; ++p) {
+    const uint32_t n = pcount[p];
+    if (n) {
+      start_pass(out.symbols + poff[p]);
+      uint32_t sym = next_symbol();
+      uint32_t ent = ctx[(sym >> 1) * kMqThreads];
+      for (uint32_t i = 1; i <= n; ++i) {
+        uint32_t nsym = 0, nent = 0;
+        if (i < n) {
+          nsym = next_symbol();
+          nent = ctx[(nsym >> 1) * kMqThreads];
+        }
+        const uint32_t pq = ent & 0xFFFF;
+        const uint32_t A1 = e.A - pq;
+        const bool is_mps = ((sym ^ (ent >> 16)) & 1) == 0;
+        if (is_mps && (A1 & 0x8000u)) {
+          e.A = A1;
+          e.C += pq;
+        } else {
+          const bool small = A1 < pq;
+          if (is_mps != small) e.C += pq;
+          e.A = (is_mps == small) ? pq : A1;
+          const uint32_t k = sym >> 1;
+          const uint32_t ne = tbl[is_mps ? (ent >> 17) & 0x7F : (ent >> 24) & 0x7F];
+          ctx[k * kMqThreads] = ne;
+          if ((nsym >> 1) == k) nent = ne;
+          int sh = __clz(e.A) - 16;   // shifts until A >= 0x8000 (at least one)
+          do {
+            const int s1 = min(sh, e.t);
+            e.A <<= s1;
+            e.C <<= s1;
+            e.t -= s1;
+            sh -= s1;
+            if (e.t == 0) mq_transfer(e, bo);
+          } while (sh > 0);
+        }
+        sym = nsym;
+        ent = nent;
       }
     }
-    uint32_t nsym = 0;
-    if (active && rem > 1) nsym = next_symbol();
-    const uint32_t nk = nsym >> 1;
-    const uint32_t nent_spec = ctx[nk * kMqThreads];
-    // mq_bit_encode (mq.c:478-556)
-    const uint32_t pq = ent & 0xFFFF;
-    const uint32_t A1 = e.A - pq;
-    const bool is_mps = ((sym ^ (ent >> 16)) & 1) == 0;
-    const bool small = A1 < pq;
-    const bool keep = !active || (is_mps && A1 >= 0x8000u);   // no renormalisation
-    if (active) {
-      e.C += (keep || (is_mps != small)) ? pq : 0u;
-      e.A = (is_mps == small) ? pq : A1;
-    }
-    const uint32_t nidx = is_mps ? (ent >> 17) & 0x7F : (ent >> 24) & 0x7F;
-    const uint32_t nent = keep ? ent : tbl[nidx];
-    ctx[k * kMqThreads] = nent;
-    int sh = keep ? 0 : (__clz(e.A) - 16);   // shifts until A >= 0x8000
-    // shift up to each due transfer, transfer, continue (at most three transfers)
-    for (int r = 0; r < 3; ++r) {
-      const int s1 = min(sh, e.t);
-      e.A <<= s1;
-      e.C <<= s1;
-      e.t -= s1;
-      sh -= s1;
-      const bool go = (e.t == 0);
-      if (!__any_sync(0xffffffffu, go)) break;
-      if (go) mq_transfer(e, bo);
-    }
-    const bool same = (nk == k);
-    ent = same ? nent : nent_spec;
-    sym = nsym;
-    k = nk;
-    if (active) --rem;
+    snapshot(p);
   }
-  if (!live) return;
   mq_terminate(e, bo);
   for (int i = 0; i < 16; ++i) {
     const int64_t q = (int64_t)e.L + i;
