@@ -769,71 +769,75 @@ __global__ void __launch_bounds__(kMqThreads) t1_mq_kernel(const CbDev *__restri
                    ((uint64_t)(uint8_t)e.t << 32) | (uint64_t)(uint32_t)e.C;
     snaps[2 * p + 1] = (uint64_t)(int64_t)e.L;
   };
-  // symbols of the current pass, four per word, the next word already in flight
-  const uint32_t *src = nullptr;
-  uint32_t w0 = 0, w1 = 0;
-  int kk = 0;
-  auto start_pass = [&](const uint8_t *base) {
-    src = reinterpret_cast<const uint32_t *>(base);
-    w1 = *src++;
-    kk = 0;
-  };
-  auto next_symbol = [&]() -> uint32_t {
-    if (kk == 0) {
-      w0 = w1;
-      w1 = *src++;
-      kk = 4;
-    }
-    const uint32_t v = w0 & 0xFF;
-    w0 >>= 8;
-    --kk;
-    return v;
-  };
   if (!live) return;
   // Each lane codes its codeblock on its own: passes in order, the state snapshot at the end of
-  // each.  Per symbol (mq_bit_encode, mq.c:478-556): the common case -- the more probable symbol
-  // with the interval staying >= 0x8000 -- is a subtraction and an addition; the rest updates
-  // the context's state, renormalises, and transfers a byte each time the counter runs out.  The
-  // next symbol's context entry is read while the current symbol is coded; a context the
-  // current symbol just changed overrides it.
+  // each.  A pass's symbols are read a 32-bit word (four symbols) at a time, two words ahead.
+  // Per symbol (mq_bit_encode, mq.c:478-556): the common case -- the more probable symbol with
+  // the interval staying >= 0x8000 -- is a subtraction and an addition; otherwise the context
+  // moves to its next state, the interval renormalises (a plain shift unless a byte falls due
+  // on the way, mq.c:85-127 then) and the coder state advances.  The next symbol's context
+  // entry is read while the current symbol is coded; a context the current symbol just changed
+  // overrides it.
+  auto code = [&](uint32_t sym, uint32_t ent, uint32_t nk, uint32_t &nent) {
+    const uint32_t pq = ent & 0xFFFF;
+    const uint32_t A1 = e.A - pq;
+    const bool is_mps = ((sym ^ (ent >> 16)) & 1) == 0;
+    if (is_mps && A1 >= 0x8000u) {
+      e.A = A1;
+      e.C += pq;
+      return;
+    }
+    const bool small = A1 < pq;
+    e.C += (is_mps != small) ? pq : 0u;
+    e.A = (is_mps == small) ? pq : A1;
+    const uint32_t k = sym >> 1;
+    const uint32_t ne = tbl[is_mps ? (ent >> 17) & 0x7F : (ent >> 24) & 0x7F];
+    ctx[k * kMqThreads] = ne;
+    if (nk == k) nent = ne;
+    int sh = __clz(e.A) - 16;   // shifts until A >= 0x8000 (at least one)
+    if (sh < e.t) {
+      e.A <<= sh;
+      e.C <<= sh;
+      e.t -= sh;
+      return;
+    }
+    do {   // shift up to each due transfer, transfer, continue
+      const int s1 = min(sh, e.t);
+      e.A <<= s1;
+      e.C <<= s1;
+      e.t -= s1;
+      sh -= s1;
+      if (e.t == 0) mq_transfer(e, bo);
+    } while (sh > 0);
+  };
   for (int p = 0; p < Z; ++p) {
     const uint32_t n = pcount[p];
     if (n) {
-      start_pass(out.symbols + poff[p]);
-      uint32_t sym = next_symbol();
-      uint32_t ent = ctx[(sym >> 1) * kMqThreads];
-      for (uint32_t i = 1; i <= n; ++i) {
-        uint32_t nsym = 0, nent = 0;
-        if (i < n) {
-          nsym = next_symbol();
-          nent = ctx[(nsym >> 1) * kMqThreads];
+      // the pass's chunk holds at least (n + 3) / 4 words
+      const uint32_t *src = reinterpret_cast<const uint32_t *>(out.symbols + poff[p]);
+      const uint32_t nw = (n + 3) >> 2;
+      uint32_t w = src[0];
+      uint32_t wn = (nw > 1) ? src[1] : 0u;
+      uint32_t ent = ctx[((w & 0xFF) >> 1) * kMqThreads];
+      uint32_t left = n;
+      for (uint32_t q = 0; q < nw; ++q) {
+        const uint32_t wc = w;
+        w = wn;
+        wn = (q + 2 < nw) ? src[q + 2] : 0u;
+        const uint32_t cnt = min(left, 4u);
+        left -= cnt;
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+          if ((uint32_t)jj < cnt) {
+            const uint32_t sym = (wc >> (8 * jj)) & 0xFF;
+            const uint32_t nsym = (jj < 3) ? (wc >> (8 * (jj + 1))) & 0xFF : (w & 0xFF);
+            // past the pass's last symbol the next byte is padding: clamp its context index
+            const uint32_t nk = min(nsym >> 1, (uint32_t)dev::kCtxTotal - 1);
+            uint32_t nent = ctx[nk * kMqThreads];
+            code(sym, ent, nk, nent);
+            ent = nent;
+          }
         }
-        const uint32_t pq = ent & 0xFFFF;
-        const uint32_t A1 = e.A - pq;
-        const bool is_mps = ((sym ^ (ent >> 16)) & 1) == 0;
-        if (is_mps && (A1 & 0x8000u)) {
-          e.A = A1;
-          e.C += pq;
-        } else {
-          const bool small = A1 < pq;
-          if (is_mps != small) e.C += pq;
-          e.A = (is_mps == small) ? pq : A1;
-          const uint32_t k = sym >> 1;
-          const uint32_t ne = tbl[is_mps ? (ent >> 17) & 0x7F : (ent >> 24) & 0x7F];
-          ctx[k * kMqThreads] = ne;
-          if ((nsym >> 1) == k) nent = ne;
-          int sh = __clz(e.A) - 16;   // shifts until A >= 0x8000 (at least one)
-          do {
-            const int s1 = min(sh, e.t);
-            e.A <<= s1;
-            e.C <<= s1;
-            e.t -= s1;
-            sh -= s1;
-            if (e.t == 0) mq_transfer(e, bo);
-          } while (sh > 0);
-        }
-        sym = nsym;
-        ent = nent;
       }
     }
     snapshot(p);
