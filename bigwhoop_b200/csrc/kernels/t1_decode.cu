@@ -96,8 +96,16 @@ struct Col {
   uint32_t L, R, U, UL, UR, D, DL, DR;   // sigma | xi << 4 of the neighbours
 };
 
-__device__ __forceinline__ Col neighbours(const uint16_t *state, const Geo &g, uint32_t col) {
-  const uint32_t x = col % g.W, j = (col / g.W) % g.nstripes;
+// stripe-column cursor: col = x + W * (j + nstripes * slice), advanced column by column
+__device__ __forceinline__ void advance(uint32_t &x, uint32_t &j, const Geo &g) {
+  if (++x == g.W) {
+    x = 0;
+    if (++j == g.nstripes) j = 0;
+  }
+}
+
+__device__ __forceinline__ Col neighbours(const uint16_t *state, const Geo &g, uint32_t col,
+                                          uint32_t x, uint32_t j) {
   Col n{0, 0, 0, 0, 0, 0, 0, 0};
   if (x > 0) n.L = state[col - 1] & 0xFF;
   if (x + 1 < g.W) n.R = state[col + 1] & 0xFF;
@@ -145,8 +153,7 @@ __device__ __forceinline__ uint32_t decode_sign(MqDec &d, uint8_t *ctx, uint32_t
 
 __device__ void dec_sp(MqDec &d, uint8_t *ctx, uint16_t *state, bwc_raw *mag, const Geo &g,
                        uint32_t cls, int b) {
-  for (uint32_t col = 0; col < g.ncols; ++col) {
-    const uint32_t j = (col / g.W) % g.nstripes;
+  for (uint32_t col = 0, x = 0, j = 0; col < g.ncols; ++col, advance(x, j, g)) {
     const bool full = j < g.nfull;
     const int lmin = full ? 0 : 4 - (int)g.rem;
     const uint32_t vmask = (0xFu >> lmin) << lmin;
@@ -156,7 +163,7 @@ __device__ void dec_sp(MqDec &d, uint8_t *ctx, uint16_t *state, bwc_raw *mag, co
       state[col] = (uint16_t)(st & 0xF0FFu);
       continue;
     }
-    const Col n = neighbours(state, g, col);
+    const Col n = neighbours(state, g, col, x, j);
     for (int l = 3; l >= lmin; --l) {
       const uint32_t m = 1u << l;
       if (!(sig & m)) {
@@ -178,8 +185,7 @@ __device__ void dec_sp(MqDec &d, uint8_t *ctx, uint16_t *state, bwc_raw *mag, co
 }
 
 __device__ void dec_mr(MqDec &d, uint8_t *ctx, uint16_t *state, bwc_raw *mag, const Geo &g, int b) {
-  for (uint32_t col = 0; col < g.ncols; ++col) {
-    const uint32_t j = (col / g.W) % g.nstripes;
+  for (uint32_t col = 0, x = 0, j = 0; col < g.ncols; ++col, advance(x, j, g)) {
     const bool full = j < g.nfull;
     const int lmin = full ? 0 : 4 - (int)g.rem;
     const uint32_t vmask = (0xFu >> lmin) << lmin;
@@ -188,7 +194,7 @@ __device__ void dec_mr(MqDec &d, uint8_t *ctx, uint16_t *state, bwc_raw *mag, co
     uint32_t delta = (st >> 12) & 0xF;
     const uint32_t todo = sig & ~pi & vmask;
     if (!todo) continue;
-    const Col n = neighbours(state, g, col);
+    const Col n = neighbours(state, g, col, x, j);
     const uint32_t Ls = n.L & 0xF, Rs = n.R & 0xF;
     for (int l = 3; l >= lmin; --l) {
       const uint32_t m = 1u << l;
@@ -213,14 +219,13 @@ __device__ void dec_mr(MqDec &d, uint8_t *ctx, uint16_t *state, bwc_raw *mag, co
 
 __device__ void dec_cu(MqDec &d, uint8_t *ctx, uint16_t *state, bwc_raw *mag, const Geo &g,
                        uint32_t cls, int b) {
-  for (uint32_t col = 0; col < g.ncols; ++col) {
-    const uint32_t j = (col / g.W) % g.nstripes;
+  for (uint32_t col = 0, x = 0, j = 0; col < g.ncols; ++col, advance(x, j, g)) {
     const bool full = j < g.nfull;
     const int lmin = full ? 0 : 4 - (int)g.rem;
     const uint32_t st = state[col];
     uint32_t sig = st & 0xF, xi = (st >> 4) & 0xF;
     const uint32_t pi = (st >> 8) & 0xF;
-    const Col n = neighbours(state, g, col);
+    const Col n = neighbours(state, g, col, x, j);
     uint32_t bits = 0;
     int r = -1;
     if (full) {

@@ -84,9 +84,16 @@ __device__ __forceinline__ uint32_t bit(uint32_t v, int i) {
 
 // Neighbourhood of column `col`: left/upper neighbours from `fin` (post-pass significance
 // estimates) when given, right/lower from `lo` (pre-pass).  Sign bits always from `lo`.
+// stripe-column cursor: col = x + W * (j + nstripes * slice), advanced column by column
+__device__ __forceinline__ void advance(uint32_t &x, uint32_t &j, const Geo &g) {
+  if (++x == g.W) {
+    x = 0;
+    if (++j == g.nstripes) j = 0;
+  }
+}
+
 __device__ __forceinline__ Nbr neighbours(const uint8_t *lo, const uint8_t *fin, const Geo &g,
-                                          uint32_t col) {
-  const uint32_t x = col % g.W, j = (col / g.W) % g.nstripes;
+                                          uint32_t col, uint32_t x, uint32_t j) {
   Nbr n{0, 0, 0, 0, 0, 0, 0, 0};
   auto fl = [&](uint32_t k) -> uint32_t {
     return fin ? ((lo[k] & 0xF0u) | fin[k]) : lo[k];
@@ -443,6 +450,7 @@ __device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ wo
   // ---- coding passes --------------------------------------------------------------------------
   const uint32_t cpt = (g.ncols + kModelThreads - 1) / kModelThreads;
   const uint32_t c0 = min(g.ncols, tid * cpt), c1 = min(g.ncols, c0 + cpt);
+  const uint32_t cx0 = c0 % g.W, cj0 = (c0 / g.W) % g.nstripes;   // cursor at c0
   uint32_t *pcount = out.pass_count + (uint64_t)c * kMaxPasses;
   uint64_t *poff = out.pass_off + (uint64_t)c * kMaxPasses;
   int64_t *dmse = out.dmse + (uint64_t)c * kMaxPasses;
@@ -459,11 +467,10 @@ __device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ wo
         // 4 * ncols + 1 rounds always suffice; the bound only guards against a logic error
         for (uint32_t it = 0; it <= 4 * g.ncols; ++it) {
           int changed = 0;
-          for (uint32_t col = c0; col < c1; ++col) {
-            const uint32_t j = (col / g.W) % g.nstripes;
+          for (uint32_t col = c0, x = cx0, j = cj0; col < c1; ++col, advance(x, j, g)) {
             const bool full = j < g.nfull;
             const int lmin = full ? 0 : 4 - (int)g.rem;
-            const Nbr n = neighbours(lo, fin, g, col);
+            const Nbr n = neighbours(lo, fin, g, col, x, j);
             const uint32_t s = sp_outcome(lo[col] & 0xF, plane[col], n, lmin, full);
             if (s != fin[col]) {
               fin[col] = (uint8_t)s;
@@ -473,11 +480,10 @@ __device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ wo
           if (!__syncthreads_or(changed)) break;
         }
         CountSink cnt;
-        for (uint32_t col = c0; col < c1; ++col) {
-          const uint32_t j = (col / g.W) % g.nstripes;
+        for (uint32_t col = c0, x = cx0, j = cj0; col < c1; ++col, advance(x, j, g)) {
           const bool full = j < g.nfull;
           const int lmin = full ? 0 : 4 - (int)g.rem;
-          const Nbr n = neighbours(lo, fin, g, col);
+          const Nbr n = neighbours(lo, fin, g, col, x, j);
           sp_symbols<CountSink, false>(lo[col] & 0xF, lo[col] >> 4, hi[col] & 0xF, plane[col], n,
                                        lmin, full, sb.cls, cnt, nullptr, planes, g.ncols, col, b);
         }
@@ -486,11 +492,10 @@ __device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ wo
         uint8_t *chunk = reserve(total);
         if (!chunk) return;
         WriteSink ws{chunk + off};
-        for (uint32_t col = c0; col < c1; ++col) {
-          const uint32_t j = (col / g.W) % g.nstripes;
+        for (uint32_t col = c0, x = cx0, j = cj0; col < c1; ++col, advance(x, j, g)) {
           const bool full = j < g.nfull;
           const int lmin = full ? 0 : 4 - (int)g.rem;
-          const Nbr n = neighbours(lo, fin, g, col);
+          const Nbr n = neighbours(lo, fin, g, col, x, j);
           const uint32_t pi = sp_symbols<WriteSink, true>(lo[col] & 0xF, lo[col] >> 4, hi[col] & 0xF,
                                                           plane[col], n, lmin, full, sb.cls, ws,
                                                           &mse, planes, g.ncols, col, b);
@@ -504,13 +509,12 @@ __device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ wo
         }
       } else if (kind == 1) {
         CountSink cnt;
-        for (uint32_t col = c0; col < c1; ++col) {
-          const uint32_t j = (col / g.W) % g.nstripes;
+        for (uint32_t col = c0, x = cx0, j = cj0; col < c1; ++col, advance(x, j, g)) {
           const bool full = j < g.nfull;
           const int lmin = full ? 0 : 4 - (int)g.rem;
           const uint32_t s = lo[col] & 0xF, p = hi[col] & 0xF;
           if (!(s & ~p)) continue;
-          const Nbr n = neighbours(lo, nullptr, g, col);
+          const Nbr n = neighbours(lo, nullptr, g, col, x, j);
           mr_symbols<CountSink, false>(s, p, hi[col] >> 4, plane[col], n, lmin, full, cnt,
                                        nullptr, planes, g.ncols, col, b);
         }
@@ -519,13 +523,12 @@ __device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ wo
         uint8_t *chunk = reserve(total);
         if (!chunk) return;
         WriteSink ws{chunk + off};
-        for (uint32_t col = c0; col < c1; ++col) {
-          const uint32_t j = (col / g.W) % g.nstripes;
+        for (uint32_t col = c0, x = cx0, j = cj0; col < c1; ++col, advance(x, j, g)) {
           const bool full = j < g.nfull;
           const int lmin = full ? 0 : 4 - (int)g.rem;
           const uint32_t s = lo[col] & 0xF, p = hi[col] & 0xF;
           if (!(s & ~p)) continue;
-          const Nbr n = neighbours(lo, nullptr, g, col);
+          const Nbr n = neighbours(lo, nullptr, g, col, x, j);
           const uint32_t dl = mr_symbols<WriteSink, true>(s, p, hi[col] >> 4, plane[col], n, lmin,
                                                           full, ws, &mse, planes, g.ncols, col, b);
           hi[col] = (uint8_t)((hi[col] & 0x0F) | (dl << 4));
@@ -536,19 +539,17 @@ __device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ wo
         }
       } else {
         // cleanup: post-pass significance in closed form
-        for (uint32_t col = c0; col < c1; ++col) {
-          const uint32_t j = (col / g.W) % g.nstripes;
+        for (uint32_t col = c0, x = cx0, j = cj0; col < c1; ++col, advance(x, j, g)) {
           const int lmin = (j < g.nfull) ? 0 : 4 - (int)g.rem;
           const uint32_t vmask = (0xFu >> lmin) << lmin;
           fin[col] = (uint8_t)((lo[col] & 0xF) | (plane[col] & ~hi[col] & vmask));
         }
         __syncthreads();
         CountSink cnt;
-        for (uint32_t col = c0; col < c1; ++col) {
-          const uint32_t j = (col / g.W) % g.nstripes;
+        for (uint32_t col = c0, x = cx0, j = cj0; col < c1; ++col, advance(x, j, g)) {
           const bool full = j < g.nfull;
           const int lmin = full ? 0 : 4 - (int)g.rem;
-          const Nbr n = neighbours(lo, fin, g, col);
+          const Nbr n = neighbours(lo, fin, g, col, x, j);
           cu_symbols<CountSink, false>(lo[col] & 0xF, lo[col] >> 4, hi[col] & 0xF, plane[col], n,
                                        lmin, full, sb.cls, cnt, nullptr, planes, g.ncols, col, b);
         }
@@ -558,11 +559,10 @@ __device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ wo
         uint8_t *chunk = reserve(total);
         if (!chunk) return;
         WriteSink ws{chunk + off};
-        for (uint32_t col = c0; col < c1; ++col) {
-          const uint32_t j = (col / g.W) % g.nstripes;
+        for (uint32_t col = c0, x = cx0, j = cj0; col < c1; ++col, advance(x, j, g)) {
           const bool full = j < g.nfull;
           const int lmin = full ? 0 : 4 - (int)g.rem;
-          const Nbr n = neighbours(lo, fin, g, col);
+          const Nbr n = neighbours(lo, fin, g, col, x, j);
           cu_symbols<WriteSink, true>(lo[col] & 0xF, lo[col] >> 4, hi[col] & 0xF, plane[col], n,
                                       lmin, full, sb.cls, ws, &mse, planes, g.ncols, col, b);
         }
