@@ -467,7 +467,7 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
   if (!cuda_ok(cudaStreamSynchronize(s), "tier-1 download")) return 0;
 
   for (uint64_t i = 0; i < ncb; ++i) {
-    if (hflags[i] & 1u) {
+    if (hflags[i] & (1u | 16u)) {
       warn("o##########################################################o\n"
            "| ERROR: tier-1 output exceeded its codeblock buffer       |\n"
            "o##########################################################o\n");
@@ -1011,7 +1011,7 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
                   s);
   if (!cuda_ok(cudaStreamSynchronize(s), "batch tier-1 download")) return 1;
   for (uint64_t c = 0; c < ncb; ++c)
-    if (hflags[c] & 1u) {
+    if (hflags[c] & (1u | 16u)) {
       warn("o##########################################################o\n"
            "| ERROR: tier-1 output exceeded its codeblock buffer       |\n"
            "o##########################################################o\n");

@@ -40,6 +40,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <type_traits>
 
 #include "bwc_b200.h"
 #include "device_common.cuh"
@@ -166,6 +167,17 @@ struct CountSink {
 struct WriteSink {
   uint8_t *p;
   __device__ __forceinline__ void put(uint32_t ctx, uint32_t b) { *p++ = (uint8_t)((ctx << 1) | b); }
+};
+// symbols held in a thread's shared-memory slice until the pass's offsets are known (a count
+// beyond `cap` marks an overflow: the bytes past it are not kept)
+struct StageSink {
+  uint8_t *p;
+  uint32_t cap;
+  uint32_t n = 0;
+  __device__ __forceinline__ void put(uint32_t ctx, uint32_t b) {
+    if (n < cap) p[n] = (uint8_t)((ctx << 1) | b);
+    ++n;
+  }
 };
 
 // ---- per-column pass logic (tier1.c:962-1146, :1177-1301, :1332-1511) -------------------------
@@ -351,7 +363,8 @@ __device__ __forceinline__ int64_t block_sum64(int64_t v, int64_t *wsum) {
 __device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ work,
                                                 const CbDev *__restrict__ cbs,
                                                 const SbDev *__restrict__ sbs,
-                                                const T1EncOut &out, const uint32_t c) {
+                                                const T1EncOut &out, const uint32_t c,
+                                                const uint32_t stage_cap) {
   extern __shared__ uint8_t smem[];
   __shared__ uint32_t s_wsum[kModelThreads / 32];
   __shared__ int64_t s_wsum64[kModelThreads / 32];
@@ -361,7 +374,10 @@ __device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ wo
   const CbDev cb = cbs[c];
   const SbDev sb = sbs[cb.sb];
   const Geo g = make_geo(cb);
-  uint8_t *lo = smem, *hi = smem + g.ncols, *fin = smem + 2 * g.ncols;
+  // dynamic shared memory: each thread's symbol staging slice (stage_cap bytes, 0 = none),
+  // then the stripe-column states
+  uint8_t *stage = smem + (size_t)tid * stage_cap;
+  uint8_t *lo = smem + (size_t)kModelThreads * stage_cap, *hi = lo + g.ncols, *fin = lo + 2 * g.ncols;
   uint8_t *planes = out.planes + cb.scratch_off;
 
   // ---- quantise -------------------------------------------------------------------------------
@@ -446,6 +462,14 @@ __device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ wo
     __syncthreads();
     return s_ok ? out.symbols + s_base : nullptr;
   };
+  // a thread's staged symbols to their place in the pass's chunk; an overflowed slice (not
+  // possible: a column yields at most 10 symbols a pass, and the slice holds 10 per column
+  // plus 4) marks the codeblock
+  auto unstage = [&](const StageSink &ss, uint8_t *dst) {
+    const uint32_t n = min(ss.n, ss.cap);
+    for (uint32_t i = 0; i < n; ++i) dst[i] = ss.p[i];
+    if (ss.n > ss.cap) out.flags[c] |= 16u;
+  };
 
   // ---- coding passes --------------------------------------------------------------------------
   const uint32_t cpt = (g.ncols + kModelThreads - 1) / kModelThreads;
@@ -479,27 +503,35 @@ __device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ wo
           }
           if (!__syncthreads_or(changed)) break;
         }
-        CountSink cnt;
-        for (uint32_t col = c0, x = cx0, j = cj0; col < c1; ++col, advance(x, j, g)) {
-          const bool full = j < g.nfull;
-          const int lmin = full ? 0 : 4 - (int)g.rem;
-          const Nbr n = neighbours(lo, fin, g, col, x, j);
-          sp_symbols<CountSink, false>(lo[col] & 0xF, lo[col] >> 4, hi[col] & 0xF, plane[col], n,
-                                       lmin, full, sb.cls, cnt, nullptr, planes, g.ncols, col, b);
-        }
+        // the pass's symbols (and, with kDist, its distortion and the visited nibbles)
+        auto sp_run = [&](auto &sink, auto dist) {
+          constexpr bool kDist = decltype(dist)::value;
+          for (uint32_t col = c0, x = cx0, j = cj0; col < c1; ++col, advance(x, j, g)) {
+            const bool full = j < g.nfull;
+            const int lmin = full ? 0 : 4 - (int)g.rem;
+            const Nbr n = neighbours(lo, fin, g, col, x, j);
+            const uint32_t pi = sp_symbols<std::remove_reference_t<decltype(sink)>, kDist>(
+                lo[col] & 0xF, lo[col] >> 4, hi[col] & 0xF, plane[col], n, lmin, full, sb.cls,
+                sink, &mse, planes, g.ncols, col, b);
+            if (kDist) hi[col] = (uint8_t)((hi[col] & 0xF0) | pi);
+          }
+        };
         uint32_t total;
-        const uint32_t off = block_exclusive_scan(cnt.n, &total, s_wsum);
-        uint8_t *chunk = reserve(total);
-        if (!chunk) return;
-        WriteSink ws{chunk + off};
-        for (uint32_t col = c0, x = cx0, j = cj0; col < c1; ++col, advance(x, j, g)) {
-          const bool full = j < g.nfull;
-          const int lmin = full ? 0 : 4 - (int)g.rem;
-          const Nbr n = neighbours(lo, fin, g, col, x, j);
-          const uint32_t pi = sp_symbols<WriteSink, true>(lo[col] & 0xF, lo[col] >> 4, hi[col] & 0xF,
-                                                          plane[col], n, lmin, full, sb.cls, ws,
-                                                          &mse, planes, g.ncols, col, b);
-          hi[col] = (uint8_t)((hi[col] & 0xF0) | pi);
+        if (stage_cap) {
+          StageSink ss{stage, stage_cap};
+          sp_run(ss, std::true_type{});
+          const uint32_t off = block_exclusive_scan(ss.n, &total, s_wsum);
+          uint8_t *chunk = reserve(total);
+          if (!chunk) return;
+          unstage(ss, chunk + off);
+        } else {
+          CountSink cnt;
+          sp_run(cnt, std::false_type{});
+          const uint32_t off = block_exclusive_scan(cnt.n, &total, s_wsum);
+          uint8_t *chunk = reserve(total);
+          if (!chunk) return;
+          WriteSink ws{chunk + off};
+          sp_run(ws, std::true_type{});
         }
         __syncthreads();
         for (uint32_t col = c0; col < c1; ++col) lo[col] = (uint8_t)((lo[col] & 0xF0) | fin[col]);
@@ -508,15 +540,13 @@ __device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ wo
           poff[pass] = s_base;
         }
       } else if (kind == 1) {
+        // one refinement symbol per significant sample not visited by this plane's
+        // significance pass
         CountSink cnt;
         for (uint32_t col = c0, x = cx0, j = cj0; col < c1; ++col, advance(x, j, g)) {
-          const bool full = j < g.nfull;
-          const int lmin = full ? 0 : 4 - (int)g.rem;
-          const uint32_t s = lo[col] & 0xF, p = hi[col] & 0xF;
-          if (!(s & ~p)) continue;
-          const Nbr n = neighbours(lo, nullptr, g, col, x, j);
-          mr_symbols<CountSink, false>(s, p, hi[col] >> 4, plane[col], n, lmin, full, cnt,
-                                       nullptr, planes, g.ncols, col, b);
+          const int lmin = (j < g.nfull) ? 0 : 4 - (int)g.rem;
+          const uint32_t vmask = (0xFu >> lmin) << lmin;
+          cnt.n += __popc((uint32_t)(lo[col] & ~hi[col]) & vmask & 0xFu);
         }
         uint32_t total;
         const uint32_t off = block_exclusive_scan(cnt.n, &total, s_wsum);
@@ -526,10 +556,12 @@ __device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ wo
         for (uint32_t col = c0, x = cx0, j = cj0; col < c1; ++col, advance(x, j, g)) {
           const bool full = j < g.nfull;
           const int lmin = full ? 0 : 4 - (int)g.rem;
-          const uint32_t s = lo[col] & 0xF, p = hi[col] & 0xF;
+          const uint32_t s = lo[col] & 0xF, p = hi[col] & 0xF, dl0 = hi[col] >> 4;
           if (!(s & ~p)) continue;
-          const Nbr n = neighbours(lo, nullptr, g, col, x, j);
-          const uint32_t dl = mr_symbols<WriteSink, true>(s, p, hi[col] >> 4, plane[col], n, lmin,
+          // neighbours only decide the context of a sample's first refinement
+          Nbr n{0, 0, 0, 0, 0, 0, 0, 0};
+          if (s & ~p & ~dl0) n = neighbours(lo, nullptr, g, col, x, j);
+          const uint32_t dl = mr_symbols<WriteSink, true>(s, p, dl0, plane[col], n, lmin,
                                                           full, ws, &mse, planes, g.ncols, col, b);
           hi[col] = (uint8_t)((hi[col] & 0x0F) | (dl << 4));
         }
@@ -545,33 +577,47 @@ __device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ wo
           fin[col] = (uint8_t)((lo[col] & 0xF) | (plane[col] & ~hi[col] & vmask));
         }
         __syncthreads();
-        CountSink cnt;
-        for (uint32_t col = c0, x = cx0, j = cj0; col < c1; ++col, advance(x, j, g)) {
-          const bool full = j < g.nfull;
-          const int lmin = full ? 0 : 4 - (int)g.rem;
-          const Nbr n = neighbours(lo, fin, g, col, x, j);
-          cu_symbols<CountSink, false>(lo[col] & 0xF, lo[col] >> 4, hi[col] & 0xF, plane[col], n,
-                                       lmin, full, sb.cls, cnt, nullptr, planes, g.ncols, col, b);
-        }
-        const uint32_t extra = (sb.erres && tid == kModelThreads - 1) ? 4u : 0u;
+        auto cu_run = [&](auto &sink, auto dist) {
+          constexpr bool kDist = decltype(dist)::value;
+          for (uint32_t col = c0, x = cx0, j = cj0; col < c1; ++col, advance(x, j, g)) {
+            const bool full = j < g.nfull;
+            const int lmin = full ? 0 : 4 - (int)g.rem;
+            const Nbr n = neighbours(lo, fin, g, col, x, j);
+            cu_symbols<std::remove_reference_t<decltype(sink)>, kDist>(
+                lo[col] & 0xF, lo[col] >> 4, hi[col] & 0xF, plane[col], n, lmin, full, sb.cls,
+                sink, &mse, planes, g.ncols, col, b);
+          }
+        };
+        // with error resilience the last thread appends the segmentation symbol after every
+        // bit plane (tier1.c:94-100)
+        const bool seg = sb.erres && tid == kModelThreads - 1;
+        auto segmark = [&](auto &sink) {
+          if (seg) {
+            sink.put(kCtxUni, 1);
+            sink.put(kCtxUni, 0);
+            sink.put(kCtxUni, 1);
+            sink.put(kCtxUni, 0);
+          }
+        };
         uint32_t total;
-        const uint32_t off = block_exclusive_scan(cnt.n + extra, &total, s_wsum);
-        uint8_t *chunk = reserve(total);
-        if (!chunk) return;
-        WriteSink ws{chunk + off};
-        for (uint32_t col = c0, x = cx0, j = cj0; col < c1; ++col, advance(x, j, g)) {
-          const bool full = j < g.nfull;
-          const int lmin = full ? 0 : 4 - (int)g.rem;
-          const Nbr n = neighbours(lo, fin, g, col, x, j);
-          cu_symbols<WriteSink, true>(lo[col] & 0xF, lo[col] >> 4, hi[col] & 0xF, plane[col], n,
-                                      lmin, full, sb.cls, ws, &mse, planes, g.ncols, col, b);
-        }
-        if (extra) {
-          // segmentation symbol after every bit plane (tier1.c:94-100)
-          ws.put(kCtxUni, 1);
-          ws.put(kCtxUni, 0);
-          ws.put(kCtxUni, 1);
-          ws.put(kCtxUni, 0);
+        if (stage_cap) {
+          StageSink ss{stage, stage_cap};
+          cu_run(ss, std::true_type{});
+          segmark(ss);
+          const uint32_t off = block_exclusive_scan(ss.n, &total, s_wsum);
+          uint8_t *chunk = reserve(total);
+          if (!chunk) return;
+          unstage(ss, chunk + off);
+        } else {
+          CountSink cnt;
+          cu_run(cnt, std::false_type{});
+          segmark(cnt);
+          const uint32_t off = block_exclusive_scan(cnt.n, &total, s_wsum);
+          uint8_t *chunk = reserve(total);
+          if (!chunk) return;
+          WriteSink ws{chunk + off};
+          cu_run(ws, std::true_type{});
+          segmark(ws);
         }
         __syncthreads();
         for (uint32_t col = c0; col < c1; ++col) lo[col] = (uint8_t)((lo[col] & 0xF0) | fin[col]);
@@ -594,9 +640,10 @@ __device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ wo
 __global__ void __launch_bounds__(kModelThreads)
     t1_model_kernel(const bwc_float *__restrict__ work, const CbDev *__restrict__ cbs,
                     uint32_t ncb, const SbDev *__restrict__ sbs, T1EncOut out,
-                    const uint32_t *__restrict__ order, uint32_t *queue) {
+                    const uint32_t *__restrict__ order, uint32_t *queue, uint32_t stage_cap) {
   if (!queue) {
-    if (blockIdx.x < ncb) model_codeblock(work, cbs, sbs, out, order ? order[blockIdx.x] : blockIdx.x);
+    if (blockIdx.x < ncb)
+      model_codeblock(work, cbs, sbs, out, order ? order[blockIdx.x] : blockIdx.x, stage_cap);
     return;
   }
   __shared__ uint32_t s_next;
@@ -606,7 +653,7 @@ __global__ void __launch_bounds__(kModelThreads)
     const uint32_t i = s_next;
     __syncthreads();   // every thread has read s_next before it is overwritten
     if (i >= ncb) return;
-    model_codeblock(work, cbs, sbs, out, order ? order[i] : i);
+    model_codeblock(work, cbs, sbs, out, order ? order[i] : i, stage_cap);
     __syncthreads();
   }
 }
@@ -929,7 +976,19 @@ __global__ void __launch_bounds__(kMqThreads) t1_mq_kernel(const CbDev *__restri
 
 }  // namespace
 
-size_t t1_model_smem(uint32_t max_cols) { return (size_t)max_cols * 3; }
+// Per-thread symbol staging slice of the modelling kernel: 10 symbols for each of the thread's
+// columns plus 4 (a pass yields at most 10 per column -- cleanup in run mode: run, two
+// position, one sign, three samples of two -- and 4 segmentation symbols), kept while the
+// whole block's slices fit in 48 KB; 0 (count the symbols first, then write them) above that.
+uint32_t t1_model_stage_cap(uint32_t max_cols) {
+  const uint32_t cpt = (max_cols + kModelThreads - 1) / kModelThreads;
+  const uint32_t cap = (cpt * 10 + 4 + 3) & ~3u;
+  return ((size_t)cap * kModelThreads <= 48 * 1024) ? cap : 0u;
+}
+
+size_t t1_model_smem(uint32_t max_cols) {
+  return (size_t)max_cols * 3 + (size_t)kModelThreads * t1_model_stage_cap(max_cols);
+}
 
 // Codeblocks per MQ warp.  Each lane runs one codeblock's coder, a long dependent chain, so a
 // warp is latency-bound and its lanes' pass ends and byte transfers diverge; fewer lanes per
@@ -1005,7 +1064,8 @@ void launch_t1_encode(const bwc_float *work, const CbDev *cbs, uint32_t ncb, con
     grid = std::min<unsigned>(ncb, (unsigned)std::max(1, sms * std::max(1, per_sm)));
     cudaMemsetAsync(queue, 0, sizeof(uint32_t), s);
   }
-  t1_model_kernel<<<grid, kModelThreads, smem, s>>>(work, cbs, ncb, sbs, out, order, queue);
+  t1_model_kernel<<<grid, kModelThreads, smem, s>>>(work, cbs, ncb, sbs, out, order, queue,
+                                                    t1_model_stage_cap(max_cols));
   const uint32_t rule = mq_lanes_per_warp(ncb);
   uint32_t lanes = rule;
   bool tune = false;

@@ -190,7 +190,7 @@ int    bwc_b200_mlp_train(float *params, const float *X, const float *t, uint32 
  *                   valid; up to 16 zero bytes after them are written too);
  *   status          device, one uint32: 0, or 1 = bytes_cap too small, 2/4 = see the flags of
  *                   the stage dump (not expected), 8 = symbol arena full (not possible within
- *                   the size limit);
+ *                   the size limit), 16 = symbol staging overflow (not possible);
  *   stream          cudaStream_t to run on (NULL = default stream).
  * Results are identical to what bwc_compress computes for the same codeblock.
  *
