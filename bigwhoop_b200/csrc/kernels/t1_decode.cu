@@ -46,6 +46,22 @@ __device__ __forceinline__ void fill_lsb(MqDec &d) {
   }
 }
 
+// Renormalisation (mq.c decoder): shift A and C left until A >= 0x8000, reading the next byte
+// whenever the bit counter t is empty before a shift.  Done in runs of min(shifts left, t)
+// shifts, the counter only empties at a run's end, so the bytes come in at the same points as
+// one shift at a time.
+__device__ __forceinline__ void renorm(MqDec &d) {
+  int sh = __clz(d.A) - 16;   // A in [1, 0x7FFF]: at least one shift
+  do {
+    if (d.t == 0) fill_lsb(d);
+    const int s1 = min(sh, d.t);
+    d.A = (d.A << s1) & 0xFFFF;
+    d.C <<= s1;
+    d.t -= s1;
+    sh -= s1;
+  } while (sh > 0);
+}
+
 __device__ __forceinline__ uint32_t mq_decode(MqDec &d, uint8_t *ctx, int k) {
   const uint32_t ent = dev::c_mq_states[ctx[k]];
   const uint32_t p = ent & 0xFFFF;
@@ -61,12 +77,7 @@ __device__ __forceinline__ uint32_t mq_decode(MqDec &d, uint8_t *ctx, int k) {
       } else {
         ctx[k] = (uint8_t)((ent >> 17) & 0x7F);
       }
-      do {
-        if (d.t == 0) fill_lsb(d);
-        d.A = (d.A << 1) & 0xFFFF;
-        d.C <<= 1;
-        d.t -= 1;
-      } while (!(d.A & 0x8000));
+      renorm(d);
     }
   } else {
     if (d.A < p) {
@@ -76,12 +87,7 @@ __device__ __forceinline__ uint32_t mq_decode(MqDec &d, uint8_t *ctx, int k) {
       ctx[k] = (uint8_t)((ent >> 24) & 0x7F);
     }
     d.A = p;
-    do {
-      if (d.t == 0) fill_lsb(d);
-      d.A = (d.A << 1) & 0xFFFF;
-      d.C <<= 1;
-      d.t -= 1;
-    } while (!(d.A & 0x8000));
+    renorm(d);
   }
   return x;
 }
@@ -194,7 +200,9 @@ __device__ void dec_mr(MqDec &d, uint8_t *ctx, uint16_t *state, bwc_raw *mag, co
     uint32_t delta = (st >> 12) & 0xF;
     const uint32_t todo = sig & ~pi & vmask;
     if (!todo) continue;
-    const Col n = neighbours(state, g, col, x, j);
+    // neighbours only decide the context of a sample's first refinement
+    Col n{0, 0, 0, 0, 0, 0, 0, 0};
+    if (todo & ~delta) n = neighbours(state, g, col, x, j);
     const uint32_t Ls = n.L & 0xF, Rs = n.R & 0xF;
     for (int l = 3; l >= lmin; --l) {
       const uint32_t m = 1u << l;
