@@ -6,10 +6,16 @@
 // (tier2.c:896-1079, :434-711).  The probe results feed a trajectory-dependent search (exact
 // exits on equality, the `tmp` fallback), so the same arithmetic -- including its quirks, such
 // as adding L[0] for a codeblock whose previous layer stopped after one pass -- is kept here.
+#include <unistd.h>
+
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
+#include <functional>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -87,6 +93,118 @@ static void encode_length(BitWriter &bw, Codeblock &cb, int q, uchar estimate) {
   }
 }
 
+extern thread_local bool t_rate_control_in_parallel_fields;
+
+// ---- packet-parallel host loops --------------------------------------------------------------
+// Rate control and packet assembly work packet by packet: a packet's computations touch only its
+// own codeblocks, its precincts' tag trees and the packet itself, and every total they feed is
+// an integer sum.  So those loops run over chunks of packets on a small persistent pool of host
+// threads, with results identical to running them in order.
+//
+// run(n, fn) calls fn(i) for every i in [0, n) on the pool's threads and the calling thread and
+// returns when all are done.  One call at a time: a second concurrent caller, a caller on one of
+// the batch driver's per-field threads (the fields already run in parallel there), or a caller
+// in a process forked after the pool started runs its loop on its own thread.
+class WorkPool {
+ public:
+  static WorkPool &instance() {
+    static WorkPool pool;
+    return pool;
+  }
+  size_t size() const { return workers_.size() + 1; }
+  void run(size_t n, const std::function<void(size_t)> &fn) {
+    std::unique_lock<std::mutex> busy(call_, std::defer_lock);
+    if (n <= 1 || workers_.empty() || t_rate_control_in_parallel_fields || getpid() != pid_ ||
+        !busy.try_lock()) {
+      for (size_t i = 0; i < n; ++i) fn(i);
+      return;
+    }
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      fn_ = &fn;
+      n_ = n;
+      next_.store(0);
+      pending_ = workers_.size();
+      ++gen_;
+    }
+    cv_.notify_all();
+    drain();
+    std::unique_lock<std::mutex> lk(m_);
+    done_.wait(lk, [&] { return pending_ == 0; });
+    fn_ = nullptr;
+  }
+
+ private:
+  WorkPool() : pid_(getpid()) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const unsigned n = std::min(16u, hw ? hw : 1u);
+    for (unsigned i = 1; i < n; ++i) workers_.emplace_back([this] { loop(); });
+  }
+  ~WorkPool() {
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto &t : workers_) t.join();
+  }
+  void drain() {
+    for (size_t i = next_.fetch_add(1); i < n_; i = next_.fetch_add(1)) (*fn_)(i);
+  }
+  void loop() {
+    uint64_t seen = 0;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lk(m_);
+        cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+        if (stop_) return;
+        seen = gen_;
+      }
+      drain();
+      std::lock_guard<std::mutex> lk(m_);
+      if (--pending_ == 0) done_.notify_one();
+    }
+  }
+  const pid_t pid_;
+  std::vector<std::thread> workers_;
+  std::mutex call_, m_;
+  std::condition_variable cv_, done_;
+  const std::function<void(size_t)> *fn_ = nullptr;
+  size_t n_ = 0, pending_ = 0;
+  std::atomic<size_t> next_{0};
+  uint64_t gen_ = 0;
+  bool stop_ = false;
+};
+
+// every packet position of the tile, in the order the codestream and the reference visit them
+struct PacketRef {
+  Parameter *par;
+  Resolution *res;
+  uint32_t p;
+  uint64_t cb_base;   // index of the parameter's first codeblock in tile order
+};
+
+static std::vector<PacketRef> packet_list(Tile &tile) {
+  std::vector<PacketRef> v;
+  uint64_t cb_base = 0;
+  for (Parameter &par : tile.params) {
+    for (Resolution &res : par.res)
+      for (uint64_t p = 0; p < res.nprec; ++p) v.push_back({&par, &res, (uint32_t)p, cb_base});
+    cb_base += par.codeblocks.size();
+  }
+  return v;
+}
+
+// fn(first, last) over contiguous chunks of [0, n), a few chunks per pool thread
+static void for_chunks(size_t n, const std::function<void(size_t, size_t)> &fn) {
+  const size_t chunks = std::min(n, WorkPool::instance().size() * 4);
+  if (chunks <= 1) {
+    if (n) fn(0, n);
+    return;
+  }
+  WorkPool::instance().run(chunks, [&](size_t c) { fn(n * c / chunks, n * (c + 1) / chunks); });
+}
+
 // create_packet (tier2.c:434-711).  est: 0 final, 1 final-size estimate, 2 probe.
 static int64_t create_packet(Parameter &par, Resolution &res, uint32_t p, int q, uchar est) {
   Packet &pk = res.packets[(uint64_t)q * res.nprec + p];
@@ -142,54 +260,64 @@ static int64_t create_packet(Parameter &par, Resolution &res, uint32_t p, int q,
   return 1;
 }
 
-// create_quality_layer (tier2.c:896-1079)
-static int64_t create_quality_layer(bwc_codec *codec, Tile &tile, uint16_t threshold, int q,
-                                    uchar est) {
-  const bwc_gl_ctrl &c = codec->control;
+// create_quality_layer (tier2.c:896-1079), a packet at a time: the truncation points of the
+// packet's codeblocks (every subband's precinct at that position), then the packet's header
+static int64_t quality_layer_packet(const bwc_gl_ctrl &c, const PacketRef &r, uint16_t threshold,
+                                    int q, uchar est) {
+  Parameter &par = *r.par;
+  Resolution &res = *r.res;
+  const uint32_t p = r.p;
   int64_t size = 0;
-  for (Parameter &par : tile.params) {
-    for (Resolution &res : par.res) {
-      for (uint8_t m = 0; m < res.nsub; ++m) {
-        const Subband &sb = par.subbands[res.first_subband + m];
-        for (uint64_t p = 0; p < res.nprec; ++p) {
-          Precinct &pr = par.precincts[sb.first_precinct + p];
-          for (uint64_t k = 0; k < pr.ncb; ++k) {
-            Codeblock &cb = par.codeblocks[pr.first_cb + k];
-            int16_t *cp = cb.cp();
-            int16_t z;
-            for (z = cb.enc.Z; z >= 0 && cb.enc.S[z] < threshold; --z) {
-            }
-            if (z < cp[q - 1]) {
-              cp[q] = cp[q - 1];
-              if (cp[q] == 1) size += (int64_t)cb.enc.L[0];
-            } else {
-              cp[q] = z;
-              if (z > 0) {
-                size += (int64_t)cb.enc.L[z - 1];
-                if (z > 1 && (cp[q - 1] > 0)) size -= (int64_t)cb.enc.L[cp[q - 1] - 1];
-              }
-            }
-            if (cp[q] > cp[q - 1]) res.packets[(uint64_t)q * res.nprec + p].e = 1;
-            if (!est) {
-              if (q == 0) tagtree_set(pr.msbs, k, cb.enc.Kmsbs);
-              if (q + 1 == c.nLayers) {
-                uint8_t l;
-                for (l = 0; (l < c.nLayers) && (cb.cp()[l] == 0); ++l) {
-                }
-                tagtree_set(pr.incl, k, l);
-              }
-            }
-          }
+  for (uint8_t m = 0; m < res.nsub; ++m) {
+    const Subband &sb = par.subbands[res.first_subband + m];
+    Precinct &pr = par.precincts[sb.first_precinct + p];
+    for (uint64_t k = 0; k < pr.ncb; ++k) {
+      Codeblock &cb = par.codeblocks[pr.first_cb + k];
+      int16_t *cp = cb.cp();
+      int16_t z;
+      for (z = cb.enc.Z; z >= 0 && cb.enc.S[z] < threshold; --z) {
+      }
+      if (z < cp[q - 1]) {
+        cp[q] = cp[q - 1];
+        if (cp[q] == 1) size += (int64_t)cb.enc.L[0];
+      } else {
+        cp[q] = z;
+        if (z > 0) {
+          size += (int64_t)cb.enc.L[z - 1];
+          if (z > 1 && (cp[q - 1] > 0)) size -= (int64_t)cb.enc.L[cp[q - 1] - 1];
         }
       }
-      for (uint64_t p = 0; p < res.nprec; ++p) {
-        const int64_t ph = create_packet(par, res, (uint32_t)p, q, est + 1);
-        if (ph < 0) return -1;
-        size += ph;
+      if (cp[q] > cp[q - 1]) res.packets[(uint64_t)q * res.nprec + p].e = 1;
+      if (!est) {
+        if (q == 0) tagtree_set(pr.msbs, k, cb.enc.Kmsbs);
+        if (q + 1 == c.nLayers) {
+          uint8_t l;
+          for (l = 0; (l < c.nLayers) && (cb.cp()[l] == 0); ++l) {
+          }
+          tagtree_set(pr.incl, k, l);
+        }
       }
     }
   }
-  return size;
+  const int64_t ph = create_packet(par, res, p, q, est + 1);
+  return (ph < 0) ? -1 : size + ph;
+}
+
+static int64_t create_quality_layer(bwc_codec *codec, Tile &tile, uint16_t threshold, int q,
+                                    uchar est) {
+  const bwc_gl_ctrl &c = codec->control;
+  const std::vector<PacketRef> pks = packet_list(tile);
+  std::atomic<int64_t> size{0};
+  std::atomic<bool> bad{false};
+  for_chunks(pks.size(), [&](size_t first, size_t last) {
+    int64_t part = 0;
+    for (size_t i = first; i < last; ++i) {
+      const int64_t v = quality_layer_packet(c, pks[i], threshold, q, est);
+      if (v < 0) bad = true; else part += v;
+    }
+    size += part;
+  });
+  return bad ? -1 : size.load();
 }
 
 // ---- rate-control probes ------------------------------------------------------------------
@@ -247,6 +375,7 @@ struct ProbeCb {
   const Codeblock *cb;
   int16_t zprev;            // truncation point of the previous layer
   uint32_t rec_off, rec_n;  // slope records
+  uint32_t pool;            // bit pool holding its tag-tree bits
   uint64_t incl_off, msbs_off;
   uint32_t incl_n, msbs_n;
 };
@@ -263,7 +392,7 @@ struct Probe {
   std::vector<uint32_t> rec_off;   // per codeblock in tile order (parameters concatenated)
   std::vector<ProbeCb> cbs;
   std::vector<ProbePacket> packets;
-  RawBits pool;
+  std::vector<RawBits> pools;   // one per chunk of packets that built them
 };
 
 void build_records(Tile &tile, Probe &pr) {
@@ -282,44 +411,58 @@ void build_records(Tile &tile, Probe &pr) {
   pr.rec_off.push_back((uint32_t)pr.rec_s.size());
 }
 
-// per-layer tables in the order create_quality_layer and create_packet visit codeblocks
+// per-layer tables in the order create_packet visits codeblocks, built a chunk of packets at a
+// time (each chunk has its own bit pool) and concatenated in packet order
 void build_layer(Tile &tile, int q, Probe &pr) {
+  const std::vector<PacketRef> pks = packet_list(tile);
+  const size_t nchunks = std::min(pks.size(), WorkPool::instance().size() * 4);
+  std::vector<std::vector<ProbeCb>> ccbs(nchunks);
+  std::vector<std::vector<ProbePacket>> cpks(nchunks);
+  pr.pools.assign(nchunks, RawBits());
+  WorkPool::instance().run(nchunks, [&](size_t ch) {
+    RawBits &pool = pr.pools[ch];
+    for (size_t i = pks.size() * ch / nchunks; i < pks.size() * (ch + 1) / nchunks; ++i) {
+      const PacketRef &r = pks[i];
+      Parameter &par = *r.par;
+      Resolution &res = *r.res;
+      ProbePacket pk{(uint32_t)ccbs[ch].size(), 0};
+      for (uint8_t m = 0; m < res.nsub; ++m) {
+        const Subband &sb = par.subbands[res.first_subband + m];
+        const Precinct &prc = par.precincts[sb.first_precinct + r.p];
+        for (uint64_t k = 0; k < prc.ncb; ++k) {
+          const uint64_t ci = prc.first_cb + k;
+          Codeblock &cb = par.codeblocks[ci];
+          ProbeCb e{};
+          e.cb = &cb;
+          e.zprev = cb.cp()[q - 1];
+          e.rec_off = pr.rec_off[r.cb_base + ci];
+          e.rec_n = pr.rec_off[r.cb_base + ci + 1] - e.rec_off;
+          e.pool = (uint32_t)ch;
+          if (e.zprev == 0) {
+            e.incl_off = pool.n;
+            tagtree_estimate(prc.incl, pool, (uint32_t)(q + 1), k);
+            e.incl_n = (uint32_t)(pool.n - e.incl_off);
+            e.msbs_off = pool.n;
+            for (uint32_t kk = 1; kk <= cb.enc.Kmsbs + 1u; ++kk)
+              tagtree_estimate(prc.msbs, pool, kk, k);
+            e.msbs_n = (uint32_t)(pool.n - e.msbs_off);
+          }
+          ccbs[ch].push_back(e);
+          pk.count++;
+        }
+      }
+      cpks[ch].push_back(pk);
+    }
+  });
   pr.cbs.clear();
   pr.packets.clear();
-  pr.pool.clear();
-  uint64_t cb_base = 0;
-  for (Parameter &par : tile.params) {
-    for (Resolution &res : par.res) {
-      for (uint64_t p = 0; p < res.nprec; ++p) {
-        ProbePacket pk{(uint32_t)pr.cbs.size(), 0};
-        for (uint8_t m = 0; m < res.nsub; ++m) {
-          const Subband &sb = par.subbands[res.first_subband + m];
-          const Precinct &prc = par.precincts[sb.first_precinct + p];
-          for (uint64_t k = 0; k < prc.ncb; ++k) {
-            const uint64_t ci = prc.first_cb + k;
-            Codeblock &cb = par.codeblocks[ci];
-            ProbeCb e{};
-            e.cb = &cb;
-            e.zprev = cb.cp()[q - 1];
-            e.rec_off = pr.rec_off[cb_base + ci];
-            e.rec_n = pr.rec_off[cb_base + ci + 1] - e.rec_off;
-            if (e.zprev == 0) {
-              e.incl_off = pr.pool.n;
-              tagtree_estimate(prc.incl, pr.pool, (uint32_t)(q + 1), k);
-              e.incl_n = (uint32_t)(pr.pool.n - e.incl_off);
-              e.msbs_off = pr.pool.n;
-              for (uint32_t kk = 1; kk <= cb.enc.Kmsbs + 1u; ++kk)
-                tagtree_estimate(prc.msbs, pr.pool, kk, k);
-              e.msbs_n = (uint32_t)(pr.pool.n - e.msbs_off);
-            }
-            pr.cbs.push_back(e);
-            pk.count++;
-          }
-        }
-        pr.packets.push_back(pk);
-      }
+  for (size_t ch = 0; ch < nchunks; ++ch) {
+    const uint32_t base = (uint32_t)pr.cbs.size();
+    for (ProbePacket pk : cpks[ch]) {
+      pk.first += base;
+      pr.packets.push_back(pk);
     }
-    cb_base += par.codeblocks.size();
+    pr.cbs.insert(pr.cbs.end(), ccbs[ch].begin(), ccbs[ch].end());
   }
 }
 
@@ -333,10 +476,12 @@ inline int16_t truncation_point(const Probe &pr, const ProbeCb &e, uint16_t thre
   return (lo < e.rec_n) ? pr.rec_z[e.rec_off + lo] : (int16_t)-1;
 }
 
-// create_quality_layer(codec, tile, threshold, q, 1) for the tables of layer q
-int64_t probe_layer(const Probe &pr, uint16_t threshold) {
+// create_quality_layer(codec, tile, threshold, q, 1) for the tables of layer q, over packets
+// [first, last)
+int64_t probe_packets(const Probe &pr, uint16_t threshold, size_t first, size_t last) {
   int64_t size = 0;
-  for (const ProbePacket &pk : pr.packets) {
+  for (size_t ip = first; ip < last; ++ip) {
+    const ProbePacket &pk = pr.packets[ip];
     StuffCounter sc;
     sc.put(1, 1);
     bool e = false;
@@ -358,8 +503,8 @@ int64_t probe_layer(const Probe &pr, uint16_t threshold) {
       const int dz = cpq - c.zprev;
       if (dz > 0) e = true;
       if (c.zprev == 0) {
-        sc.put_bits(pr.pool, c.incl_off, c.incl_n);
-        if (cpq) sc.put_bits(pr.pool, c.msbs_off, c.msbs_n);
+        sc.put_bits(pr.pools[c.pool], c.incl_off, c.incl_n);
+        if (cpq) sc.put_bits(pr.pools[c.pool], c.msbs_off, c.msbs_n);
       } else {
         sc.put(dz ? 1 : 0, 1);
       }
@@ -386,6 +531,20 @@ int64_t probe_layer(const Probe &pr, uint16_t threshold) {
     size += e ? (int64_t)sc.finish() : 1;
   }
   return size;
+}
+
+// probe_packets for several thresholds at once: every (threshold, chunk of packets) pair is a
+// task on the pool
+void probe_thresholds(const Probe &pr, const std::vector<uint16_t> &thr, std::vector<int64_t> &out) {
+  const size_t np = pr.packets.size(), nt = thr.size();
+  const size_t chunks = std::max<size_t>(1, std::min(np, WorkPool::instance().size() * 4 / nt + 1));
+  std::vector<int64_t> part(nt * chunks, 0);
+  WorkPool::instance().run(nt * chunks, [&](size_t i) {
+    const size_t k = i / chunks, c = i % chunks;
+    part[i] = probe_packets(pr, thr[k], np * c / chunks, np * (c + 1) / chunks);
+  });
+  out.assign(nt, 0);
+  for (size_t i = 0; i < nt * chunks; ++i) out[i / chunks] += part[i];
 }
 
 }  // namespace
@@ -484,11 +643,8 @@ static uchar create_quality_layers(bwc_codec *codec, Tile &tile) {
   std::vector<float> pred(c.nLayers, -1.f);
   const bool have_pred =
       !check && c.nLayers <= 64 && mlp_predict(tile.rc_features.data(), c.nLayers, pred.data());
-  uint64_t ncb_total = 0;
-  for (const Parameter &par : tile.params) ncb_total += par.codeblocks.size();
   // with no spare threads the prediction is recorded but probes are evaluated on demand
   const bool speculate = have_pred && !t_rate_control_in_parallel_fields;
-  const bool parallel = speculate && ncb_total >= 256;
   for (uint8_t l = 0; l < c.nLayers; ++l) {
     uint16_t slope;
     int probes = 0, rounds = 0;
@@ -520,16 +676,8 @@ static uchar create_quality_layers(bwc_codec *codec, Tile &tile) {
             todo = predicted_path(st, pslope, target - est_tile - (int64_t)header_size);
             if (todo.empty() || todo[0] != s) todo.insert(todo.begin(), s);
           }
-          std::vector<int64_t> res(todo.size());
-          if (parallel && todo.size() > 1) {
-            std::vector<std::thread> th;
-            for (size_t k = 1; k < todo.size(); ++k)
-              th.emplace_back([&, k]() { res[k] = probe_layer(probe, todo[k]); });
-            res[0] = probe_layer(probe, todo[0]);
-            for (auto &t : th) t.join();
-          } else {
-            for (size_t k = 0; k < todo.size(); ++k) res[k] = probe_layer(probe, todo[k]);
-          }
+          std::vector<int64_t> res;
+          probe_thresholds(probe, todo, res);
           for (size_t k = 0; k < todo.size(); ++k) known.emplace_back(todo[k], res[k]);
           ++rounds;
           e = res[0];
@@ -573,25 +721,28 @@ static uchar create_quality_layers(bwc_codec *codec, Tile &tile) {
 // coding state is cleared as in the reference.
 static uchar create_packets(bwc_codec *codec, Tile &tile) {
   const bwc_gl_ctrl &c = codec->control;
-  for (Parameter &par : tile.params) {
-    for (Resolution &res : par.res) {
-      for (uint64_t p = 0; p < res.nprec; ++p) {
-        for (uint8_t l = 0; l < c.nLayers; ++l)
-          if (create_packet(par, res, (uint32_t)p, l, 0) < 0) return 1;
-        // the reference clears each codeblock's coding state once its packets exist
-        for (uint8_t m = 0; m < res.nsub; ++m) {
-          const Subband &sb = par.subbands[res.first_subband + m];
-          const Precinct &pr = par.precincts[sb.first_precinct + p];
-          for (uint64_t k = 0; k < pr.ncb; ++k) {
-            Codeblock &cb = par.codeblocks[pr.first_cb + k];
-            cb.enc = CodedBlock();
-            for (int l = 0; l < c.nLayers; ++l) cb.cp()[l] = 0;
-          }
+  const std::vector<PacketRef> pks = packet_list(tile);
+  std::atomic<bool> bad{false};
+  for_chunks(pks.size(), [&](size_t first, size_t last) {
+    for (size_t i = first; i < last; ++i) {
+      Parameter &par = *pks[i].par;
+      Resolution &res = *pks[i].res;
+      const uint32_t p = pks[i].p;
+      for (uint8_t l = 0; l < c.nLayers; ++l)
+        if (create_packet(par, res, p, l, 0) < 0) bad = true;
+      // the reference clears each codeblock's coding state once its packets exist
+      for (uint8_t m = 0; m < res.nsub; ++m) {
+        const Subband &sb = par.subbands[res.first_subband + m];
+        const Precinct &pr = par.precincts[sb.first_precinct + p];
+        for (uint64_t k = 0; k < pr.ncb; ++k) {
+          Codeblock &cb = par.codeblocks[pr.first_cb + k];
+          cb.enc = CodedBlock();
+          for (int l = 0; l < c.nLayers; ++l) cb.cp()[l] = 0;
         }
       }
     }
-  }
-  return 0;
+  });
+  return bad ? 1 : 0;
 }
 
 uchar t2_encode(bwc_codec *codec, Tile &tile) {
