@@ -330,23 +330,22 @@ static int64_t create_quality_layer(bwc_codec *codec, Tile &tile, uint16_t thres
 
 namespace {
 
-// byte count of a bit string written with BitWriter::emit and BitWriter::flush
+// byte count of a bit string written with BitWriter::emit and BitWriter::flush: bytes of 8
+// bits, except that a byte after 0xFF holds 7 (its top bit is the stuffed 0); a string ending
+// right after 0xFF still gets that next byte
 struct StuffCounter {
-  uint32_t T = 0;
-  int t = 8;
+  uint64_t acc = 0;   // pending bits (the low `nacc`)
+  int nacc = 0;
+  int w = 8;          // width of the byte being filled
   uint64_t bytes = 0;
-  void put(uint64_t v, int n) {   // the n (<= 64) low bits of v, most significant first
-    while (n > 0) {
-      const int k = n < t ? n : t;
-      const uint32_t chunk = (uint32_t)(v >> (n - k)) & ((1u << k) - 1u);
-      T |= chunk << (t - k);
-      t -= k;
-      n -= k;
-      if (t == 0) {
-        bytes++;
-        t = (T == 0xFF) ? 7 : 8;
-        T = 0;
-      }
+  void put(uint64_t v, int n) {   // the n (<= 56) low bits of v, most significant first
+    acc = (acc << n) | (v & ((1ull << n) - 1));
+    nacc += n;
+    while (nacc >= w) {
+      nacc -= w;
+      const uint32_t byte = (uint32_t)(acc >> nacc) & ((1u << w) - 1);
+      bytes++;
+      w = (w == 8 && byte == 0xFF) ? 7 : 8;
     }
   }
   void put_bits(const RawBits &rb, uint64_t off, uint64_t n) {
@@ -355,45 +354,73 @@ struct StuffCounter {
       uint64_t m = 64 - b;
       if (m > n) m = n;
       if (m > 56) m = 56;
-      const uint64_t v = (rb.words[off >> 6] << b) >> (64 - m);
-      put(v, (int)m);
+      put((rb.words[off >> 6] << b) >> (64 - m), (int)m);
       off += m;
       n -= m;
     }
   }
-  void put_ones(int n) {
-    while (n > 0) {
-      const int m = n < 32 ? n : 32;
-      put((1ull << m) - 1, m);
-      n -= m;
-    }
-  }
-  uint64_t finish() const { return bytes + (t != 8 ? 1 : 0); }
+  uint64_t finish() const { return bytes + ((nacc > 0 || w == 7) ? 1 : 0); }
 };
 
+// what a probe reads of a codeblock, kept together (the codeblocks' own records are large and
+// scattered: reading them per probe is cache-miss bound)
 struct ProbeCb {
-  const Codeblock *cb;
   int16_t zprev;            // truncation point of the previous layer
+  uint16_t beta_est;        // length-code state of the estimates
   uint32_t rec_off, rec_n;  // slope records
   uint32_t pool;            // bit pool holding its tag-tree bits
+  uint64_t L0, Lprev;       // L[0] and L[zprev - 1] (0 where they do not exist)
   uint64_t incl_off, msbs_off;
   uint32_t incl_n, msbs_n;
 };
 
 struct ProbePacket {
   uint32_t first, count;
+  uint32_t piece0, npieces;   // its pieces (runs of at most kPieceCbs codeblocks)
 };
+
+// a run of codeblocks of one packet, the unit of parallel work
+struct ProbePiece {
+  uint32_t packet, first, count;   // codeblocks [first, first + count) of pr.cbs
+};
+constexpr uint32_t kPieceCbs = 512;
 
 struct Probe {
   // right-to-left slope records of every codeblock: z in decreasing order with strictly
   // increasing S; max{z : S[z] >= t} is the first record whose S >= t
   std::vector<uint16_t> rec_s;
   std::vector<int16_t> rec_z;
+  std::vector<uint64_t> rec_L;     // L[z - 1] of the record's z (0 for z = 0)
   std::vector<uint32_t> rec_off;   // per codeblock in tile order (parameters concatenated)
   std::vector<ProbeCb> cbs;
   std::vector<ProbePacket> packets;
-  std::vector<RawBits> pools;   // one per chunk of packets that built them
+  std::vector<ProbePiece> pieces;
+  std::vector<RawBits> pools;   // tag-tree bits, one pool per piece
 };
+
+// appending to a bit string, most significant bit first
+static void bits_append(RawBits &rb, uint64_t v, int n) {   // the n (<= 57) low bits of v
+  while (n > 0) {
+    const int used = (int)(rb.n & 63);
+    if (used == 0) rb.words.push_back(0);
+    const int k = std::min(n, 64 - used);
+    const uint64_t chunk = (v >> (n - k)) & ((k == 64) ? ~0ull : ((1ull << k) - 1));
+    rb.words.back() |= chunk << (64 - used - k);
+    rb.n += (uint64_t)k;
+    n -= k;
+  }
+}
+static void bits_append_range(RawBits &rb, const RawBits &src, uint64_t off, uint64_t n) {
+  while (n) {
+    const uint64_t b = off & 63;
+    uint64_t m = 64 - b;
+    if (m > n) m = n;
+    if (m > 56) m = 56;
+    bits_append(rb, (src.words[off >> 6] << b) >> (64 - m), (int)m);
+    off += m;
+    n -= m;
+  }
+}
 
 void build_records(Tile &tile, Probe &pr) {
   for (Parameter &par : tile.params)
@@ -405,146 +432,178 @@ void build_records(Tile &tile, Probe &pr) {
           best = cb.enc.S[z];
           pr.rec_s.push_back(cb.enc.S[z]);
           pr.rec_z.push_back((int16_t)z);
+          pr.rec_L.push_back(z > 0 ? cb.enc.L[z - 1] : 0);
         }
       }
     }
   pr.rec_off.push_back((uint32_t)pr.rec_s.size());
 }
 
-// per-layer tables in the order create_packet visits codeblocks, built a chunk of packets at a
-// time (each chunk has its own bit pool) and concatenated in packet order
+// per-layer tables in the order create_packet visits codeblocks: the packets' codeblocks are
+// laid out first, then pieces of at most kPieceCbs codeblocks are filled in parallel, each
+// with its own pool of tag-tree bits (tag-tree estimates only read the trees)
 void build_layer(Tile &tile, int q, Probe &pr) {
   const std::vector<PacketRef> pks = packet_list(tile);
-  const size_t nchunks = std::min(pks.size(), WorkPool::instance().size() * 4);
-  std::vector<std::vector<ProbeCb>> ccbs(nchunks);
-  std::vector<std::vector<ProbePacket>> cpks(nchunks);
-  pr.pools.assign(nchunks, RawBits());
-  WorkPool::instance().run(nchunks, [&](size_t ch) {
-    RawBits &pool = pr.pools[ch];
-    for (size_t i = pks.size() * ch / nchunks; i < pks.size() * (ch + 1) / nchunks; ++i) {
-      const PacketRef &r = pks[i];
-      Parameter &par = *r.par;
-      Resolution &res = *r.res;
-      ProbePacket pk{(uint32_t)ccbs[ch].size(), 0};
-      for (uint8_t m = 0; m < res.nsub; ++m) {
-        const Subband &sb = par.subbands[res.first_subband + m];
-        const Precinct &prc = par.precincts[sb.first_precinct + r.p];
-        for (uint64_t k = 0; k < prc.ncb; ++k) {
-          const uint64_t ci = prc.first_cb + k;
-          Codeblock &cb = par.codeblocks[ci];
-          ProbeCb e{};
-          e.cb = &cb;
-          e.zprev = cb.cp()[q - 1];
-          e.rec_off = pr.rec_off[r.cb_base + ci];
-          e.rec_n = pr.rec_off[r.cb_base + ci + 1] - e.rec_off;
-          e.pool = (uint32_t)ch;
-          if (e.zprev == 0) {
-            e.incl_off = pool.n;
-            tagtree_estimate(prc.incl, pool, (uint32_t)(q + 1), k);
-            e.incl_n = (uint32_t)(pool.n - e.incl_off);
-            e.msbs_off = pool.n;
-            for (uint32_t kk = 1; kk <= cb.enc.Kmsbs + 1u; ++kk)
-              tagtree_estimate(prc.msbs, pool, kk, k);
-            e.msbs_n = (uint32_t)(pool.n - e.msbs_off);
-          }
-          ccbs[ch].push_back(e);
-          pk.count++;
+  pr.packets.clear();
+  pr.pieces.clear();
+  uint32_t ncb = 0;
+  for (uint32_t i = 0; i < (uint32_t)pks.size(); ++i) {
+    const PacketRef &r = pks[i];
+    uint32_t count = 0;
+    for (uint8_t m = 0; m < r.res->nsub; ++m) {
+      const Subband &sb = r.par->subbands[r.res->first_subband + m];
+      count += (uint32_t)r.par->precincts[sb.first_precinct + r.p].ncb;
+    }
+    ProbePacket pk{ncb, count, (uint32_t)pr.pieces.size(), 0};
+    for (uint32_t b = 0; b < count; b += kPieceCbs) {
+      pr.pieces.push_back({i, ncb + b, std::min(kPieceCbs, count - b)});
+      pk.npieces++;
+    }
+    pr.packets.push_back(pk);
+    ncb += count;
+  }
+  pr.cbs.assign(ncb, ProbeCb{});
+  pr.pools.resize(pr.pieces.size());
+  WorkPool::instance().run(pr.pieces.size(), [&](size_t ip) {
+    const ProbePiece &pc = pr.pieces[ip];
+    const PacketRef &r = pks[pc.packet];
+    Parameter &par = *r.par;
+    Resolution &res = *r.res;
+    RawBits &pool = pr.pools[ip];
+    pool.clear();
+    // codeblock positions [lo, hi) within the packet, walked subband by subband
+    const uint32_t lo = pc.first - pr.packets[pc.packet].first, hi = lo + pc.count;
+    uint32_t pos = 0;
+    for (uint8_t m = 0; m < res.nsub && pos < hi; ++m) {
+      const Subband &sb = par.subbands[res.first_subband + m];
+      const Precinct &prc = par.precincts[sb.first_precinct + r.p];
+      for (uint64_t k = 0; k < prc.ncb; ++k, ++pos) {
+        if (pos < lo || pos >= hi) continue;
+        const uint64_t ci = prc.first_cb + k;
+        Codeblock &cb = par.codeblocks[ci];
+        ProbeCb &e = pr.cbs[pr.packets[pc.packet].first + pos];
+        e.zprev = cb.cp()[q - 1];
+        e.beta_est = cb.beta_est;
+        e.L0 = cb.enc.Z > 0 ? cb.enc.L[0] : 0;
+        e.Lprev = e.zprev > 0 ? cb.enc.L[e.zprev - 1] : 0;
+        e.rec_off = pr.rec_off[r.cb_base + ci];
+        e.rec_n = pr.rec_off[r.cb_base + ci + 1] - e.rec_off;
+        e.pool = (uint32_t)ip;
+        if (e.zprev == 0) {
+          e.incl_off = pool.n;
+          tagtree_estimate(prc.incl, pool, (uint32_t)(q + 1), k);
+          e.incl_n = (uint32_t)(pool.n - e.incl_off);
+          e.msbs_off = pool.n;
+          for (uint32_t kk = 1; kk <= cb.enc.Kmsbs + 1u; ++kk)
+            tagtree_estimate(prc.msbs, pool, kk, k);
+          e.msbs_n = (uint32_t)(pool.n - e.msbs_off);
         }
       }
-      cpks[ch].push_back(pk);
     }
   });
-  pr.cbs.clear();
-  pr.packets.clear();
-  for (size_t ch = 0; ch < nchunks; ++ch) {
-    const uint32_t base = (uint32_t)pr.cbs.size();
-    for (ProbePacket pk : cpks[ch]) {
-      pk.first += base;
-      pr.packets.push_back(pk);
-    }
-    pr.cbs.insert(pr.cbs.end(), ccbs[ch].begin(), ccbs[ch].end());
-  }
 }
 
-inline int16_t truncation_point(const Probe &pr, const ProbeCb &e, uint16_t threshold) {
-  uint32_t lo = 0, hi = e.rec_n;   // first record with S >= threshold
+// index (in the tables) of the codeblock's first record with S >= threshold, or ~0u
+inline uint32_t truncation_record(const Probe &pr, const ProbeCb &e, uint16_t threshold) {
+  uint32_t lo = 0, hi = e.rec_n;
   const uint16_t *s = pr.rec_s.data() + e.rec_off;
   while (lo < hi) {
     const uint32_t mid = (lo + hi) >> 1;
     if (s[mid] >= threshold) hi = mid; else lo = mid + 1;
   }
-  return (lo < e.rec_n) ? pr.rec_z[e.rec_off + lo] : (int16_t)-1;
+  return (lo < e.rec_n) ? e.rec_off + lo : ~0u;
 }
 
-// create_quality_layer(codec, tile, threshold, q, 1) for the tables of layer q, over packets
-// [first, last)
-int64_t probe_packets(const Probe &pr, uint16_t threshold, size_t first, size_t last) {
-  int64_t size = 0;
-  for (size_t ip = first; ip < last; ++ip) {
-    const ProbePacket &pk = pr.packets[ip];
-    StuffCounter sc;
-    sc.put(1, 1);
-    bool e = false;
-    for (uint32_t i = pk.first; i < pk.first + pk.count; ++i) {
-      const ProbeCb &c = pr.cbs[i];
-      const CodedBlock &enc = c.cb->enc;
-      const int16_t z = truncation_point(pr, c, threshold);
-      int16_t cpq;
-      if (z < c.zprev) {
-        cpq = c.zprev;
-        if (cpq == 1) size += (int64_t)enc.L[0];
-      } else {
-        cpq = z;
-        if (z > 0) {
-          size += (int64_t)enc.L[z - 1];
-          if (z > 1 && c.zprev > 0) size -= (int64_t)enc.L[c.zprev - 1];
-        }
+// One piece under one threshold: the body bytes its codeblocks add, whether any is included
+// further (the packet's `e`), and its codeblocks' header bits in order.
+struct PieceResult {
+  int64_t body = 0;
+  bool e = false;
+  RawBits hdr;
+};
+
+void probe_piece(const Probe &pr, uint16_t threshold, const ProbePiece &pc, PieceResult &out) {
+  out.body = 0;
+  out.e = false;
+  out.hdr.clear();
+  RawBits &hb = out.hdr;
+  for (uint32_t i = pc.first; i < pc.first + pc.count; ++i) {
+    const ProbeCb &c = pr.cbs[i];
+    const uint32_t r = truncation_record(pr, c, threshold);
+    const int16_t z = (r != ~0u) ? pr.rec_z[r] : (int16_t)-1;
+    const uint64_t Lz = (r != ~0u) ? pr.rec_L[r] : 0;   // L[z - 1]
+    int16_t cpq;
+    if (z < c.zprev) {
+      cpq = c.zprev;
+      if (cpq == 1) out.body += (int64_t)c.L0;
+    } else {
+      cpq = z;
+      if (z > 0) {
+        out.body += (int64_t)Lz;
+        if (z > 1 && c.zprev > 0) out.body -= (int64_t)c.Lprev;
       }
-      const int dz = cpq - c.zprev;
-      if (dz > 0) e = true;
-      if (c.zprev == 0) {
-        sc.put_bits(pr.pools[c.pool], c.incl_off, c.incl_n);
-        if (cpq) sc.put_bits(pr.pools[c.pool], c.msbs_off, c.msbs_n);
-      } else {
-        sc.put(dz ? 1 : 0, 1);
-      }
-      if (!dz) continue;
-      // encode_delta_z
-      if (dz == 1) sc.put(0, 1);
-      else if (dz == 2) sc.put(2, 2);
-      else if (dz < 6) sc.put(12u | (uint32_t)(dz - 3), 4);
-      else if (dz < 37) sc.put((15u << 5) | (uint32_t)(dz - 6), 9);
-      else if (dz < 293) sc.put((511u << 8) | (uint32_t)(dz - 37), 17);
-      // encode_length with the estimate state
-      const int16_t z_curr = cpq - 1, z_prev = c.zprev - 1;
-      const uint16_t beta = c.cb->beta_est;
-      uint16_t max_beta = beta;
-      const uint32_t L = (uint32_t)(enc.L[z_curr] - ((z_prev >= 0) ? enc.L[z_prev] : 0));
-      const uint16_t cp_bits = ilog2_u16((uint64_t)(z_curr - z_prev));
-      const int32_t L_bits = (int32_t)ilog2_u16(L) + 1 - cp_bits;
-      max_beta = (max_beta < L_bits) ? (uint16_t)L_bits : max_beta;
-      sc.put_ones(max_beta - beta);
-      sc.put(0, 1);
-      const int sh = max_beta + cp_bits - 1;
-      if (sh >= 0 && sh < 31) sc.put(L & (uint32_t)((2ull << sh) - 1), sh + 1);
     }
-    size += e ? (int64_t)sc.finish() : 1;
+    const int dz = cpq - c.zprev;
+    if (dz > 0) out.e = true;
+    if (c.zprev == 0) {
+      bits_append_range(hb, pr.pools[c.pool], c.incl_off, c.incl_n);
+      if (cpq) bits_append_range(hb, pr.pools[c.pool], c.msbs_off, c.msbs_n);
+    } else {
+      bits_append(hb, dz ? 1 : 0, 1);
+    }
+    if (!dz) continue;
+    // encode_delta_z
+    if (dz == 1) bits_append(hb, 0, 1);
+    else if (dz == 2) bits_append(hb, 2, 2);
+    else if (dz < 6) bits_append(hb, 12u | (uint32_t)(dz - 3), 4);
+    else if (dz < 37) bits_append(hb, (15u << 5) | (uint32_t)(dz - 6), 9);
+    else if (dz < 293) bits_append(hb, (511u << 8) | (uint32_t)(dz - 37), 17);
+    // encode_length with the estimate state
+    // here cpq = z > zprev: L[cpq - 1] is the record's, L[zprev - 1] the previous layer's
+    const int16_t z_curr = cpq - 1, z_prev = c.zprev - 1;
+    const uint16_t beta = c.beta_est;
+    uint16_t max_beta = beta;
+    const uint32_t L = (uint32_t)(Lz - ((z_prev >= 0) ? c.Lprev : 0));
+    const uint16_t cp_bits = ilog2_u16((uint64_t)(z_curr - z_prev));
+    const int32_t L_bits = (int32_t)ilog2_u16(L) + 1 - cp_bits;
+    max_beta = (max_beta < L_bits) ? (uint16_t)L_bits : max_beta;
+    for (int n1 = max_beta - beta; n1 > 0; n1 -= 32) {
+      const int m = n1 < 32 ? n1 : 32;
+      bits_append(hb, (1ull << m) - 1, m);
+    }
+    bits_append(hb, 0, 1);
+    const int sh = max_beta + cp_bits - 1;
+    if (sh >= 0 && sh < 31) bits_append(hb, L & (uint32_t)((2ull << sh) - 1), sh + 1);
   }
-  return size;
 }
 
-// probe_packets for several thresholds at once: every (threshold, chunk of packets) pair is a
-// task on the pool
+// create_quality_layer(codec, tile, threshold, q, 1) for the tables of layer q, for several
+// thresholds at once: every (threshold, piece) pair is a task on the pool, then every
+// threshold's packets are sized (a packet header: a 1 bit, its pieces' bits, byte stuffing;
+// an empty packet: one byte) as a task of its own
 void probe_thresholds(const Probe &pr, const std::vector<uint16_t> &thr, std::vector<int64_t> &out) {
-  const size_t np = pr.packets.size(), nt = thr.size();
-  const size_t chunks = std::max<size_t>(1, std::min(np, WorkPool::instance().size() * 4 / nt + 1));
-  std::vector<int64_t> part(nt * chunks, 0);
-  WorkPool::instance().run(nt * chunks, [&](size_t i) {
-    const size_t k = i / chunks, c = i % chunks;
-    part[i] = probe_packets(pr, thr[k], np * c / chunks, np * (c + 1) / chunks);
+  const size_t nt = thr.size(), np = pr.pieces.size();
+  std::vector<PieceResult> part(nt * np);
+  WorkPool::instance().run(nt * np, [&](size_t i) {
+    probe_piece(pr, thr[i / np], pr.pieces[i % np], part[i]);
   });
   out.assign(nt, 0);
-  for (size_t i = 0; i < nt * chunks; ++i) out[i / chunks] += part[i];
+  WorkPool::instance().run(nt, [&](size_t k) {
+    int64_t size = 0;
+    for (const ProbePacket &pk : pr.packets) {
+      StuffCounter sc;
+      sc.put(1, 1);
+      bool e = false;
+      for (uint32_t j = pk.piece0; j < pk.piece0 + pk.npieces; ++j) {
+        const PieceResult &r = part[k * np + j];
+        size += r.body;
+        e = e || r.e;
+        sc.put_bits(r.hdr, 0, r.hdr.n);
+      }
+      size += e ? (int64_t)sc.finish() : 1;
+    }
+    out[k] = size;
+  });
 }
 
 }  // namespace
@@ -554,9 +613,9 @@ void probe_thresholds(const Probe &pr, const std::vector<uint16_t> &thr, std::ve
 // a full truncation-and-header estimate.  Its outcome depends on the exact sequence of probes,
 // so the search itself is kept: the same probes, compared the same way, in the same order.
 // What a predicted final threshold changes is WHEN the probes are evaluated: from the
-// prediction the whole probe path is simulated (assuming the size falls as the threshold
-// rises) and evaluated at once, in parallel host threads; the exact bisection then replays over
-// those results, and only when its path leaves the predicted one is a new round needed (again
+// prediction the probe path is simulated (assuming the size falls as the threshold rises) and
+// its next few probes are evaluated at once, in parallel host threads; the exact bisection then
+// replays over those results, and only when it leaves them is a new round needed (again
 // speculated from the prediction).  The selected slope, and so every output byte, is the
 // plain search's; what the prediction saves is rounds of dependent probes.
 //
@@ -566,20 +625,40 @@ void probe_thresholds(const Probe &pr, const std::vector<uint16_t> &thr, std::ve
 
 namespace {
 
-void rate_features(const Tile &tile, float bpv, float *out) {
-  double hist[32] = {};
-  double total = 0;
+// counts[i] = codeblock passes (z >= 1, non-zero slope) with S >> 11 == i; counts[32] = total
+static void rate_histogram(const Tile &tile, uint64_t counts[33]) {
+  std::vector<const Codeblock *> all;
   for (const Parameter &par : tile.params)
-    for (const Codeblock &cb : par.codeblocks)
-      for (int z = 1; z <= cb.enc.Z; ++z)
-        if (cb.enc.S[z]) {
-          hist[cb.enc.S[z] >> 11] += 1;
-          total += 1;
+    for (const Codeblock &cb : par.codeblocks) all.push_back(&cb);
+  std::mutex m;
+  for (int i = 0; i < 33; ++i) counts[i] = 0;
+  for_chunks(all.size(), [&](size_t first, size_t last) {
+    uint64_t c[33] = {};
+    for (size_t k = first; k < last; ++k) {
+      const CodedBlock &enc = all[k]->enc;
+      for (int z = 1; z <= enc.Z; ++z)
+        if (enc.S[z]) {
+          c[enc.S[z] >> 11]++;
+          c[32]++;
         }
-  for (int i = 0; i < 32; ++i) out[i] = total > 0 ? (float)(hist[i] / total) : 0.f;
+    }
+    std::lock_guard<std::mutex> lk(m);
+    for (int i = 0; i < 33; ++i) counts[i] += c[i];
+  });
+}
+
+static void rate_features_from(const Tile &tile, const uint64_t counts[33], float bpv, float *out) {
+  const double total = (double)counts[32];
+  for (int i = 0; i < 32; ++i) out[i] = total > 0 ? (float)((double)counts[i] / total) : 0.f;
   uint64_t values = tile.box.size() * tile.params.size();
   out[32] = (float)(std::log((double)std::max(bpv, 1e-6f)) / 4.0);
   out[33] = (float)((std::log((double)std::max<uint64_t>(values, 1)) - 14.0) / 4.0);
+}
+
+void rate_features(const Tile &tile, float bpv, float *out) {
+  uint64_t counts[33];
+  rate_histogram(tile, counts);
+  rate_features_from(tile, counts, bpv, out);
 }
 
 // One bisection step of tier2.c:1115-1254; returns true when the search is over.
@@ -623,6 +702,9 @@ std::vector<uint16_t> predicted_path(Search st, uint16_t pred, int64_t target) {
 // the speculative probes of one field are not spread over further threads.
 thread_local bool t_rate_control_in_parallel_fields = false;
 
+// probes of the predicted path evaluated per round (the first being the one the search needs)
+constexpr size_t kSpeculatedProbes = 4;
+
 // create_quality_layers (tier2.c:1115-1254)
 static uchar create_quality_layers(bwc_codec *codec, Tile &tile) {
   const bwc_gl_ctrl &c = codec->control;
@@ -638,8 +720,10 @@ static uchar create_quality_layers(bwc_codec *codec, Tile &tile) {
   // features and, when a model is set, the predicted final slope of every layer
   tile.rc_features.assign((size_t)c.nLayers * kRateFeatures, 0.f);
   tile.rc_stats.assign((size_t)c.nLayers * kRateStats, 0.0);
+  uint64_t counts[33];
+  rate_histogram(tile, counts);
   for (uint8_t l = 0; l < c.nLayers; ++l)
-    rate_features(tile, c.bitrate[l], tile.rc_features.data() + (size_t)l * kRateFeatures);
+    rate_features_from(tile, counts, c.bitrate[l], tile.rc_features.data() + (size_t)l * kRateFeatures);
   std::vector<float> pred(c.nLayers, -1.f);
   const bool have_pred =
       !check && c.nLayers <= 64 && mlp_predict(tile.rc_features.data(), c.nLayers, pred.data());
@@ -675,6 +759,9 @@ static uchar create_quality_layers(bwc_codec *codec, Tile &tile) {
           if (speculate) {
             todo = predicted_path(st, pslope, target - est_tile - (int64_t)header_size);
             if (todo.empty() || todo[0] != s) todo.insert(todo.begin(), s);
+            // the next few probes of the path: deeper ones are rarely reached before the
+            // search leaves the path, and each costs a full probe
+            if (todo.size() > kSpeculatedProbes) todo.resize(kSpeculatedProbes);
           }
           std::vector<int64_t> res;
           probe_thresholds(probe, todo, res);
