@@ -379,7 +379,8 @@ def run_ours(a):
                         "codestream_bytes": len(cs), "bpv": len(cs) * 8 / field.numel(),
                         "device_and_host_codestreams_equal": cs == cs_dev},
             "clocks": clocks.summary(),
-            "gpu_launches": launches,
+            # plus the rate model's forward pass (one launch for all layers) when it predicted
+            "gpu_launches": launches + (1 if (rate_warm[:, 3] >= 0).any() else 0),
             "rate_control": {
                 "warm_start": "built-in model (bigwhoop_b200/data/pcrd_mlp.npy)",
                 "dependent_probe_rounds_per_layer": [int(v) for v in rate_warm[:, 2]],
