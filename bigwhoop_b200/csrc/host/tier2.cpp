@@ -383,7 +383,7 @@ struct ProbePacket {
 struct ProbePiece {
   uint32_t packet, first, count;   // codeblocks [first, first + count) of pr.cbs
 };
-constexpr uint32_t kPieceCbs = 512;
+constexpr uint32_t kPieceCbs = 256;
 
 struct Probe {
   // right-to-left slope records of every codeblock: z in decreasing order with strictly
@@ -423,20 +423,42 @@ static void bits_append_range(RawBits &rb, const RawBits &src, uint64_t off, uin
 }
 
 void build_records(Tile &tile, Probe &pr) {
+  std::vector<const Codeblock *> all;
   for (Parameter &par : tile.params)
-    for (Codeblock &cb : par.codeblocks) {
-      pr.rec_off.push_back((uint32_t)pr.rec_s.size());
-      int best = -1;
-      for (int z = cb.enc.Z; z >= 0; --z) {
-        if ((int)cb.enc.S[z] > best) {
-          best = cb.enc.S[z];
-          pr.rec_s.push_back(cb.enc.S[z]);
-          pr.rec_z.push_back((int16_t)z);
-          pr.rec_L.push_back(z > 0 ? cb.enc.L[z - 1] : 0);
-        }
+    for (Codeblock &cb : par.codeblocks) all.push_back(&cb);
+  // records of a codeblock: the passes z (from Z down to 0) whose S exceeds every later one's
+  auto walk = [](const CodedBlock &e, auto &&emit) {
+    int best = -1;
+    for (int z = e.Z; z >= 0; --z)
+      if ((int)e.S[z] > best) {
+        best = e.S[z];
+        emit(z);
       }
+  };
+  pr.rec_off.assign(all.size() + 1, 0);
+  for_chunks(all.size(), [&](size_t first, size_t last) {
+    for (size_t i = first; i < last; ++i) {
+      uint32_t n = 0;
+      walk(all[i]->enc, [&](int) { ++n; });
+      pr.rec_off[i + 1] = n;
     }
-  pr.rec_off.push_back((uint32_t)pr.rec_s.size());
+  });
+  for (size_t i = 0; i < all.size(); ++i) pr.rec_off[i + 1] += pr.rec_off[i];
+  pr.rec_s.resize(pr.rec_off.back());
+  pr.rec_z.resize(pr.rec_off.back());
+  pr.rec_L.resize(pr.rec_off.back());
+  for_chunks(all.size(), [&](size_t first, size_t last) {
+    for (size_t i = first; i < last; ++i) {
+      const CodedBlock &e = all[i]->enc;
+      uint32_t k = pr.rec_off[i];
+      walk(e, [&](int z) {
+        pr.rec_s[k] = e.S[z];
+        pr.rec_z[k] = (int16_t)z;
+        pr.rec_L[k] = z > 0 ? e.L[z - 1] : 0;
+        ++k;
+      });
+    }
+  });
 }
 
 // per-layer tables in the order create_packet visits codeblocks: the packets' codeblocks are
@@ -583,7 +605,12 @@ void probe_piece(const Probe &pr, uint16_t threshold, const ProbePiece &pc, Piec
 // an empty packet: one byte) as a task of its own
 void probe_thresholds(const Probe &pr, const std::vector<uint16_t> &thr, std::vector<int64_t> &out) {
   const size_t nt = thr.size(), np = pr.pieces.size();
-  std::vector<PieceResult> part(nt * np);
+  // result buffers of the calling thread, kept (with their capacity) from probe to probe; the
+  // pool's tasks reach them through this reference (a thread_local named inside the tasks would
+  // be each worker's own)
+  thread_local std::vector<PieceResult> part_tls;
+  std::vector<PieceResult> &part = part_tls;
+  if (part.size() < nt * np) part.resize(nt * np);
   WorkPool::instance().run(nt * np, [&](size_t i) {
     probe_piece(pr, thr[i / np], pr.pieces[i % np], part[i]);
   });
