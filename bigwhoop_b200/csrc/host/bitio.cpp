@@ -13,16 +13,6 @@
 
 namespace bwcb {
 
-void BitWriter::emit(uint64_t bit) {
-  t--;
-  if (bit) T |= (uint8_t)(1u << t);
-  if (!t) {
-    mem.push_back(T);
-    t = (T == 0xFF) ? 7 : 8;
-    T = 0;
-  }
-}
-
 void BitWriter::flush() {
   if (t != 8) mem.push_back(T);
 }

@@ -191,7 +191,16 @@ struct BitWriter {
   uint8_t T = 0;
   int8_t t = 8;
   uint64_t L() const { return mem.size(); }
-  void emit(uint64_t bit);
+  // one bit, most significant first; a byte after 0xFF holds 7 bits (bit stuffing)
+  void emit(uint64_t bit) {
+    t--;
+    if (bit) T |= (uint8_t)(1u << t);
+    if (!t) {
+      mem.push_back(T);
+      t = (T == 0xFF) ? 7 : 8;
+      T = 0;
+    }
+  }
   void flush();
   uint64_t bytes_used() const { return T == 0xFF ? mem.size() + 1 : mem.size(); }
 };
