@@ -834,14 +834,14 @@ extern "C" uchar bwc_create_compression(bwc_codec *const codec, bwc_stream *cons
   c->bitrate = (float *)realloc(c->bitrate, c->nLayers * sizeof(float));
   if (c->nTiles != 1) {
     warn("o##########################################################o\n"
-         "| ERROR: this build codes single-tile codestreams only     |\n"
+         "| ERROR: this library codes single-tile codestreams only   |\n"
          "o##########################################################o\n");
     return 1;
   }
   if (c->KernelX != bwc_dwt_9_7 || c->KernelY != bwc_dwt_9_7 || c->KernelZ != bwc_dwt_9_7 ||
       (c->KernelTS != bwc_dwt_9_7 && c->decompTS > 0 && info->nTS > 1)) {
     warn("o##########################################################o\n"
-         "| ERROR: this build implements the CDF 9/7 wavelet only    |\n"
+         "| ERROR: this library implements the CDF 9/7 wavelet only  |\n"
          "o##########################################################o\n");
     return 1;
   }

@@ -291,7 +291,7 @@ uchar parse_main_header(bwc_codec *codec, bwc_stream *data, BitReader &br) {
         }
         if (c.nTiles != 1) {
           warn("o##########################################################o\n"
-               "| ERROR: this build decodes single-tile codestreams only   |\n"
+               "| ERROR: this library decodes single-tile codestreams only |\n"
                "o##########################################################o\n");
           return 1;
         }

@@ -18,7 +18,7 @@
 extern "C" {
 #endif
 
-/* Library identification: returns PREC_BIT of this build (63 double, 31 single). */
+/* Library identification: returns PREC_BIT of the loaded library (63 double, 31 single). */
 int bwc_b200_precision_bits(void);
 
 /* The reference keeps process-wide subband energy gains that every configure_codec and
