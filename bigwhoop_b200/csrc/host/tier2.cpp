@@ -376,14 +376,23 @@ struct ProbeCb {
 
 struct ProbePacket {
   uint32_t first, count;
-  uint32_t piece0, npieces;   // its pieces (runs of at most kPieceCbs codeblocks)
+  uint32_t piece0, npieces;   // its pieces (runs of at most piece_cbs() codeblocks)
 };
 
 // a run of codeblocks of one packet, the unit of parallel work
 struct ProbePiece {
   uint32_t packet, first, count;   // codeblocks [first, first + count) of pr.cbs
 };
-constexpr uint32_t kPieceCbs = 256;
+// codeblocks per piece: 256, or BWC_B200_T2_PIECE (tests set a tiny size so that small fields
+// split their packets into many pieces too)
+static uint32_t piece_cbs() {
+  static const uint32_t n = [] {
+    const char *e = getenv("BWC_B200_T2_PIECE");
+    const long v = e ? strtol(e, nullptr, 10) : 0;
+    return (uint32_t)((v > 0 && v <= (1 << 20)) ? v : 256);
+  }();
+  return n;
+}
 
 struct Probe {
   // right-to-left slope records of every codeblock: z in decreasing order with strictly
@@ -462,7 +471,7 @@ void build_records(Tile &tile, Probe &pr) {
 }
 
 // per-layer tables in the order create_packet visits codeblocks: the packets' codeblocks are
-// laid out first, then pieces of at most kPieceCbs codeblocks are filled in parallel, each
+// laid out first, then pieces of at most piece_cbs() codeblocks are filled in parallel, each
 // with its own pool of tag-tree bits (tag-tree estimates only read the trees)
 void build_layer(Tile &tile, int q, Probe &pr) {
   const std::vector<PacketRef> pks = packet_list(tile);
@@ -477,8 +486,9 @@ void build_layer(Tile &tile, int q, Probe &pr) {
       count += (uint32_t)r.par->precincts[sb.first_precinct + r.p].ncb;
     }
     ProbePacket pk{ncb, count, (uint32_t)pr.pieces.size(), 0};
-    for (uint32_t b = 0; b < count; b += kPieceCbs) {
-      pr.pieces.push_back({i, ncb + b, std::min(kPieceCbs, count - b)});
+    const uint32_t per = piece_cbs();
+    for (uint32_t b = 0; b < count; b += per) {
+      pr.pieces.push_back({i, ncb + b, std::min(per, count - b)});
       pk.npieces++;
     }
     pr.packets.push_back(pk);

@@ -144,3 +144,21 @@ def test_fast_rate_control_probes_equal_the_plain_probes():
                        text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     assert "mismatch" not in r.stderr
+
+
+def test_rate_control_in_small_pieces():
+    """The tier-2 probes split each packet into pieces of codeblocks evaluated in parallel;
+    small fields fit in one piece, so here every piece holds two codeblocks
+    (BWC_B200_T2_PIECE=2) and the probe self-check is on: codestreams must still equal the
+    reference's and every probe the plain evaluation."""
+    import os
+    import subprocess
+    import sys
+    need_ref("double")
+    env = dict(os.environ, BWC_B200_T2_PIECE="2", BWC_B200_CHECK_PROBES="1")
+    here = os.path.dirname(os.path.abspath(__file__))
+    r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-x", "-k", "tier2_codestream_identical",
+                        os.path.join(here, "test_host_parity.py")], env=env, capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "mismatch" not in r.stderr
