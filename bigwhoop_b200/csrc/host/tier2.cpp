@@ -95,11 +95,13 @@ static void encode_length(BitWriter &bw, Codeblock &cb, int q, uchar estimate) {
 
 extern thread_local bool t_rate_control_in_parallel_fields;
 
-// ---- packet-parallel host loops --------------------------------------------------------------
+// ---- parallel host loops ----------------------------------------------------------------------
 // Rate control and packet assembly work packet by packet: a packet's computations touch only its
 // own codeblocks, its precincts' tag trees and the packet itself, and every total they feed is
-// an integer sum.  So those loops run over chunks of packets on a small persistent pool of host
-// threads, with results identical to running them in order.
+// an integer sum.  So those loops run on a small persistent pool of host threads, with results
+// identical to running them in order: the final layer evaluation and the final headers over
+// chunks of packets, the probe tables and the probes over pieces of a packet's codeblocks (a
+// probe's per-codeblock work is independent; only its header bits are then counted in order).
 //
 // run(n, fn) calls fn(i) for every i in [0, n) on the pool's threads and the calling thread and
 // returns when all are done.  One call at a time: a second concurrent caller, a caller on one of
