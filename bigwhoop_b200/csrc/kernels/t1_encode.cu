@@ -22,14 +22,17 @@
 //     is monotone in the neighbours' significance, so the iteration climbs from the pre-pass
 //     state to the sequential result, which is the unique fixed point (dependencies point
 //     backwards in scan order).
-// Symbols are counted, offsets come from a CTA-wide prefix sum, and each thread writes its
-// columns' symbols.  Per pass the kernel records the symbol count and the distortion decrease.
+// Each thread generates its columns' symbols once, into its own shared-memory slice; a
+// CTA-wide prefix sum of the counts places them in the pass's arena chunk, and each thread
+// copies its slice there (without the slices -- codeblocks over 4608 stripe columns -- the
+// symbols are counted first and written in a second run).  Per pass the kernel records the
+// symbol count and the distortion decrease.
 //
 // t1_mq_kernel -- one lane per codeblock.  Runs the MQ arithmetic coder over the codeblock's
 // symbol stream (the only part that is inherently sequential), records the coder state at the
 // end of every pass, terminates, derives the minimal truncation length of every pass, builds
-// the convex hull and the 16-bit log slopes.  A warp codes 1 to 32 codeblocks concurrently
-// (mq_lanes_per_warp).
+// the convex hull and the 16-bit log slopes.  A warp holds 1 to 32 codeblocks, each lane with
+// its own loop (mq_lanes_per_warp, or the autotuned count).
 //
 // Stripe-column state (shared memory, one byte each): lo = significance | sign << 4 (read by
 // neighbours), hi = visited-in-significance-pass | refined << 4 (owner only).  Bit planes: one
@@ -990,11 +993,12 @@ size_t t1_model_smem(uint32_t max_cols) {
   return (size_t)max_cols * 3 + (size_t)kModelThreads * t1_model_stage_cap(max_cols);
 }
 
-// Codeblocks per MQ warp.  Each lane runs one codeblock's coder, a long dependent chain, so a
-// warp is latency-bound and its lanes' pass ends and byte transfers diverge; fewer lanes per
-// warp waste less, until the warps' instructions saturate the schedulers.  Measured on B200
-// (FP64, 32x32x16 codeblocks): 1030 codeblocks code fastest at 1 per warp, 8192 at 4 per warp,
-// i.e. at about three warps per scheduler (148 SMs x 4).
+// Codeblocks per MQ warp, the rule used when the autotuner has no entry.  Each lane runs one
+// codeblock's coder, a long dependent chain, so a warp is latency-bound and its lanes diverge
+// (symbol kinds, byte transfers, pass ends); fewer lanes per warp waste less, until the warps'
+// instructions saturate the schedulers.  Measured on B200 (FP64, 32x32x16 codeblocks): 1030
+// codeblocks code fastest at 1 per warp, 8192 at 4 per warp, i.e. at about three warps per
+// scheduler (148 SMs x 4).
 uint32_t mq_lanes_per_warp(uint32_t ncb) {
   const uint32_t target_warps = (uint32_t)dev::kNumSMs * 4 * 3;
   uint32_t lanes = 1;
