@@ -2,9 +2,11 @@
 // (dwt.c:354-466 lifting, :286-342 boundary extension, :645-789 de-/interleave,
 // :1216-2246 level/axis drivers).
 //
-// Each level's spatial axes are transformed by one fused pass (dwt_level_kernel: a 3D tile with
-// halos in shared memory, lifted along x, y and z, interior stored de-interleaved), reading one
-// field-sized buffer and writing the other; the time axis of 4D fields, when transformed, gets
+// Each level's spatial axes are transformed by one fused pass, reading one field-sized buffer
+// and writing the other: the z-streaming kernel (dwt_stream_fwd_kernel) for large forward 3D
+// levels, else dwt_level_kernel (a 3D tile with halos in shared memory, lifted along x, y and
+// z, interior stored de-interleaved, or in natural order for the inverse); the time axis of 4D
+// fields, when transformed, gets
 // an in-place pass of its own (dwt_cols_kernel) in the reference's axis order.  Arithmetic is
 // the reference's: float-literal lifting constants in the codec's type, a + c * (b0 + b1) with
 // separately rounded products and sums, and whole-point symmetric extension of every line
