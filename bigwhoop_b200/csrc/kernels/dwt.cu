@@ -6,12 +6,12 @@
 // and writing the other: the z-streaming kernel (dwt_stream_fwd_kernel) for large forward 3D
 // levels, else dwt_level_kernel (a 3D tile with halos in shared memory, lifted along x, y and
 // z, interior stored de-interleaved, or in natural order for the inverse); the time axis of 4D
-// fields, when transformed, gets
-// an in-place pass of its own (dwt_cols_kernel) in the reference's axis order.  Arithmetic is
-// the reference's: float-literal lifting constants in the codec's type, a + c * (b0 + b1) with
-// separately rounded products and sums, and whole-point symmetric extension of every line
-// (repeated for lines shorter than the filter), which the tiles reproduce by loading reflected
-// samples into their halos and lifting them like the reference lifts its extended lines.
+// fields, when transformed, gets an in-place pass of its own (dwt_cols_kernel) in the
+// reference's axis order.  Arithmetic is the reference's: float-literal lifting constants in
+// the codec's type, a + c * (b0 + b1) with separately rounded products and sums, and
+// whole-point symmetric extension of every line (repeated for lines shorter than the filter),
+// which the tiles reproduce by loading reflected samples into their halos and lifting them
+// like the reference lifts its extended lines.
 #include <algorithm>
 #include <cstdio>
 
