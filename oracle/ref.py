@@ -41,6 +41,7 @@ def load(precision="double"):
                                    C.c_int, C.c_int, C.c_char_p, vp]
     L.rp_compress_full.restype = C.c_size_t
     L.rp_compress_full.argtypes = [vp]
+    L.rp_set_precincts.argtypes = [u8p]
     for n in ("rp_stage_normalize", "rp_stage_dwt", "rp_stage_t1", "rp_dstage_t1",
               "rp_dstage_idwt", "rp_dstage_finish"):
         getattr(L, n).restype = C.c_int
@@ -98,7 +99,7 @@ class RefCompressor:
     """One reference compression, optionally run stage by stage."""
 
     def __init__(self, field, *, precision="double", decomp=None, cb=None, qm=-1, erres=False,
-                 rate="2", n_par=None):
+                 rate="2", n_par=None, precincts=None):
         self.L = load(precision)
         self.precision = precision
         f = np.ascontiguousarray(field)
@@ -117,12 +118,19 @@ class RefCompressor:
         self.h = None
         self.out = np.zeros(f.nbytes + (1 << 16), dtype=np.uint8)
         rate_b = None if rate is None else rate.encode()
-        self.h = self.L.rp_open_compress(
+        self.L.rp_set_precincts(_u8arr(precincts))
+        try:
+            self.h = self._open(f, dims, n_par, decomp, cb, qm, erres, rate_b)
+        finally:
+            self.L.rp_set_precincts(None)
+        if not self.h:
+            raise RuntimeError("reference rejected the configuration")
+
+    def _open(self, f, dims, n_par, decomp, cb, qm, erres, rate_b):
+        return self.L.rp_open_compress(
             f.ctypes.data, dims[0], dims[1], dims[2], dims[3], n_par,
             8 if f.dtype == np.float64 else 4, _u8arr(decomp), _u8arr(cb), int(qm), int(erres),
             rate_b, self.out.ctypes.data)
-        if not self.h:
-            raise RuntimeError("reference rejected the configuration")
 
     def close(self):
         if self.h:

@@ -76,6 +76,15 @@ void rp_get_gain_lut(double *out)
 
 /* decomp/cb: 4 entries each or NULL (library defaults); qm < 0: default; erres: call
  * bwc_set_error_resilience once; rate NULL: lossless default (PREC_BIT + 1 bpv). */
+/* precinct sizes (log2 per axis) applied by the next rp_open_compress calls; NULL: defaults */
+static uint8 rp_prec[4];
+static int   rp_prec_set = 0;
+void rp_set_precincts(const uint8 *p)
+{
+   if(p) { memcpy(rp_prec, p, 4); rp_prec_set = 1; }
+   else  rp_prec_set = 0;
+}
+
 rp_handle *rp_open_compress(void *field, uint64 nX, uint64 nY, uint64 nZ, uint64 nTS,
                             uint8 nPar, int data_prec, const uint8 *decomp, const uint8 *cb,
                             int qm, int erres, const char *rate, void *out)
@@ -87,6 +96,7 @@ rp_handle *rp_open_compress(void *field, uint64 nX, uint64 nY, uint64 nZ, uint64
    if(erres)  bwc_set_error_resilience(h->codec);
    if(decomp) bwc_set_decomp(h->codec, decomp[0], decomp[1], decomp[2], decomp[3]);
    if(cb)     bwc_set_codeblocks(h->codec, cb[0], cb[1], cb[2], cb[3]);
+   if(rp_prec_set) bwc_set_precincts(h->codec, rp_prec[0], rp_prec[1], rp_prec[2], rp_prec[3]);
    if(qm >= 0) bwc_set_qm(h->codec, (uint8)qm);
    h->stream = bwc_init_stream(field, out, comp);
    if(rate)

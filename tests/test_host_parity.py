@@ -28,12 +28,14 @@ def _field(shape, dtype, seed=3):
     return fields.spectral_field(shape, seed).astype(dtype)
 
 
-def _assemble_both(f, precision, decomp, cb, rate):
+def _assemble_both(f, precision, decomp, cb, rate, precincts=None):
     ref = need_ref(precision)
     ref.reset_gain_lut(precision)
     bwc.reset_gain_state(precision)
-    rc = ref.RefCompressor(f, precision=precision, decomp=decomp, cb=cb, rate=rate)
-    mc = bwc.Compressor(f, precision=precision, decomp=decomp, codeblocks=cb, rate=rate)
+    rc = ref.RefCompressor(f, precision=precision, decomp=decomp, cb=cb, rate=rate,
+                           precincts=precincts)
+    mc = bwc.Compressor(f, precision=precision, decomp=decomp, codeblocks=cb, rate=rate,
+                        precincts=precincts)
     try:
         assert np.array_equal(ref.gain_lut(precision), bwc.gain_state(precision))
         ncb = rc.num_codeblocks()
@@ -81,6 +83,23 @@ def _assemble_both(f, precision, decomp, cb, rate):
 def test_tier2_codestream_identical(shape, precision, dtype, decomp, cb, rate):
     f = _field(shape, dtype)
     cs_ref, cs_me = _assemble_both(f, precision, decomp, cb, rate)
+    assert len(cs_me) == len(cs_ref)
+    assert cs_me == cs_ref
+
+
+PRECINCT_CASES = [
+    # shape, decomp, codeblocks, precincts (log2 sizes), rate: many precincts, so every
+    # resolution has many packets
+    ((64, 64, 64), (3, 3, 3, 0), (3, 3, 3, 0), (4, 4, 4, 0), "0.5,2"),
+    ((33, 47, 61), (2, 2, 2, 0), (3, 3, 3, 0), (4, 4, 5, 0), "1"),
+    ((8, 20, 24, 30), (2, 2, 2, 1), (2, 2, 2, 1), (3, 3, 3, 1), "0.25,4"),
+]
+
+
+@pytest.mark.parametrize("shape,decomp,cb,precincts,rate", PRECINCT_CASES)
+def test_tier2_codestream_identical_with_precincts(shape, decomp, cb, precincts, rate):
+    f = _field(shape, np.float64)
+    cs_ref, cs_me = _assemble_both(f, "double", decomp, cb, rate, precincts=precincts)
     assert len(cs_me) == len(cs_ref)
     assert cs_me == cs_ref
 
