@@ -46,6 +46,18 @@ def test_stage_and_codestream_parity(gpu, case):
     assert n_bit_diffs(out, out_ref) == 0
 
 
+def test_many_precincts(gpu):
+    """16^3 precincts over 8^3 codeblocks: many packets per resolution, stage by stage and the
+    decompressed field."""
+    ref = need_ref("double")
+    f = fields.spectral_field((64, 64, 64), 11)
+    rep, cs, cs_ref = compare_stages(f, ref, decomp=(3, 3, 3, 0), cb=(3, 3, 3, 0),
+                                     precincts=(4, 4, 4, 0), rate="0.5,2")
+    assert rep == dict(normalized=0, transformed=0, codeblocks=0, flags=0, codestream=0), rep
+    out = bwc.decompress_array(cs)
+    assert n_bit_diffs(out, ref.decompress(cs_ref, f.shape, f.dtype)) == 0
+
+
 def test_shock_field_with_constant_quarter(gpu):
     """Shock fronts and a constant quarter (all-zero codeblocks: K = 0) at 128^3, 4 layers."""
     ref = need_ref("double")
