@@ -638,13 +638,19 @@ static uchar decompress_impl(bwc_codec *codec, bwc_stream *stream) {
         !dv->mags.ensure(st * sizeof(bwc_raw)) || !dv->K.ensure(ncb) || !dv->Z.ensure(ncb) ||
         !dv->lmax.ensure(ncb * 4) || !dv->flags.ensure(ncb * 4) || !dv->counter.ensure(4) ||
         !dv->pieces.ensure(pieces.size() * sizeof(GatherPiece) + 16) ||
-        (big && !dv->scratch.ensure(st * 2 + 64)))
+        !dv->order.ensure(ncb * 4) || (big && !dv->scratch.ensure(st * 2 + 64)))
       return 1;
+    // decoding order: longest coded length first, so the longest decoding chains start first
+    std::vector<uint32_t> dorder(ncb);
+    for (uint64_t i = 0; i < ncb; ++i) dorder[i] = (uint32_t)i;
+    std::stable_sort(dorder.begin(), dorder.end(),
+                     [&](uint32_t a, uint32_t b) { return hLmax[a] > hLmax[b]; });
     cudaMemcpyAsync(dv->cbtab.p, cbs.data(), sizeof(CbDev) * ncb, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(dv->sbtab.p, sbs.data(), sizeof(SbDev) * sbs.size(), cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(dv->K.p, hK.data(), ncb, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(dv->Z.p, hZ.data(), ncb, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(dv->lmax.p, hLmax.data(), ncb * 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dv->order.p, dorder.data(), ncb * 4, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(dv->pieces.p, pieces.data(), pieces.size() * sizeof(GatherPiece),
                     cudaMemcpyHostToDevice, s);
     cudaMemsetAsync(dv->bytes.p, 0, off + 64, s);
@@ -662,7 +668,7 @@ static uchar decompress_impl(bwc_codec *codec, bwc_stream *stream) {
                         dv->Z.as<uint8_t>(), dv->lmax.as<uint32_t>(), c.error_resilience,
                         dv->mags.as<bwc_raw>(), dv->flags.as<uint32_t>(), state_cap,
                         big ? dv->scratch.as<uint16_t>() : nullptr, dv->counter.as<uint32_t>(),
-                        grid, s);
+                        grid, s, dv->order.as<uint32_t>());
     if (p == 0 && dv->ddump_set && dv->ddump.dequantized)
       cudaMemcpyAsync(dv->ddump.dequantized, dv->temp.p, n * sizeof(bwc_float), cudaMemcpyDeviceToHost, s);
     cudaEventRecord(b2, s);

@@ -99,7 +99,8 @@ void launch_t1_decode_ex(bwc_float *work, const CbDev *cbs, uint32_t ncb,
                          const SbDev *sbs, const uint8_t *data, const uint8_t *K,
                          const uint8_t *Z, const uint32_t *Lmax, uchar erres, bwc_raw *mags,
                          uint32_t *flags, uint32_t state_cap, uint16_t *gstate,
-                         uint32_t *work_counter, int grid, cudaStream_t s);
+                         uint32_t *work_counter, int grid, cudaStream_t s,
+                         const uint32_t *order = nullptr);
 
 // mlp.cu: the rate-control warm start's network (34 -> 64 -> 64 -> 1, FP32).
 constexpr int kMlpInputs = kRateFeatures;

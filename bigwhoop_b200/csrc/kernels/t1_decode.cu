@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
                      const uint8_t *__restrict__ Kin, const uint8_t *__restrict__ Zin,
                      const uint32_t *__restrict__ Lmax, uint32_t erres, bwc_raw *mags,
                      uint32_t *flags, uint32_t state_cap, uint16_t *gstate,
-                     uint32_t *work_counter) {
+                     uint32_t *work_counter, const uint32_t *__restrict__ order) {
   extern __shared__ unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   uint8_t *ctx = smem_raw + wib * 32;
@@ -287,6 +287,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     if (lane == 0) c = atomicAdd(work_counter, 1u);
     c = __shfl_sync(0xffffffffu, c, 0);
     if (c >= ncb) break;
+    if (order) c = order[c];   // the queue position's codeblock (largest coded length first)
     const CbDev cb = cbs[c];
     const SbDev sb = sbs[cb.sb];
     Geo g;
@@ -389,12 +390,13 @@ void launch_t1_decode_ex(bwc_float *work, const CbDev *cbs, uint32_t ncb,
                          const SbDev *sbs, const uint8_t *data, const uint8_t *K,
                          const uint8_t *Z, const uint32_t *Lmax, uchar erres, bwc_raw *mags,
                          uint32_t *flags, uint32_t state_cap, uint16_t *gstate,
-                         uint32_t *work_counter, int grid, cudaStream_t s) {
+                         uint32_t *work_counter, int grid, cudaStream_t s,
+                         const uint32_t *order) {
   const size_t smem = 32 * kWarpsPerBlock + (size_t)state_cap * sizeof(uint16_t) * kWarpsPerBlock;
   cudaFuncSetAttribute(t1_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   t1_decode_kernel<<<grid, kWarpsPerBlock * 32, smem, s>>>(work, cbs, ncb, sbs, data, K, Z,
                                                             Lmax, erres, mags, flags, state_cap,
-                                                            gstate, work_counter);
+                                                            gstate, work_counter, order);
 }
 
 }  // namespace bwcb
