@@ -28,14 +28,14 @@ def _field(shape, dtype, seed=3):
     return fields.spectral_field(shape, seed).astype(dtype)
 
 
-def _assemble_both(f, precision, decomp, cb, rate, precincts=None):
+def _assemble_both(f, precision, decomp, cb, rate, precincts=None, qm=None, erres=False):
     ref = need_ref(precision)
     ref.reset_gain_lut(precision)
     bwc.reset_gain_state(precision)
     rc = ref.RefCompressor(f, precision=precision, decomp=decomp, cb=cb, rate=rate,
-                           precincts=precincts)
+                           precincts=precincts, qm=-1 if qm is None else qm, erres=erres)
     mc = bwc.Compressor(f, precision=precision, decomp=decomp, codeblocks=cb, rate=rate,
-                        precincts=precincts)
+                        precincts=precincts, qm=qm, erres=erres)
     try:
         assert np.array_equal(ref.gain_lut(precision), bwc.gain_state(precision))
         ncb = rc.num_codeblocks()
@@ -101,6 +101,21 @@ def test_tier2_codestream_identical_with_precincts(shape, decomp, cb, precincts,
     f = _field(shape, np.float64)
     cs_ref, cs_me = _assemble_both(f, "double", decomp, cb, rate, precincts=precincts)
     assert len(cs_me) == len(cs_ref)
+    assert cs_me == cs_ref
+
+
+@pytest.mark.parametrize("qm,erres", [(40, False), (None, True)])
+def test_tier2_codestream_identical_with_precincts_qm_erres(qm, erres):
+    f = _field((32, 32, 32), np.float64)
+    cs_ref, cs_me = _assemble_both(f, "double", (3, 3, 3, 0), (3, 3, 3, 0), "1,3",
+                                   precincts=(4, 4, 4, 0), qm=qm, erres=erres)
+    assert cs_me == cs_ref
+
+
+def test_tier2_codestream_identical_with_precincts_single_precision():
+    f = _field((33, 47, 61), np.float32)
+    cs_ref, cs_me = _assemble_both(f, "single", (2, 2, 2, 0), (3, 3, 3, 0), "1,2",
+                                   precincts=(4, 4, 4, 0))
     assert cs_me == cs_ref
 
 
