@@ -119,12 +119,18 @@ def test_tier2_codestream_identical_with_precincts_single_precision():
     assert cs_me == cs_ref
 
 
-@pytest.mark.parametrize("shape,precision,dtype,decomp,cb,rate", CASES[:6])
-def test_parse_identical(shape, precision, dtype, decomp, cb, rate):
+PARSE_CASES = [c + (None,) for c in CASES[:6]] + [
+    ((64, 64, 64), "double", np.float64, (3, 3, 3, 0), (3, 3, 3, 0), "0.5,2", (4, 4, 4, 0)),
+]
+
+
+@pytest.mark.parametrize("shape,precision,dtype,decomp,cb,rate,precincts", PARSE_CASES)
+def test_parse_identical(shape, precision, dtype, decomp, cb, rate, precincts):
     ref = need_ref(precision)
     f = _field(shape, dtype)
     ref.reset_gain_lut(precision)
-    cs = ref.compress(f, precision=precision, decomp=decomp, cb=cb, rate=rate)
+    cs = ref.compress(f, precision=precision, decomp=decomp, cb=cb, rate=rate,
+                      precincts=precincts)
     rd = ref.RefDecompressor(cs, f.shape, f.dtype, precision=precision)
     d = bwc.Decompressor(cs, precision=precision)
     try:
