@@ -170,6 +170,16 @@ void free_engine(bwc_codec *codec) {
   codec->tile = nullptr;
 }
 
+// host memory that is page-locked (registered with or allocated by CUDA)
+static bool is_pinned_host(const void *p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
 static bool is_device_pointer(const void *p) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -733,6 +743,9 @@ struct BatchState {
   // sources and buffer addresses); the few most recent are kept
   std::vector<std::pair<std::string, cudaGraphExec_t>> graphs;
   uint64_t graph_launches = 0, graph_captures = 0;
+  // page-locked staging area for inputs in pageable host memory (kept, grown as needed)
+  void *pinned = nullptr;
+  uint64_t pinned_cap = 0;
 };
 
 constexpr int kBatchStreams = 8;
@@ -867,10 +880,58 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
       !bs->symused.ensure(8) || !bs->order.ensure(ncb * 4) || !bs->queue.ensure(4))
     return 1;
   const std::vector<uint32_t> order = work_order(allcb, allsb, 0, ncb);
+  // Inputs in pageable host memory go through a page-locked staging area: several host threads
+  // copy them in, then each is uploaded by DMA (a copy straight from pageable memory is staged
+  // by the driver in small page-locked chunks, several times slower).  Page-locked host inputs
+  // are uploaded as they are; device inputs need no upload.
+  std::vector<uint64_t> stage_off(nf, ~0ull);
+  uint64_t stage_total = 0;
   for (uint32_t i = 0; i < nf; ++i)
-    if (in_off[i] != ~0ull)
-      cudaMemcpyAsync(bs->in.as<uint8_t>() + in_off[i], streams[i]->inp, in_bytes[i],
+    if (in_off[i] != ~0ull && !is_pinned_host(streams[i]->inp)) {
+      stage_off[i] = stage_total;
+      stage_total += in_bytes[i];
+    }
+  if (stage_total > bs->pinned_cap) {
+    if (bs->pinned) cudaFreeHost(bs->pinned);
+    bs->pinned = nullptr;
+    bs->pinned_cap = 0;
+    if (cudaHostAlloc(&bs->pinned, stage_total, cudaHostAllocDefault) == cudaSuccess) {
+      bs->pinned_cap = stage_total;
+    } else {
+      cudaGetLastError();   // no staging area: upload from pageable memory directly
+      bs->pinned = nullptr;
+    }
+  }
+  const bool staged = stage_total > 0 && bs->pinned != nullptr;
+  if (staged) {
+    // an earlier call that returned early may still be uploading from the staging area
+    if (!cuda_ok(cudaStreamSynchronize(s), "batch staging")) return 1;
+    // the inputs, concatenated, cut into equal spans, one per thread
+    const unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> th;
+    for (unsigned k = 0; k < nt; ++k)
+      th.emplace_back([&, k] {
+        const uint64_t a = stage_total * k / nt, b = stage_total * (k + 1) / nt;
+        for (uint32_t i = 0; i < nf; ++i) {
+          if (stage_off[i] == ~0ull) continue;
+          const uint64_t lo = std::max(a, stage_off[i]);
+          const uint64_t hi = std::min(b, stage_off[i] + in_bytes[i]);
+          if (lo < hi)
+            std::memcpy(static_cast<uint8_t *>(bs->pinned) + lo,
+                        static_cast<const uint8_t *>(streams[i]->inp) + (lo - stage_off[i]),
+                        hi - lo);
+        }
+      });
+    for (auto &t : th) t.join();
+  }
+  for (uint32_t i = 0; i < nf; ++i)
+    if (in_off[i] != ~0ull) {
+      const void *from = (staged && stage_off[i] != ~0ull)
+                             ? static_cast<const void *>(static_cast<uint8_t *>(bs->pinned) + stage_off[i])
+                             : streams[i]->inp;
+      cudaMemcpyAsync(bs->in.as<uint8_t>() + in_off[i], from, in_bytes[i],
                       cudaMemcpyHostToDevice, s);
+    }
   for (BatchUnit &u : units) {
     const bwc_codec *codec = codecs[u.field];
     const size_t dsz = u.src_double ? 8 : 4;
