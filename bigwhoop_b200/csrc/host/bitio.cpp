@@ -17,6 +17,24 @@ void BitWriter::flush() {
   if (t != 8) mem.push_back(T);
 }
 
+void BitWriter::append(const RawBits &rb) {
+  for (uint64_t off = 0; off < rb.n;) {
+    // as many of the next bits as the current byte has room for
+    const int k = (int)std::min<uint64_t>((uint64_t)t, rb.n - off);
+    const uint64_t b = off & 63;
+    uint64_t v = rb.words[off >> 6] << b;
+    if (b + (uint64_t)k > 64) v |= rb.words[(off >> 6) + 1] >> (64 - b);
+    t = (int8_t)(t - k);
+    T |= (uint8_t)((uint32_t)(v >> (64 - k)) << t);
+    off += (uint64_t)k;
+    if (!t) {
+      mem.push_back(T);
+      t = (T == 0xFF) ? 7 : 8;
+      T = 0;
+    }
+  }
+}
+
 uchar BitReader::get_bit() {
   if (!t) {
     if (L == Lmax) return 1;
@@ -145,6 +163,11 @@ static void tagtree_walk(Tree &tt, Writer &bw, uint32_t threshold, uint64_t leaf
 void tagtree_encode(TagTree &tt, BitWriter &bw, uint32_t threshold, uint64_t leaf,
                     uchar estimate) {
   tagtree_walk(tt, bw, threshold, leaf, !estimate);
+}
+
+void tagtree_encode_bits(TagTree &tt, RawBits &out, uint32_t threshold, uint64_t leaf,
+                         uchar estimate) {
+  tagtree_walk(tt, out, threshold, leaf, !estimate);
 }
 
 void tagtree_estimate(const TagTree &tt, RawBits &out, uint32_t threshold, uint64_t leaf) {

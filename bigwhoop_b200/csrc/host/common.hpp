@@ -186,6 +186,8 @@ uchar build_geometry(bwc_codec *codec);   // create_codec
 void free_engine(bwc_codec *codec);
 
 // ---- bit I/O and tag trees (bitio.cpp) ------------------------------------------------------
+struct RawBits;
+
 struct BitWriter {
   std::vector<uint8_t> mem;
   uint8_t T = 0;
@@ -202,6 +204,8 @@ struct BitWriter {
     }
   }
   void flush();
+  // every bit of an unstuffed bit string, as emit() would write them one by one
+  void append(const RawBits &rb);
   uint64_t bytes_used() const { return T == 0xFF ? mem.size() + 1 : mem.size(); }
 };
 
@@ -237,6 +241,9 @@ void tagtree_init(TagTree &tt, uint64_t lx, uint64_t ly, uint64_t lz, uint64_t l
 void tagtree_reset(TagTree &tt);
 void tagtree_set(TagTree &tt, uint64_t leaf, uint16_t value);
 void tagtree_encode(TagTree &tt, BitWriter &bw, uint32_t threshold, uint64_t leaf, uchar estimate);
+// the same bits, unstuffed (byte stuffing is applied when they are appended to a BitWriter)
+void tagtree_encode_bits(TagTree &tt, RawBits &out, uint32_t threshold, uint64_t leaf,
+                         uchar estimate);
 // the bits an estimating tagtree_encode would emit (the tree is left unchanged)
 void tagtree_estimate(const TagTree &tt, RawBits &out, uint32_t threshold, uint64_t leaf);
 uchar tagtree_decode(TagTree &tt, BitReader &br, uint32_t threshold, uint64_t leaf);

@@ -31,7 +31,8 @@ static inline uint16_t ilog2_u16(uint64_t x) {
   return (uint16_t)(63 - __builtin_clzll(x));
 }
 
-static void encode_delta_z(BitWriter &bw, int dz) {
+template <class Writer>
+static void encode_delta_z(Writer &bw, int dz) {
   if (dz == 1) {
     bw.emit(0);
   } else if (dz == 2) {
@@ -65,7 +66,8 @@ static int decode_delta_z(BitReader &br) {
   return dz + 37;
 }
 
-static void encode_length(BitWriter &bw, Codeblock &cb, int q, uchar estimate) {
+template <class Writer>
+static void encode_length(Writer &bw, Codeblock &cb, int q, uchar estimate) {
   int16_t *cp = cb.cp();
   const int16_t z_curr = cp[q] - 1, z_prev = cp[q - 1] - 1;
   uint16_t beta = (!estimate) ? cb.beta : cb.beta_est;
@@ -207,6 +209,43 @@ static void for_chunks(size_t n, const std::function<void(size_t, size_t)> &fn) 
   WorkPool::instance().run(chunks, [&](size_t c) { fn(n * c / chunks, n * (c + 1) / chunks); });
 }
 
+using BodyPieces = std::vector<std::pair<uint64_t, uint32_t>>;
+
+// What the precinct of subband m at packet position p adds to the header of layer q's packet
+// (create_packet's codeblock loop, tier2.c:434-711, for one subband): its header bits, unstuffed,
+// and its body, counted (est 1) or as pieces (est 0).  Each subband's precinct has tag trees of
+// its own, so different subbands can be coded at the same time and their bits joined in order.
+static void segment_bits(Parameter &par, Resolution &res, uint32_t p, uint8_t m, int q,
+                         uchar est, RawBits &hdr, uint64_t &body, BodyPieces &pieces) {
+  const Subband &sb = par.subbands[res.first_subband + m];
+  Precinct &pr = par.precincts[sb.first_precinct + p];
+  for (uint64_t k = 0; k < pr.ncb; ++k) {
+    Codeblock &cb = par.codeblocks[pr.first_cb + k];
+    int16_t *cp = cb.cp();
+    const int dz = cp[q] - cp[q - 1];
+    if (cp[q - 1] == 0) {
+      tagtree_encode_bits(pr.incl, hdr, (uint32_t)(q + 1), k, est);
+      if (cp[q])
+        for (uint32_t kk = 1; kk <= cb.enc.Kmsbs + 1u; ++kk)
+          tagtree_encode_bits(pr.msbs, hdr, kk, k, est);
+    } else {
+      hdr.emit(dz);
+    }
+    if (dz) {
+      encode_delta_z(hdr, dz);
+      encode_length(hdr, cb, q, est);
+      if (est <= 1) {
+        const uint32_t start = (cp[q - 1] == 0) ? 0 : (uint32_t)cb.enc.L[cp[q - 1] - 1];
+        const uint32_t end = (cp[q] == 0) ? 0 : (uint32_t)cb.enc.L[cp[q] - 1];
+        if (est == 1)
+          body += (uint32_t)(end - start);
+        else
+          pieces.emplace_back(cb.data_off + start, (uint32_t)(end - start));
+      }
+    }
+  }
+}
+
 // create_packet (tier2.c:434-711).  est: 0 final, 1 final-size estimate, 2 probe.
 static int64_t create_packet(Parameter &par, Resolution &res, uint32_t p, int q, uchar est) {
   Packet &pk = res.packets[(uint64_t)q * res.nprec + p];
@@ -215,35 +254,14 @@ static int64_t create_packet(Parameter &par, Resolution &res, uint32_t p, int q,
     hdr.mem.reserve(64);
     if (!est) pk.pieces.clear();
     hdr.emit(1);
+    RawBits seg;
+    uint64_t body = 0;
     for (uint8_t m = 0; m < res.nsub; ++m) {
-      const Subband &sb = par.subbands[res.first_subband + m];
-      Precinct &pr = par.precincts[sb.first_precinct + p];
-      for (uint64_t k = 0; k < pr.ncb; ++k) {
-        Codeblock &cb = par.codeblocks[pr.first_cb + k];
-        int16_t *cp = cb.cp();
-        const int dz = cp[q] - cp[q - 1];
-        if (cp[q - 1] == 0) {
-          tagtree_encode(pr.incl, hdr, (uint32_t)(q + 1), k, est);
-          if (cp[q])
-            for (uint32_t kk = 1; kk <= cb.enc.Kmsbs + 1u; ++kk)
-              tagtree_encode(pr.msbs, hdr, kk, k, est);
-        } else {
-          hdr.emit(dz);
-        }
-        if (dz) {
-          encode_delta_z(hdr, dz);
-          encode_length(hdr, cb, q, est);
-          if (est <= 1) {
-            const uint32_t start = (cp[q - 1] == 0) ? 0 : (uint32_t)cb.enc.L[cp[q - 1] - 1];
-            const uint32_t end = (cp[q] == 0) ? 0 : (uint32_t)cb.enc.L[cp[q] - 1];
-            if (est == 1)
-              pk.body_size += (uint32_t)(end - start);
-            else
-              pk.pieces.emplace_back(cb.data_off + start, (uint32_t)(end - start));
-          }
-        }
-      }
+      seg.clear();
+      segment_bits(par, res, p, m, q, est, seg, body, pk.pieces);
+      hdr.append(seg);
     }
+    if (est == 1) pk.body_size += body;
     hdr.flush();
     if (est) {
       if (est == 2) pk.e = 0;
@@ -262,47 +280,89 @@ static int64_t create_packet(Parameter &par, Resolution &res, uint32_t p, int q,
   return 1;
 }
 
+// create_quality_layer's codeblock loop (tier2.c:896-1079) for the precinct of subband m at the
+// position of r: each codeblock's truncation point for layer q under `threshold`, the body bytes
+// that adds, and (final call) the tag-tree values; `grows` when a codeblock gains passes
+static int64_t truncate_segment(const bwc_gl_ctrl &c, const PacketRef &r, uint8_t m,
+                                uint16_t threshold, int q, uchar est, bool &grows) {
+  Parameter &par = *r.par;
+  Resolution &res = *r.res;
+  const Subband &sb = par.subbands[res.first_subband + m];
+  Precinct &pr = par.precincts[sb.first_precinct + r.p];
+  int64_t size = 0;
+  for (uint64_t k = 0; k < pr.ncb; ++k) {
+    Codeblock &cb = par.codeblocks[pr.first_cb + k];
+    int16_t *cp = cb.cp();
+    int16_t z;
+    for (z = cb.enc.Z; z >= 0 && cb.enc.S[z] < threshold; --z) {
+    }
+    if (z < cp[q - 1]) {
+      cp[q] = cp[q - 1];
+      if (cp[q] == 1) size += (int64_t)cb.enc.L[0];
+    } else {
+      cp[q] = z;
+      if (z > 0) {
+        size += (int64_t)cb.enc.L[z - 1];
+        if (z > 1 && (cp[q - 1] > 0)) size -= (int64_t)cb.enc.L[cp[q - 1] - 1];
+      }
+    }
+    if (cp[q] > cp[q - 1]) grows = true;
+    if (!est) {
+      if (q == 0) tagtree_set(pr.msbs, k, cb.enc.Kmsbs);
+      if (q + 1 == c.nLayers) {
+        uint8_t l;
+        for (l = 0; (l < c.nLayers) && (cb.cp()[l] == 0); ++l) {
+        }
+        tagtree_set(pr.incl, k, l);
+      }
+    }
+  }
+  return size;
+}
+
 // create_quality_layer (tier2.c:896-1079), a packet at a time: the truncation points of the
 // packet's codeblocks (every subband's precinct at that position), then the packet's header
 static int64_t quality_layer_packet(const bwc_gl_ctrl &c, const PacketRef &r, uint16_t threshold,
                                     int q, uchar est) {
-  Parameter &par = *r.par;
   Resolution &res = *r.res;
-  const uint32_t p = r.p;
   int64_t size = 0;
-  for (uint8_t m = 0; m < res.nsub; ++m) {
-    const Subband &sb = par.subbands[res.first_subband + m];
-    Precinct &pr = par.precincts[sb.first_precinct + p];
-    for (uint64_t k = 0; k < pr.ncb; ++k) {
-      Codeblock &cb = par.codeblocks[pr.first_cb + k];
-      int16_t *cp = cb.cp();
-      int16_t z;
-      for (z = cb.enc.Z; z >= 0 && cb.enc.S[z] < threshold; --z) {
-      }
-      if (z < cp[q - 1]) {
-        cp[q] = cp[q - 1];
-        if (cp[q] == 1) size += (int64_t)cb.enc.L[0];
-      } else {
-        cp[q] = z;
-        if (z > 0) {
-          size += (int64_t)cb.enc.L[z - 1];
-          if (z > 1 && (cp[q - 1] > 0)) size -= (int64_t)cb.enc.L[cp[q - 1] - 1];
-        }
-      }
-      if (cp[q] > cp[q - 1]) res.packets[(uint64_t)q * res.nprec + p].e = 1;
-      if (!est) {
-        if (q == 0) tagtree_set(pr.msbs, k, cb.enc.Kmsbs);
-        if (q + 1 == c.nLayers) {
-          uint8_t l;
-          for (l = 0; (l < c.nLayers) && (cb.cp()[l] == 0); ++l) {
-          }
-          tagtree_set(pr.incl, k, l);
-        }
-      }
+  bool grows = false;
+  for (uint8_t m = 0; m < res.nsub; ++m)
+    size += truncate_segment(c, r, m, threshold, q, est, grows);
+  if (grows) res.packets[(uint64_t)q * res.nprec + r.p].e = 1;
+  const int64_t ph = create_packet(*r.par, res, r.p, q, est + 1);
+  return (ph < 0) ? -1 : size + ph;
+}
+
+// The final passes work on segments: one subband's precinct at one packet position (its
+// codeblocks and tag trees belong to no other segment), taken largest first.
+struct Segment {
+  uint32_t packet;   // index into the packet list
+  uint8_t m;         // subband within the resolution
+  uint64_t ncb;
+};
+
+// segments of every packet, in packet then subband order (first[i]: packet i's first segment),
+// and the order to work on them
+static std::vector<Segment> segment_list(const std::vector<PacketRef> &pks,
+                                         std::vector<uint32_t> &first,
+                                         std::vector<uint32_t> &order) {
+  std::vector<Segment> segs;
+  first.assign(pks.size() + 1, 0);
+  for (uint32_t i = 0; i < (uint32_t)pks.size(); ++i) {
+    first[i] = (uint32_t)segs.size();
+    const PacketRef &r = pks[i];
+    for (uint8_t m = 0; m < r.res->nsub; ++m) {
+      const Subband &sb = r.par->subbands[r.res->first_subband + m];
+      segs.push_back({i, m, r.par->precincts[sb.first_precinct + r.p].ncb});
     }
   }
-  const int64_t ph = create_packet(par, res, p, q, est + 1);
-  return (ph < 0) ? -1 : size + ph;
+  first[pks.size()] = (uint32_t)segs.size();
+  order.resize(segs.size());
+  for (uint32_t j = 0; j < (uint32_t)segs.size(); ++j) order[j] = j;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](uint32_t a, uint32_t b) { return segs[a].ncb > segs[b].ncb; });
+  return segs;
 }
 
 static int64_t create_quality_layer(bwc_codec *codec, Tile &tile, uint16_t threshold, int q,
@@ -645,6 +705,60 @@ void probe_thresholds(const Probe &pr, const std::vector<uint16_t> &thr, std::ve
   });
 }
 
+// create_quality_layer(codec, tile, threshold, q, 0) over segments in parallel: truncation
+// points and tag-tree values of every segment; then the packets' `e`; then every segment's header
+// bits (estimating: the trees are only read, the length codes' estimate state advances); then
+// each packet's header is sized as a probe sizes it (a 1 bit, its segments' bits, byte stuffing;
+// an empty packet: one byte).  Same sums, same states as the packet-at-a-time loop.
+int64_t final_quality_layer(bwc_codec *codec, Tile &tile, uint16_t threshold, int q) {
+  const bwc_gl_ctrl &c = codec->control;
+  const std::vector<PacketRef> pks = packet_list(tile);
+  std::vector<uint32_t> first, order;
+  const std::vector<Segment> segs = segment_list(pks, first, order);
+  const size_t ns = segs.size();
+  std::vector<int64_t> size(ns, 0);
+  std::vector<uint8_t> grows(ns, 0);
+  WorkPool::instance().run(ns, [&](size_t j) {
+    const uint32_t s = order[j];
+    bool g = false;
+    size[s] = truncate_segment(c, pks[segs[s].packet], segs[s].m, threshold, q, 0, g);
+    grows[s] = g ? 1 : 0;
+  });
+  std::vector<uint8_t> e(pks.size(), 0);
+  for (size_t i = 0; i < pks.size(); ++i) {
+    Packet &pk = pks[i].res->packets[(uint64_t)q * pks[i].res->nprec + pks[i].p];
+    for (uint32_t s = first[i]; s < first[i + 1]; ++s)
+      if (grows[s]) pk.e = 1;
+    e[i] = pk.e;
+  }
+  std::vector<RawBits> bits(ns);
+  std::vector<uint64_t> body(ns, 0);
+  WorkPool::instance().run(ns, [&](size_t j) {
+    const uint32_t s = order[j];
+    if (!e[segs[s].packet]) return;
+    const PacketRef &r = pks[segs[s].packet];
+    BodyPieces unused;
+    segment_bits(*r.par, *r.res, r.p, segs[s].m, q, 1, bits[s], body[s], unused);
+  });
+  int64_t total = 0;
+  for (size_t i = 0; i < pks.size(); ++i) {
+    for (uint32_t s = first[i]; s < first[i + 1]; ++s) total += size[s];
+    if (!e[i]) {
+      total += 1;
+      continue;
+    }
+    Packet &pk = pks[i].res->packets[(uint64_t)q * pks[i].res->nprec + pks[i].p];
+    StuffCounter sc;
+    sc.put(1, 1);
+    for (uint32_t s = first[i]; s < first[i + 1]; ++s) {
+      sc.put_bits(bits[s], 0, bits[s].n);
+      pk.body_size += body[s];
+    }
+    total += (int64_t)sc.finish();
+  }
+  return total;
+}
+
 }  // namespace
 
 // ---- rate-control warm start ---------------------------------------------------------------
@@ -834,7 +948,7 @@ static uchar create_quality_layers(bwc_codec *codec, Tile &tile) {
     rs[3] = have_pred ? (double)pslope : -1.0;
     rs[4] = tile.slope_min;
     rs[5] = tile.slope_max;
-    est = create_quality_layer(codec, tile, slope, l, 0);
+    est = final_quality_layer(codec, tile, slope, l);
     if (est >= 0)
       est_tile += est + (int64_t)header_size;
     else
@@ -844,31 +958,60 @@ static uchar create_quality_layers(bwc_codec *codec, Tile &tile) {
 }
 
 // create_packets (tier2.c:751-849): final headers for every packet, then the per-codeblock
-// coding state is cleared as in the reference.
+// coding state is cleared as in the reference.  Each segment codes its layers in order (its tag
+// trees and length codes carry state from layer to layer) in parallel with the others; then
+// every packet's header is its segments' bits joined in subband order behind the leading 1 bit.
 static uchar create_packets(bwc_codec *codec, Tile &tile) {
   const bwc_gl_ctrl &c = codec->control;
+  const int nl = c.nLayers;
   const std::vector<PacketRef> pks = packet_list(tile);
-  std::atomic<bool> bad{false};
-  for_chunks(pks.size(), [&](size_t first, size_t last) {
-    for (size_t i = first; i < last; ++i) {
-      Parameter &par = *pks[i].par;
-      Resolution &res = *pks[i].res;
-      const uint32_t p = pks[i].p;
-      for (uint8_t l = 0; l < c.nLayers; ++l)
-        if (create_packet(par, res, p, l, 0) < 0) bad = true;
-      // the reference clears each codeblock's coding state once its packets exist
-      for (uint8_t m = 0; m < res.nsub; ++m) {
-        const Subband &sb = par.subbands[res.first_subband + m];
-        const Precinct &pr = par.precincts[sb.first_precinct + p];
-        for (uint64_t k = 0; k < pr.ncb; ++k) {
-          Codeblock &cb = par.codeblocks[pr.first_cb + k];
-          cb.enc = CodedBlock();
-          for (int l = 0; l < c.nLayers; ++l) cb.cp()[l] = 0;
-        }
-      }
+  std::vector<uint32_t> first, order;
+  const std::vector<Segment> segs = segment_list(pks, first, order);
+  std::vector<RawBits> bits(segs.size() * (size_t)nl);
+  std::vector<BodyPieces> body(segs.size() * (size_t)nl);
+  WorkPool::instance().run(segs.size(), [&](size_t j) {
+    const uint32_t s = order[j];
+    const PacketRef &r = pks[segs[s].packet];
+    Parameter &par = *r.par;
+    Resolution &res = *r.res;
+    uint64_t unused = 0;
+    for (int l = 0; l < nl; ++l)
+      if (res.packets[(uint64_t)l * res.nprec + r.p].e)
+        segment_bits(par, res, r.p, segs[s].m, l, 0, bits[(size_t)s * nl + l], unused,
+                     body[(size_t)s * nl + l]);
+    // the reference clears each codeblock's coding state once its packets exist
+    const Subband &sb = par.subbands[res.first_subband + segs[s].m];
+    const Precinct &pr = par.precincts[sb.first_precinct + r.p];
+    for (uint64_t k = 0; k < pr.ncb; ++k) {
+      Codeblock &cb = par.codeblocks[pr.first_cb + k];
+      cb.enc = CodedBlock();
+      for (int l = 0; l < nl; ++l) cb.cp()[l] = 0;
     }
   });
-  return bad ? 1 : 0;
+  for_chunks(pks.size() * (size_t)nl, [&](size_t lo, size_t hi) {
+    for (size_t x = lo; x < hi; ++x) {
+      const size_t i = x / nl;
+      const int l = (int)(x % nl);
+      Packet &pk = pks[i].res->packets[(uint64_t)l * pks[i].res->nprec + pks[i].p];
+      if (!pk.e) {
+        pk.size = 1;
+        pk.header.assign(1, 0);
+        continue;
+      }
+      BitWriter hdr;
+      hdr.emit(1);
+      pk.pieces.clear();
+      for (uint32_t s = first[i]; s < first[i + 1]; ++s) {
+        hdr.append(bits[(size_t)s * nl + l]);
+        const BodyPieces &b = body[(size_t)s * nl + l];
+        pk.pieces.insert(pk.pieces.end(), b.begin(), b.end());
+      }
+      hdr.flush();
+      pk.header = std::move(hdr.mem);
+      pk.size = pk.body_size + pk.header.size();
+    }
+  });
+  return 0;
 }
 
 uchar t2_encode(bwc_codec *codec, Tile &tile) {
