@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <condition_variable>
 #include <cstdio>
@@ -128,13 +129,14 @@ class WorkPool {
       fn_ = &fn;
       n_ = n;
       next_.store(0);
-      pending_ = workers_.size();
-      ++gen_;
+      pending_.store(workers_.size());
+      gen_.store(gen_.load() + 1);
     }
     cv_.notify_all();
     drain();
+    spin([&] { return pending_.load(std::memory_order_acquire) == 0; });
     std::unique_lock<std::mutex> lk(m_);
-    done_.wait(lk, [&] { return pending_ == 0; });
+    done_.wait(lk, [&] { return pending_.load() == 0; });
     fn_ = nullptr;
   }
 
@@ -147,7 +149,7 @@ class WorkPool {
   ~WorkPool() {
     {
       std::lock_guard<std::mutex> lk(m_);
-      stop_ = true;
+      stop_.store(true);
     }
     cv_.notify_all();
     for (auto &t : workers_) t.join();
@@ -155,18 +157,39 @@ class WorkPool {
   void drain() {
     for (size_t i = next_.fetch_add(1); i < n_; i = next_.fetch_add(1)) (*fn_)(i);
   }
+  // Rate control calls run() many times in a row with short gaps (one probe after another), so
+  // a thread that waits first polls for up to kSpinMicros before it sleeps: waking a sleeping
+  // thread costs tens of microseconds, more than a probe's share of work.
+  static constexpr int kSpinMicros = 200;
+  template <class Ready>
+  static void spin(Ready &&ready) {
+    const auto until = std::chrono::steady_clock::now() + std::chrono::microseconds(kSpinMicros);
+    for (;;) {
+      for (int i = 0; i < 64; ++i) {
+        if (ready()) return;
+#if defined(__x86_64__) || defined(__i386__)
+        __builtin_ia32_pause();
+#elif defined(__aarch64__)
+        asm volatile("yield");
+#endif
+      }
+      if (std::chrono::steady_clock::now() >= until) return;
+    }
+  }
   void loop() {
     uint64_t seen = 0;
     for (;;) {
+      spin([&] { return stop_.load(std::memory_order_acquire) ||
+                        gen_.load(std::memory_order_acquire) != seen; });
       {
         std::unique_lock<std::mutex> lk(m_);
-        cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
-        if (stop_) return;
-        seen = gen_;
+        cv_.wait(lk, [&] { return stop_.load() || gen_.load() != seen; });
+        if (stop_.load()) return;
+        seen = gen_.load();
       }
       drain();
       std::lock_guard<std::mutex> lk(m_);
-      if (--pending_ == 0) done_.notify_one();
+      if (pending_.fetch_sub(1) == 1) done_.notify_one();
     }
   }
   const pid_t pid_;
@@ -174,10 +197,10 @@ class WorkPool {
   std::mutex call_, m_;
   std::condition_variable cv_, done_;
   const std::function<void(size_t)> *fn_ = nullptr;
-  size_t n_ = 0, pending_ = 0;
-  std::atomic<size_t> next_{0};
-  uint64_t gen_ = 0;
-  bool stop_ = false;
+  size_t n_ = 0;
+  std::atomic<size_t> next_{0}, pending_{0};
+  std::atomic<uint64_t> gen_{0};
+  std::atomic<bool> stop_{false};
 };
 
 // every packet position of the tile, in the order the codestream and the reference visit them
@@ -403,6 +426,16 @@ struct StuffCounter {
   void put(uint64_t v, int n) {   // the n (<= 56) low bits of v, most significant first
     acc = (acc << n) | (v & ((1ull << n) - 1));
     nacc += n;
+    // a byte can only be 0xFF where 8 ones run in a row: with no such run among the pending
+    // bits, and full bytes being filled, every whole byte is an 8-bit one
+    uint64_t run = acc & (acc << 1);
+    run &= run << 2;
+    run &= run << 4;
+    if (w == 8 && (run & ((nacc >= 64) ? ~0ull : ((1ull << nacc) - 1))) == 0) {
+      bytes += (uint64_t)(nacc >> 3);
+      nacc &= 7;
+      return;
+    }
     while (nacc >= w) {
       nacc -= w;
       const uint32_t byte = (uint32_t)(acc >> nacc) & ((1u << w) - 1);
