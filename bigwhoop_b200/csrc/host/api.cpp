@@ -170,6 +170,19 @@ void free_engine(bwc_codec *codec) {
   codec->tile = nullptr;
 }
 
+// timing events of one stage sequence, released however the scope is left
+struct ScopedEvents {
+  cudaEvent_t e[4];
+  ScopedEvents() {
+    for (auto &x : e) cudaEventCreate(&x);
+  }
+  ~ScopedEvents() {
+    for (auto &x : e) cudaEventDestroy(x);
+  }
+  ScopedEvents(const ScopedEvents &) = delete;
+  ScopedEvents &operator=(const ScopedEvents &) = delete;
+};
+
 // host memory that is page-locked (registered with or allocated by CUDA)
 static bool is_pinned_host(const void *p) {
   cudaPointerAttributes a;
@@ -396,8 +409,8 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
   }
   float t_norm = 0, t_dwt = 0, t_t1 = 0;
   for (int p = 0; p < info.nPar; ++p) {
-    cudaEvent_t a, b2, c2, d2;
-    cudaEventCreate(&a); cudaEventCreate(&b2); cudaEventCreate(&c2); cudaEventCreate(&d2);
+    const ScopedEvents evs;
+    cudaEvent_t a = evs.e[0], b2 = evs.e[1], c2 = evs.e[2], d2 = evs.e[3];
     cudaEventRecord(a, s);
     launch_fill_minmax(src + (uint64_t)p * n * dsz, dsz == 8, n, dv->temp.as<bwc_float>(),
                        dv->keys.as<uint64_t>() + 2 * p, s);
@@ -456,7 +469,6 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
     cudaEventElapsedTime(&x, a, b2); t_norm += x;
     cudaEventElapsedTime(&x, b2, c2); t_dwt += x;
     cudaEventElapsedTime(&x, c2, d2); t_t1 += x;
-    cudaEventDestroy(a); cudaEventDestroy(b2); cudaEventDestroy(c2); cudaEventDestroy(d2);
   }
 
   // tier-1 summary to the host
@@ -528,8 +540,6 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
   tile.slope_max = (uint16_t)hslopes[1];
 
   // tier 2 on the host
-  cudaEvent_t t2a;
-  cudaEventCreate(&t2a);
   const auto h0 = std::chrono::steady_clock::now();
   if (t2_encode(codec, tile)) return 0;
   std::vector<uint8_t> blob;
@@ -558,7 +568,6 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
   if (!out_dev) cudaMemcpyAsync(stream->out, csdst, total, cudaMemcpyDeviceToHost, s);
   cudaEventRecord(dv->ev[5], s);
   if (!cuda_ok(cudaStreamSynchronize(s), "codestream assembly")) return 0;
-  cudaEventDestroy(t2a);
 
   float up = 0, dl = 0, as = 0;
   cudaEventElapsedTime(&up, dv->ev[0], dv->ev[1]);
@@ -668,8 +677,8 @@ static uchar decompress_impl(bwc_codec *codec, bwc_stream *stream) {
     cudaMemsetAsync(dv->counter.p, 0, 4, s);
     launch_gather(dv->bytes.as<uint8_t>(), dcs, nullptr, dv->pieces.as<GatherPiece>(),
                   pieces.size(), s);
-    cudaEvent_t a, b2, c2, d2;
-    cudaEventCreate(&a); cudaEventCreate(&b2); cudaEventCreate(&c2); cudaEventCreate(&d2);
+    const ScopedEvents evs;
+    cudaEvent_t a = evs.e[0], b2 = evs.e[1], c2 = evs.e[2], d2 = evs.e[3];
     cudaEventRecord(a, s);
     cudaMemsetAsync(dv->temp.p, 0, n * sizeof(bwc_float), s);
     const int grid = t1_grid(nullptr, smem);
@@ -695,7 +704,6 @@ static uchar decompress_impl(bwc_codec *codec, bwc_stream *stream) {
     cudaEventElapsedTime(&x, a, b2); t_t1 += x;
     cudaEventElapsedTime(&x, b2, c2); t_dwt += x;
     cudaEventElapsedTime(&x, c2, d2); t_norm += x;
-    cudaEventDestroy(a); cudaEventDestroy(b2); cudaEventDestroy(c2); cudaEventDestroy(d2);
   }
   cudaEventRecord(dv->ev[2], s);
   if (!out_dev) cudaMemcpyAsync(stream->out, dout, out_bytes, cudaMemcpyDeviceToHost, s);
