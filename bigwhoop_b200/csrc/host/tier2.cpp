@@ -502,29 +502,42 @@ struct Probe {
   std::vector<RawBits> pools;   // tag-tree bits, one pool per piece
 };
 
-// appending to a bit string, most significant bit first
-static void bits_append(RawBits &rb, uint64_t v, int n) {   // the n (<= 57) low bits of v
-  while (n > 0) {
-    const int used = (int)(rb.n & 63);
-    if (used == 0) rb.words.push_back(0);
-    const int k = std::min(n, 64 - used);
-    const uint64_t chunk = (v >> (n - k)) & ((k == 64) ? ~0ull : ((1ull << k) - 1));
-    rb.words.back() |= chunk << (64 - used - k);
-    rb.n += (uint64_t)k;
-    n -= k;
+// Appends to a bit string, most significant bit first, through a 64-bit register: only whole
+// words are stored until finish() stores the rest.
+struct BitSink {
+  RawBits &rb;
+  uint64_t acc = 0;   // the pending bits (the low `nacc`; nothing above them)
+  int nacc = 0;
+  explicit BitSink(RawBits &r) : rb(r) { rb.clear(); }
+  void put(uint64_t v, int n) {   // the n (<= 57) low bits of v; v has no bits above them
+    if (nacc + n < 64) {
+      acc = (acc << n) | v;
+      nacc += n;
+    } else {
+      const int k = 64 - nacc;   // 7 <= k <= n: the bits of v that complete the word
+      rb.words.push_back((acc << k) | (v >> (n - k)));
+      nacc = n - k;
+      acc = nacc ? (v & ((1ull << nacc) - 1)) : 0;
+    }
+    rb.n += (uint64_t)n;
   }
-}
-static void bits_append_range(RawBits &rb, const RawBits &src, uint64_t off, uint64_t n) {
-  while (n) {
-    const uint64_t b = off & 63;
-    uint64_t m = 64 - b;
-    if (m > n) m = n;
-    if (m > 56) m = 56;
-    bits_append(rb, (src.words[off >> 6] << b) >> (64 - m), (int)m);
-    off += m;
-    n -= m;
+  void put_range(const RawBits &src, uint64_t off, uint64_t n) {
+    while (n) {
+      const uint64_t b = off & 63;
+      uint64_t m = 64 - b;
+      if (m > n) m = n;
+      if (m > 56) m = 56;
+      put((src.words[off >> 6] << b) >> (64 - m), (int)m);
+      off += m;
+      n -= m;
+    }
   }
-}
+  void finish() {
+    if (nacc) rb.words.push_back(acc << (64 - nacc));
+    nacc = 0;
+    acc = 0;
+  }
+};
 
 void build_records(Tile &tile, Probe &pr) {
   std::vector<const Codeblock *> all;
@@ -652,8 +665,7 @@ struct PieceResult {
 void probe_piece(const Probe &pr, uint16_t threshold, const ProbePiece &pc, PieceResult &out) {
   out.body = 0;
   out.e = false;
-  out.hdr.clear();
-  RawBits &hb = out.hdr;
+  BitSink hb(out.hdr);
   for (uint32_t i = pc.first; i < pc.first + pc.count; ++i) {
     const ProbeCb &c = pr.cbs[i];
     const uint32_t r = truncation_record(pr, c, threshold);
@@ -673,18 +685,18 @@ void probe_piece(const Probe &pr, uint16_t threshold, const ProbePiece &pc, Piec
     const int dz = cpq - c.zprev;
     if (dz > 0) out.e = true;
     if (c.zprev == 0) {
-      bits_append_range(hb, pr.pools[c.pool], c.incl_off, c.incl_n);
-      if (cpq) bits_append_range(hb, pr.pools[c.pool], c.msbs_off, c.msbs_n);
+      hb.put_range(pr.pools[c.pool], c.incl_off, c.incl_n);
+      if (cpq) hb.put_range(pr.pools[c.pool], c.msbs_off, c.msbs_n);
     } else {
-      bits_append(hb, dz ? 1 : 0, 1);
+      hb.put(dz ? 1 : 0, 1);
     }
     if (!dz) continue;
     // encode_delta_z
-    if (dz == 1) bits_append(hb, 0, 1);
-    else if (dz == 2) bits_append(hb, 2, 2);
-    else if (dz < 6) bits_append(hb, 12u | (uint32_t)(dz - 3), 4);
-    else if (dz < 37) bits_append(hb, (15u << 5) | (uint32_t)(dz - 6), 9);
-    else if (dz < 293) bits_append(hb, (511u << 8) | (uint32_t)(dz - 37), 17);
+    if (dz == 1) hb.put(0, 1);
+    else if (dz == 2) hb.put(2, 2);
+    else if (dz < 6) hb.put(12u | (uint32_t)(dz - 3), 4);
+    else if (dz < 37) hb.put((15u << 5) | (uint32_t)(dz - 6), 9);
+    else if (dz < 293) hb.put((511u << 8) | (uint32_t)(dz - 37), 17);
     // encode_length with the estimate state
     // here cpq = z > zprev: L[cpq - 1] is the record's, L[zprev - 1] the previous layer's
     const int16_t z_curr = cpq - 1, z_prev = c.zprev - 1;
@@ -696,12 +708,13 @@ void probe_piece(const Probe &pr, uint16_t threshold, const ProbePiece &pc, Piec
     max_beta = (max_beta < L_bits) ? (uint16_t)L_bits : max_beta;
     for (int n1 = max_beta - beta; n1 > 0; n1 -= 32) {
       const int m = n1 < 32 ? n1 : 32;
-      bits_append(hb, (1ull << m) - 1, m);
+      hb.put((1ull << m) - 1, m);
     }
-    bits_append(hb, 0, 1);
+    hb.put(0, 1);
     const int sh = max_beta + cp_bits - 1;
-    if (sh >= 0 && sh < 31) bits_append(hb, L & (uint32_t)((2ull << sh) - 1), sh + 1);
+    if (sh >= 0 && sh < 31) hb.put(L & (uint32_t)((2ull << sh) - 1), sh + 1);
   }
+  hb.finish();
 }
 
 // create_quality_layer(codec, tile, threshold, q, 1) for the tables of layer q, for several
