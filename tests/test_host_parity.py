@@ -21,6 +21,9 @@ CASES = [
     ((8, 20, 24, 30), "double", np.float64, (2, 2, 2, 1), (3, 3, 3, 1), "0.25,8"),
     ((40, 17, 90), "double", np.float64, (3, 2, 4, 0), (4, 3, 5, 0), "4,0.5"),
     ((1, 1, 300), "double", np.float64, (4, 0, 0, 0), (6, 0, 0, 0), "2"),
+    # eight layers: tag-tree and length-code state carried through many final headers
+    ((48, 40, 36), "double", np.float64, (2, 2, 2, 0), (4, 4, 3, 0),
+     "0.125,0.25,0.5,1,1.5,2,3,6"),
 ]
 
 
@@ -93,6 +96,7 @@ PRECINCT_CASES = [
     ((64, 64, 64), (3, 3, 3, 0), (3, 3, 3, 0), (4, 4, 4, 0), "0.5,2"),
     ((33, 47, 61), (2, 2, 2, 0), (3, 3, 3, 0), (4, 4, 5, 0), "1"),
     ((8, 20, 24, 30), (2, 2, 2, 1), (2, 2, 2, 1), (3, 3, 3, 1), "0.25,4"),
+    ((40, 36, 44), (2, 2, 2, 0), (3, 3, 3, 0), (4, 4, 4, 0), "0.1,0.3,0.6,1,2,5"),
 ]
 
 
