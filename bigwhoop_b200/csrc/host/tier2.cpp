@@ -99,12 +99,13 @@ static void encode_length(Writer &bw, Codeblock &cb, int q, uchar estimate) {
 extern thread_local bool t_rate_control_in_parallel_fields;
 
 // ---- parallel host loops ----------------------------------------------------------------------
-// Rate control and packet assembly work packet by packet: a packet's computations touch only its
-// own codeblocks, its precincts' tag trees and the packet itself, and every total they feed is
-// an integer sum.  So those loops run on a small persistent pool of host threads, with results
-// identical to running them in order: the final layer evaluation and the final headers over
-// chunks of packets, the probe tables and the probes over pieces of a packet's codeblocks (a
-// probe's per-codeblock work is independent; only its header bits are then counted in order).
+// Rate control and packet assembly split into independent parts: a subband's precinct at one
+// packet position (a segment) touches only its own codeblocks and tag trees, and every total
+// they feed is an integer sum.  So those loops run on a small persistent pool of host threads,
+// with results identical to running them in order: the final layer evaluation and the final
+// headers over segments (their header bits joined in order afterwards), the probe tables and
+// the probes over pieces of a packet's codeblocks (a probe's per-codeblock work is independent;
+// only its header bits are then counted in order).
 //
 // run(n, fn) calls fn(i) for every i in [0, n) on the pool's threads and the calling thread and
 // returns when all are done.  One call at a time: a second concurrent caller, a caller on one of
@@ -343,8 +344,9 @@ static int64_t truncate_segment(const bwc_gl_ctrl &c, const PacketRef &r, uint8_
   return size;
 }
 
-// create_quality_layer (tier2.c:896-1079), a packet at a time: the truncation points of the
-// packet's codeblocks (every subband's precinct at that position), then the packet's header
+// create_quality_layer (tier2.c:896-1079) for one packet: the truncation points of the packet's
+// codeblocks (every subband's precinct at that position), then the packet's header; used by the
+// probe cross-check (the final evaluation runs per segment)
 static int64_t quality_layer_packet(const bwc_gl_ctrl &c, const PacketRef &r, uint16_t threshold,
                                     int q, uchar est) {
   Resolution &res = *r.res;
