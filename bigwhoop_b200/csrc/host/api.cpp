@@ -202,6 +202,107 @@ static bool is_device_pointer(const void *p) {
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+// Copies between pageable host memory and the device through two page-locked chunks kept per
+// device: host threads fill (or empty) one chunk while the copy engine moves the other.  A copy
+// straight from or to pageable memory is staged by the driver through small buffers of its
+// own, several times slower.  Page-locked host memory is copied directly, and so is everything
+// when the chunks are in use by another call or cannot be allocated.
+class HostStaging {
+ public:
+  static constexpr uint64_t kChunk = 32ull << 20;
+  static constexpr uint64_t kMinBytes = 4ull << 20;   // smaller copies go directly
+
+  static HostStaging *for_device(int device) {
+    static std::mutex m;
+    static std::map<int, HostStaging *> all;   // kept for the process's lifetime
+    std::lock_guard<std::mutex> l(m);
+    HostStaging *&h = all[device];
+    if (!h) h = new (std::nothrow) HostStaging();
+    return h;
+  }
+
+  // host -> device; returns false (nothing copied) when the caller should copy directly
+  bool upload(void *dst, const void *src, uint64_t n, cudaStream_t s) {
+    std::unique_lock<std::mutex> busy(m_, std::try_to_lock);
+    if (!busy.owns_lock() || n < kMinBytes || is_pinned_host(src) || !ready()) return false;
+    for (uint64_t off = 0, k = 0; off < n; off += kChunk, ++k) {
+      const int h = (int)(k & 1);
+      const uint64_t len = std::min(kChunk, n - off);
+      cudaEventSynchronize(done_[h]);   // the copy that last read this chunk has finished
+      fill(buf_[h], static_cast<const uint8_t *>(src) + off, len);
+      if (cudaMemcpyAsync(static_cast<uint8_t *>(dst) + off, buf_[h], len,
+                          cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return fail();
+      cudaEventRecord(done_[h], s);
+    }
+    return true;
+  }
+
+  // device -> host, complete on return; false (nothing copied) when the caller should copy
+  // directly
+  bool download(void *dst, const void *src, uint64_t n, cudaStream_t s) {
+    std::unique_lock<std::mutex> busy(m_, std::try_to_lock);
+    if (!busy.owns_lock() || n < kMinBytes || is_pinned_host(dst) || !ready()) return false;
+    uint64_t prev_off = 0, prev_len = 0;
+    for (uint64_t off = 0, k = 0;; off += kChunk, ++k) {
+      const int h = (int)(k & 1);
+      const uint64_t len = off < n ? std::min(kChunk, n - off) : 0;
+      if (len) {
+        cudaEventSynchronize(done_[h]);
+        if (cudaMemcpyAsync(buf_[h], static_cast<const uint8_t *>(src) + off, len,
+                            cudaMemcpyDeviceToHost, s) != cudaSuccess)
+          return fail();
+        cudaEventRecord(done_[h], s);
+      }
+      if (prev_len) {   // while chunk k moves, empty chunk k - 1
+        if (cudaEventSynchronize(done_[h ^ 1]) != cudaSuccess) return fail();
+        fill(static_cast<uint8_t *>(dst) + prev_off, buf_[h ^ 1], prev_len);
+      }
+      if (!len) break;
+      prev_off = off;
+      prev_len = len;
+    }
+    return true;
+  }
+
+ private:
+  bool ready() {
+    if (buf_[0]) return true;
+    if (failed_) return false;
+    for (int h = 0; h < 2; ++h)
+      if (cudaHostAlloc(&buf_[h], kChunk, cudaHostAllocPortable) != cudaSuccess ||
+          cudaEventCreateWithFlags(&done_[h], cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        for (int j = 0; j < 2; ++j) {
+          if (buf_[j]) cudaFreeHost(buf_[j]);
+          if (done_[j]) cudaEventDestroy(done_[j]);
+          buf_[j] = nullptr;
+          done_[j] = nullptr;
+        }
+        failed_ = true;
+        return false;
+      }
+    return true;
+  }
+  static bool fail() {   // a copy could not be queued: the caller copies directly (and reports)
+    cudaGetLastError();
+    return false;
+  }
+  // one chunk, in slices on the host thread pool
+  static void fill(void *dst, const void *src, uint64_t len) {
+    constexpr uint64_t kSlice = 2ull << 20;
+    const size_t ns = (size_t)((len + kSlice - 1) / kSlice);
+    host_parallel(ns, [&](size_t i) {
+      const uint64_t a = i * kSlice, b = std::min(len, a + kSlice);
+      std::memcpy(static_cast<uint8_t *>(dst) + a, static_cast<const uint8_t *>(src) + a, b - a);
+    });
+  }
+  std::mutex m_;
+  void *buf_[2] = {nullptr, nullptr};
+  cudaEvent_t done_[2] = {nullptr, nullptr};
+  bool failed_ = false;
+};
+
 static DwtPlan make_plan(const bwc_gl_ctrl &c, const Parameter &par) {
   DwtPlan plan{};
   plan.levels = c.nDecomp;
@@ -328,7 +429,9 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
   const uint8_t *src = (const uint8_t *)stream->inp;
   if (!is_device_pointer(stream->inp)) {
     if (!dv->in.ensure(in_bytes)) return 0;
-    if (!cuda_ok(cudaMemcpyAsync(dv->in.p, stream->inp, in_bytes, cudaMemcpyHostToDevice, s), "upload"))
+    HostStaging *hs = HostStaging::for_device(dv->device);
+    if (!(hs && hs->upload(dv->in.p, stream->inp, in_bytes, s)) &&
+        !cuda_ok(cudaMemcpyAsync(dv->in.p, stream->inp, in_bytes, cudaMemcpyHostToDevice, s), "upload"))
       return 0;
     src = dv->in.as<uint8_t>();
   }
@@ -565,7 +668,11 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
   }
   launch_gather(csdst, dv->blob.as<uint8_t>(), dv->bytes.as<uint8_t>(),
                 dv->pieces.as<GatherPiece>(), pieces.size(), s);
-  if (!out_dev) cudaMemcpyAsync(stream->out, csdst, total, cudaMemcpyDeviceToHost, s);
+  if (!out_dev) {
+    HostStaging *hs = HostStaging::for_device(dv->device);
+    if (!(hs && hs->download(stream->out, csdst, total, s)))
+      cudaMemcpyAsync(stream->out, csdst, total, cudaMemcpyDeviceToHost, s);
+  }
   cudaEventRecord(dv->ev[5], s);
   if (!cuda_ok(cudaStreamSynchronize(s), "codestream assembly")) return 0;
 
@@ -608,7 +715,9 @@ static uchar decompress_impl(bwc_codec *codec, bwc_stream *stream) {
   const uint8_t *dcs = (const uint8_t *)stream->inp;
   if (!is_device_pointer(stream->inp)) {
     if (!dv->cs.ensure(cs_len)) return 1;
-    cudaMemcpyAsync(dv->cs.p, stream->inp, cs_len, cudaMemcpyHostToDevice, s);
+    HostStaging *hs = HostStaging::for_device(dv->device);
+    if (!(hs && hs->upload(dv->cs.p, stream->inp, cs_len, s)))
+      cudaMemcpyAsync(dv->cs.p, stream->inp, cs_len, cudaMemcpyHostToDevice, s);
     dcs = dv->cs.as<uint8_t>();
   }
   const bool out_dev = is_device_pointer(stream->out);
@@ -706,7 +815,11 @@ static uchar decompress_impl(bwc_codec *codec, bwc_stream *stream) {
     cudaEventElapsedTime(&x, c2, d2); t_norm += x;
   }
   cudaEventRecord(dv->ev[2], s);
-  if (!out_dev) cudaMemcpyAsync(stream->out, dout, out_bytes, cudaMemcpyDeviceToHost, s);
+  if (!out_dev) {
+    HostStaging *hs = HostStaging::for_device(dv->device);
+    if (!(hs && hs->download(stream->out, dout, out_bytes, s)))
+      cudaMemcpyAsync(stream->out, dout, out_bytes, cudaMemcpyDeviceToHost, s);
+  }
   cudaEventRecord(dv->ev[3], s);
   if (!cuda_ok(cudaStreamSynchronize(s), "decompression download")) return 1;
   float up = 0, dl = 0;

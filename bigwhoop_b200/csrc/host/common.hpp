@@ -10,6 +10,7 @@
 
 #include <cstdint>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -251,6 +252,8 @@ uchar tagtree_decode(TagTree &tt, BitReader &br, uint32_t threshold, uint64_t le
 // ---- tier 2 and codestream (tier2.cpp, codestream.cpp) ------------------------------------------
 uchar t2_encode(bwc_codec *codec, Tile &tile);
 extern thread_local bool t_rate_control_in_parallel_fields;
+// fn(i) for every i in [0, n) on the host thread pool of tier 2 (and the calling thread)
+void host_parallel(size_t n, const std::function<void(size_t)> &fn);
 uchar parse_packet(bwc_codec *codec, Tile &tile, Packet &packet, const uint8_t *cs,
                    uint64_t cs_len, uint64_t pos, uint64_t body_size);
 uchar sequence_packets(bwc_codec *codec, Tile &tile);

@@ -223,6 +223,10 @@ static std::vector<PacketRef> packet_list(Tile &tile) {
   return v;
 }
 
+void host_parallel(size_t n, const std::function<void(size_t)> &fn) {
+  WorkPool::instance().run(n, fn);
+}
+
 // fn(first, last) over contiguous chunks of [0, n), a few chunks per pool thread
 static void for_chunks(size_t n, const std::function<void(size_t, size_t)> &fn) {
   const size_t chunks = std::min(n, WorkPool::instance().size() * 4);

@@ -134,6 +134,48 @@ def test_device_buffers_match_host_buffers(gpu):
     assert n_bit_diffs(rec.cpu().numpy(), bwc.decompress_array(cs_host)) == 0
 
 
+def test_pageable_host_buffers_match_device_buffers(gpu):
+    """Inputs and outputs in pageable host memory large enough to go through the library's
+    page-locked staging chunks (32 MiB) in several pieces, the last one partial: the same bytes
+    as device-resident and page-locked buffers, both ways."""
+    import torch
+    f = fields.shock_field((200, 256, 264), 5, device="cuda")   # 103 MiB FP64
+    host = f.cpu().numpy()
+    kw = dict(decomp=(3, 3, 3, 0), codeblocks=(5, 5, 4, 0), rate="2,28")
+    bwc.reset_gain_state()
+    cs_host = bwc.compress_array(host, **kw)
+    assert len(cs_host) > (36 << 20)   # the codestream too spans two staging chunks
+    out_dev = torch.zeros(host.nbytes + (1 << 20), dtype=torch.uint8, device="cuda")
+    bwc.reset_gain_state()
+    c = bwc.Compressor(device_ptr=(f.data_ptr(), host.shape, host.dtype), out=out_dev.data_ptr(),
+                       **kw)
+    try:
+        n = c.compress()
+    finally:
+        c.close()
+    assert bytes(out_dev[:n].cpu().numpy()) == cs_host
+    pinned_in = f.cpu().pin_memory()
+    pinned_out = torch.zeros(host.nbytes + (1 << 20), dtype=torch.uint8).pin_memory()
+    bwc.reset_gain_state()
+    c = bwc.Compressor(device_ptr=(pinned_in.data_ptr(), host.shape, host.dtype),
+                       out=pinned_out.data_ptr(), **kw)
+    try:
+        n = c.compress()
+    finally:
+        c.close()
+    assert bytes(pinned_out[:n].numpy()) == cs_host
+    rec_host = bwc.decompress_array(cs_host)
+    rec_dev = torch.zeros(host.shape, dtype=torch.float64, device="cuda")
+    d = bwc.Decompressor(cs_host, out=rec_dev.data_ptr())
+    try:
+        d.decompress()
+    finally:
+        d.close()
+    assert n_bit_diffs(rec_dev.cpu().numpy(), rec_host) == 0
+    del f, rec_dev, out_dev
+    torch.cuda.empty_cache()
+
+
 def test_repeated_calls_are_deterministic(gpu):
     f = fields.shock_field((64, 72, 80), 3)
     outs = []
