@@ -298,7 +298,8 @@ class Compressor:
         if qm is not None:
             self.L.bwc_set_qm(self.codec, qm)
         if out is None:
-            self.out = np.zeros(nbytes + (1 << 16), dtype=np.uint8)
+            # not zero-filled: compress() reads back only the bytes the library wrote
+            self.out = np.empty(nbytes + (1 << 16), dtype=np.uint8)
             outp = self.out.ctypes.data
         else:
             self.out = out
@@ -374,7 +375,8 @@ class Decompressor:
         if hdr["nPar"] > 1:
             self.shape = (hdr["nPar"],) + self.shape
         self.dtype = np.float64 if hdr["data_prec"] == 8 else np.float32
-        self.out = np.zeros(self.shape, dtype=self.dtype) if out is None else out
+        # decompression writes every value of the field
+        self.out = np.empty(self.shape, dtype=self.dtype) if out is None else out
         self.codec = self.L.bwc_alloc_decoder()
         outp = self.out.ctypes.data if hasattr(self.out, "ctypes") else self.out
         self.stream = self.L.bwc_init_stream(self.cs.ctypes.data, outp, DECOMP)
