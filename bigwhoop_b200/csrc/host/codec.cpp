@@ -845,6 +845,12 @@ extern "C" uchar bwc_create_compression(bwc_codec *const codec, bwc_stream *cons
          "o##########################################################o\n");
     return 1;
   }
+  if (c->quantization_style != bwc_qt_derived) {
+    warn("o##########################################################o\n"
+         "| ERROR: this library implements derived quantisation only |\n"
+         "o##########################################################o\n");
+    return 1;
+  }
   if (create_codec(codec)) return 1;
   c->headerSize = 111 + (uint64_t)info->nPar * c->nTiles * 2 * kPrecByte + c->nLayers * 4;
   if (stream->codestream.aux) c->headerSize += 6 + stream->codestream.aux->size;

@@ -295,6 +295,19 @@ uchar parse_main_header(bwc_codec *codec, bwc_stream *data, BitReader &br) {
                "o##########################################################o\n");
           return 1;
         }
+        if (c.KernelX != bwc_dwt_9_7 || c.KernelY != bwc_dwt_9_7 || c.KernelZ != bwc_dwt_9_7 ||
+            (c.KernelTS != bwc_dwt_9_7 && c.decompTS > 0 && info.nTS > 1)) {
+          warn("o##########################################################o\n"
+               "| ERROR: this library implements the CDF 9/7 wavelet only  |\n"
+               "o##########################################################o\n");
+          return 1;
+        }
+        if (c.quantization_style != bwc_qt_derived) {
+          warn("o##########################################################o\n"
+               "| ERROR: this library implements derived quantisation only |\n"
+               "o##########################################################o\n");
+          return 1;
+        }
         if (build_geometry(codec)) return 1;
         sgc = true;
         break;

@@ -219,3 +219,88 @@ def test_create_decompression_rejects_truncated_codestream():
         finally:
             L.bwc_free_codec(c)
             C.CDLL(None).free(C.c_void_p(s))
+
+
+@pytest.mark.parametrize("case", ["two_tiles", "kernel_5_3", "kernel_haar", "no_quantisation"])
+def test_create_compression_rejects_configurations_off_the_accelerated_path(case):
+    """Multi-tile codestreams, the 5/3 and Haar kernels and bwc_qt_none are not on the
+    accelerated path: bwc_create_compression refuses them with return code 1 (the default
+    configuration of the same field is accepted)."""
+    f = np.zeros((16, 16, 16))
+    out = np.zeros(1 << 16, np.uint8)
+    L = C.CDLL(bwc.lib_path("double"))
+    L.bwc_alloc_coder.restype = C.c_void_p
+    L.bwc_alloc_coder.argtypes = [C.c_uint64] * 4 + [C.c_uint8, C.c_int]
+    L.bwc_init_stream.restype = C.c_void_p
+    L.bwc_init_stream.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+    L.bwc_create_compression.restype = C.c_uint8
+    L.bwc_create_compression.argtypes = [C.c_void_p, C.c_void_p, C.c_char_p]
+    L.bwc_free_codec.argtypes = [C.c_void_p]
+    L.bwc_set_tiles.argtypes = [C.c_void_p] + [C.c_uint64] * 4 + [C.c_int]
+    L.set_kernels.argtypes = [C.c_void_p] + [C.c_int] * 4
+    L.set_quant_style.argtypes = [C.c_void_p, C.c_int]
+    for configure in (False, True):
+        c = L.bwc_alloc_coder(16, 16, 16, 1, 1, 8)
+        s = L.bwc_init_stream(f.ctypes.data, out.ctypes.data, bwc.COMP)
+        try:
+            if configure:
+                if case == "two_tiles":
+                    L.bwc_set_tiles(c, 8, 16, 16, 1, 0)   # bwc_tile_sizeof: 8 x 16 x 16 tiles
+                elif case == "kernel_5_3":
+                    L.set_kernels(c, 1, 1, 1, 1)
+                elif case == "kernel_haar":
+                    L.set_kernels(c, 2, 2, 2, 2)
+                else:
+                    L.set_quant_style(c, 0)
+            rc = L.bwc_create_compression(c, s, C.create_string_buffer(b"2"))
+            assert rc == (1 if configure else 0), (case, configure)
+        finally:
+            L.bwc_free_codec(c)
+            C.CDLL(None).free(C.c_void_p(s))
+
+
+@pytest.mark.parametrize("case", ["default", "kernel_5_3"])
+def test_create_decompression_rejects_codestreams_off_the_accelerated_path(case):
+    """A reference codestream made with the 5/3 kernel is refused by bwc_create_decompression
+    (return code 1) instead of being decoded as 9/7.  The reference's own bwc_compress crashes
+    (segmentation fault, some runs) with the Haar kernel or without quantisation on this input,
+    so no such codestream is made here; the header checks for them are the same."""
+    need_ref("double")
+    from oracle import ref
+    from bigwhoop_b200 import fields
+    f = fields.spectral_field((16, 16, 16), 3)
+    out = np.zeros(1 << 20, np.uint8)
+    R = C.CDLL(ref.lib_path("double"))
+    R.bwc_alloc_coder.restype = C.c_void_p
+    R.bwc_alloc_coder.argtypes = [C.c_uint64] * 4 + [C.c_uint8, C.c_int]
+    R.bwc_init_stream.restype = C.c_void_p
+    R.bwc_init_stream.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+    R.bwc_create_compression.restype = C.c_uint8
+    R.bwc_create_compression.argtypes = [C.c_void_p, C.c_void_p, C.c_char_p]
+    R.bwc_compress.restype = C.c_size_t
+    R.bwc_compress.argtypes = [C.c_void_p, C.c_void_p]
+    R.bwc_free_codec.argtypes = [C.c_void_p]
+    R.set_kernels.argtypes = [C.c_void_p] + [C.c_int] * 4
+    c = R.bwc_alloc_coder(16, 16, 16, 1, 1, 8)
+    s = R.bwc_init_stream(f.ctypes.data, out.ctypes.data, bwc.COMP)
+    try:
+        if case == "kernel_5_3":
+            R.set_kernels(c, 1, 1, 1, 1)
+        assert R.bwc_create_compression(c, s, C.create_string_buffer(b"4")) == 0
+        n = R.bwc_compress(c, s)
+        assert n > 0
+    finally:
+        R.bwc_free_codec(c)
+        C.CDLL(None).free(C.c_void_p(s))
+    cs = np.zeros(n + 64, np.uint8)
+    cs[:n] = out[:n]
+    L = _lib()
+    rec = np.zeros(f.size, np.float64)
+    d = L.bwc_alloc_decoder()
+    st = L.bwc_init_stream(cs.ctypes.data, rec.ctypes.data, bwc.DECOMP)
+    try:
+        rc = L.bwc_create_decompression(d, st, 0)
+    finally:
+        L.bwc_free_codec(d)
+        C.CDLL(None).free(C.c_void_p(st))
+    assert rc == (0 if case == "default" else 1), case
