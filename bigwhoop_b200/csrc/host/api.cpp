@@ -1319,12 +1319,12 @@ using namespace bwcb;
 
 extern "C" size_t bwc_compress(bwc_codec *const codec, bwc_stream *const data) {
   if (!codec || !data) return 0;
-  return compress_impl(codec, data);
+  return guarded<size_t>(0, [&] { return compress_impl(codec, data); });
 }
 
 extern "C" uchar bwc_decompress(bwc_codec *const codec, bwc_stream *const stream) {
   if (!codec || !stream) return 1;
-  return decompress_impl(codec, stream);
+  return guarded<uchar>(1, [&] { return decompress_impl(codec, stream); });
 }
 
 extern "C" int bwc_b200_precision_bits(void) { return kPrecBit; }
@@ -1363,7 +1363,7 @@ extern "C" int bwc_b200_last_timings(bwc_codec *const codec, double *out_ms, int
 extern "C" uchar bwc_b200_compress_batch(bwc_codec *const *codecs, bwc_stream *const *streams,
                                          uint32 n, size_t *sizes) {
   if (!codecs || !streams || !sizes || n == 0) return 1;
-  return compress_batch_impl(codecs, streams, n, sizes);
+  return guarded<uchar>(1, [&] { return compress_batch_impl(codecs, streams, n, sizes); });
 }
 
 extern "C" int bwc_b200_last_batch_timings(double *out_ms, int n) {

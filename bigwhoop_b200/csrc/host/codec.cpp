@@ -660,6 +660,26 @@ static uchar init_subband(bwc_codec *codec, Parameter &par, uint32_t r, uint8_t 
 uchar build_geometry(bwc_codec *codec) {
   const bwc_gl_ctrl &c = codec->control;
   const bwc_gl_inf &info = codec->info;
+  // A geometry no device could hold (from a corrupt header, say) is refused before it is
+  // built: building it codeblock by codeblock would run for hours, or exhaust host memory
+  // (about 2 KB a codeblock).  The bound, 2^21 codeblocks at the field's codeblock size, is
+  // over ten times the codeblocks of the largest field whose compression fits a B200's memory
+  // (about 77 bytes of device memory a value, 32 x 32 x 16 codeblocks).
+  {
+    const uint64_t n[4] = {info.nX, info.nY, info.nZ, info.nTS};
+    const uint64_t tsz[4] = {c.tileSizeX, c.tileSizeY, c.tileSizeZ, c.tileSizeTS};
+    const uint8_t cb[4] = {c.cbX, c.cbY, c.cbZ, c.cbTS};
+    double cells = info.nPar;
+    bool empty = info.nPar == 0;
+    for (int a = 0; a < 4; ++a) {
+      empty = empty || n[a] == 0 || tsz[a] == 0;
+      cells *= std::ceil((double)n[a] / std::ldexp(1.0, cb[a] < 63 ? cb[a] : 63));
+    }
+    if (empty || cells > (double)(1ull << 21)) {
+      warn(kMemError);
+      return 1;
+    }
+  }
   free_engine(codec);
   bwc_b200_engine *eng = new (std::nothrow) bwc_b200_engine();
   if (!eng) {
@@ -779,8 +799,14 @@ extern "C" uchar create_codec(bwc_codec *const codec) { return bwcb::build_geome
 // ---------------------------------------------------------------------------------------------
 // bwc_create_compression: rate string parsing (libbwc.c:2970-3131)
 // ---------------------------------------------------------------------------------------------
+static uchar bwc_create_compression_body(bwc_codec *const codec, bwc_stream *const stream, char *const rate_control);
+
 extern "C" uchar bwc_create_compression(bwc_codec *const codec, bwc_stream *const stream,
                                         char *const rate_control) {
+  return guarded<uchar>(1, [&] { return bwc_create_compression_body(codec, stream, rate_control); });
+}
+
+static uchar bwc_create_compression_body(bwc_codec *const codec, bwc_stream *const stream, char *const rate_control) {
   bwc_gl_ctrl *c = &codec->control;
   bwc_gl_inf *info = &codec->info;
   size_t size = 10;

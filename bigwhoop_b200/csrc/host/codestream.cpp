@@ -494,7 +494,13 @@ uchar parse_codestream(bwc_codec *codec, bwc_stream *data, uint8_t layer) {
 
 using namespace bwcb;
 
+static bwc_header * bwc_open_header_body(void *const inpbuf);
+
 extern "C" bwc_header *bwc_open_header(void *const inpbuf) {
+  return guarded<bwc_header *>(nullptr, [&] { return bwc_open_header_body(inpbuf); });
+}
+
+static bwc_header * bwc_open_header_body(void *const inpbuf) {
   bwc_stream *data = bwc_init_stream(inpbuf, nullptr, decomp);
   bwc_codec *codec = bwc_alloc_decoder();
   if (!data || !codec) {
@@ -551,8 +557,14 @@ extern "C" void bwc_close_header(bwc_header *const header) {
   free(header);
 }
 
+static uchar bwc_create_decompression_body(bwc_codec *const codec, bwc_stream *const stream, uint8 const layer);
+
 extern "C" uchar bwc_create_decompression(bwc_codec *const codec, bwc_stream *const stream,
                                           uint8 const layer) {
+  return guarded<uchar>(1, [&] { return bwc_create_decompression_body(codec, stream, layer); });
+}
+
+static uchar bwc_create_decompression_body(bwc_codec *const codec, bwc_stream *const stream, uint8 const layer) {
   if (!codec || !stream) return 1;
   return parse_codestream(codec, stream, layer) ? 1 : 0;
 }

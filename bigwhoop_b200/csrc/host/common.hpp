@@ -274,4 +274,18 @@ void warn(const char *msg);
 extern const char *kMemError;
 extern const char *kCsError;
 
+// No C++ exception may cross the C API (a corrupt codestream can ask for an impossible
+// geometry, and std::bad_alloc would end the caller's process): every entry point that
+// allocates runs its body through this and returns `on_error` instead, after the reference's
+// memory-error message.
+template <class R, class F>
+R guarded(R on_error, F &&body) noexcept {
+  try {
+    return body();
+  } catch (...) {
+    warn(kMemError);
+  }
+  return on_error;
+}
+
 }  // namespace bwcb

@@ -51,12 +51,18 @@ extern "C" int bwc_b200_parsed_codeblock(bwc_codec *const codec, uint8 const par
   return 0;
 }
 
+static size_t bwc_b200_assemble_from_tier1_body(bwc_codec *const codec, bwc_stream *const stream, uint8 const *K, uint8 const *Z, uint64 const *L, uint16 const *S, uint8 const *bytes, uint64 const *byte_offsets, bwc_float const *minmax, uint16 const slope_min, uint16 const slope_max);
+
 extern "C" size_t bwc_b200_assemble_from_tier1(bwc_codec *const codec, bwc_stream *const stream,
                                                uint8 const *K, uint8 const *Z, uint64 const *L,
                                                uint16 const *S, uint8 const *bytes,
                                                uint64 const *byte_offsets,
                                                bwc_float const *minmax, uint16 const slope_min,
                                                uint16 const slope_max) {
+  return guarded<size_t>(0, [&] { return bwc_b200_assemble_from_tier1_body(codec, stream, K, Z, L, S, bytes, byte_offsets, minmax, slope_min, slope_max); });
+}
+
+static size_t bwc_b200_assemble_from_tier1_body(bwc_codec *const codec, bwc_stream *const stream, uint8 const *K, uint8 const *Z, uint64 const *L, uint16 const *S, uint8 const *bytes, uint64 const *byte_offsets, bwc_float const *minmax, uint16 const slope_min, uint16 const slope_max) {
   if (!codec || !codec->tile || codec->tile->tiles.empty()) return 0;
   Tile &tile = codec->tile->tiles[0];
   uint64_t g = 0;

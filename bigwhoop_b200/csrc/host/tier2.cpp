@@ -1072,8 +1072,11 @@ uchar t2_encode(bwc_codec *codec, Tile &tile) {
   return 0;
 }
 
-static void decode_length(BitReader &br, Codeblock &cb, int q) {
-  while (br.get_bit()) cb.beta++;
+// false on a run of 1 bits longer than any length code needs: a corrupt or truncated header
+// (past its end the reader yields 1 bits, so the loop would not end)
+static bool decode_length(BitReader &br, Codeblock &cb, int q) {
+  while (br.get_bit())
+    if (++cb.beta > 64) return false;
   int16_t *cp = cb.cp();
   const int16_t z_curr = cp[q] - 1, z_prev = cp[q - 1] - 1;
   uint16_t L_bits = (uint16_t)(cb.beta + ilog2_u16((uint64_t)(z_curr - z_prev)));
@@ -1083,6 +1086,7 @@ static void decode_length(BitReader &br, Codeblock &cb, int q) {
     i |= br.get_bit();
   }
   cb.enc.L[z_curr] = ((z_prev >= 0) ? cb.enc.L[z_prev] : 0) + i;
+  return true;
 }
 
 // parse_packet (tier2.c:1364-1684).  `pos` is the packet's first byte in the codestream,
@@ -1111,8 +1115,9 @@ uchar parse_packet(bwc_codec *codec, Tile &tile, Packet &pk, const uint8_t *cs, 
           if (pr.incl.nodes[k].value <= q) {
             dz = 1;
             uint32_t kk = 1;
-            while (tagtree_decode(pr.msbs, br, kk++, k)) {
-            }
+            while (tagtree_decode(pr.msbs, br, kk++, k))
+              if (kk > 255) return 1;   // no bit-plane count is this large: corrupt header
+            if (pr.msbs.nodes[k].value > sb.Kmax) return 1;   // more missing planes than exist
             cb.enc.Kmsbs = (uint8_t)pr.msbs.nodes[k].value;
           }
         } else {
@@ -1122,8 +1127,11 @@ uchar parse_packet(bwc_codec *codec, Tile &tile, Packet &pk, const uint8_t *cs, 
         if (dz) {
           dz = decode_delta_z(br);
           cp[q] += dz;
+          // no more passes than the codeblock's bit planes have (3 K - 2): a corrupt header
+          // would otherwise index past the pass tables here and in the decoder
+          if (cp[q] > 3 * (int)(sb.Kmax - cb.enc.Kmsbs) - 2 || cp[q] > kMaxPasses) return 1;
           cb.enc.Z = (uint8_t)cp[q];
-          decode_length(br, cb, q);
+          if (!decode_length(br, cb, q)) return 1;
         }
       } else {
         cp[q] = cp[q - 1];
