@@ -76,7 +76,7 @@ struct CodedBlock {
   uint8_t K = 0;
   uint8_t Kmsbs = 0;
   uint8_t Z = 0;
-  uint64_t L[kMaxPasses] = {};
+  uint32_t L[kMaxPasses] = {};   // cumulative codeword bytes after each pass (< 4 GiB)
   uint16_t S[kMaxPasses + 1] = {};
 };
 

@@ -47,7 +47,8 @@ extern "C" int bwc_b200_parsed_codeblock(bwc_codec *const codec, uint8 const par
   meta3[0] = par->subbands[cb.subband].Kmax - cb.enc.Kmsbs;
   meta3[1] = cb.enc.Kmsbs;
   meta3[2] = cb.enc.Z;
-  if (L) std::memcpy(L, cb.enc.L, sizeof(cb.enc.L));
+  if (L)
+    for (int j = 0; j < kMaxPasses; ++j) L[j] = cb.enc.L[j];
   return 0;
 }
 
@@ -75,7 +76,7 @@ static size_t bwc_b200_assemble_from_tier1_body(bwc_codec *const codec, bwc_stre
       e.K = K[g];
       e.Z = Z[g];
       e.Kmsbs = e.K ? (uint8_t)(par.subbands[cb.subband].Kmax - e.K) : 0;
-      for (int j = 0; j < e.Z; ++j) e.L[j] = L[g * kMaxPasses + j];
+      for (int j = 0; j < e.Z; ++j) e.L[j] = (uint32_t)L[g * kMaxPasses + j];
       for (int j = 0; j <= e.Z; ++j) e.S[j] = S[g * (kMaxPasses + 1) + j];
       cb.data_off = byte_offsets[g];
       ++g;
