@@ -720,6 +720,15 @@ uchar build_geometry(bwc_codec *codec) {
             par.pmin = kFltMax;
             par.box = tile.box;
             par.res.resize(c.nDecomp + 1);
+            {
+              // room for about the codeblocks the tile will have (codeblocks are large: growing
+              // the vector a doubling at a time would move them several times)
+              double cells = 1.0;
+              const uint64_t ext[4] = {tile.box.nx(), tile.box.ny(), tile.box.nz(), tile.box.nt()};
+              const uint8_t cbe[4] = {c.cbX, c.cbY, c.cbZ, c.cbTS};
+              for (int a = 0; a < 4; ++a) cells *= std::ceil((double)ext[a] / std::ldexp(1.0, cbe[a]));
+              par.codeblocks.reserve((size_t)(cells * 1.25) + 64);
+            }
             for (int r = 0; r < c.nDecomp + 1; ++r) {
               Resolution &res = par.res[r];
               res.box.X0 = res_bound(par.box.X0, std::min<int>(c.nDecomp - r, c.decompX));
