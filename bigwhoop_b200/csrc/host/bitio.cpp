@@ -174,6 +174,47 @@ void tagtree_estimate(const TagTree &tt, RawBits &out, uint32_t threshold, uint6
   tagtree_walk(tt, out, threshold, leaf, false);
 }
 
+// tagtree_decode(tt, br, t, leaf) for t = 1, 2, ... while it returns 1 (the packet parser's
+// loop over a codeblock's missing bit planes, tier2.c), in one walk setting: a node whose
+// value and whose ancestors' values are all known is left as it is by every later call, so
+// each call starts below that prefix.  The same bits are read in the same order.  Returns false
+// when the leaf is still unknown after the call with t = tmax.
+bool tagtree_decode_until_known(TagTree &tt, BitReader &br, uint64_t leaf, uint32_t tmax) {
+  int64_t branch[64];
+  int nb = 0;
+  int64_t n = (int64_t)leaf;
+  while (n >= 0) {
+    if (tt.nodes[n].value == 0xFFFF) tt.nodes[n].value = 0;
+    branch[nb++] = n;
+    n = tt.nodes[n].parent;
+  }
+  int first = nb - 1;        // highest node on the path whose value is not yet known
+  uint32_t tmin_first = 0;   // what its parent hands down
+  for (uint32_t t = 1;; ++t) {
+    uint32_t tmin = tmin_first;
+    for (int i = first; i >= 0; --i) {
+      TagNode &node = tt.nodes[branch[i]];
+      if (node.threshold < tmin) {
+        node.value = (uint16_t)tmin;
+        node.threshold = (uint16_t)tmin;
+      }
+      while ((node.value == node.threshold) && (node.threshold < t)) {
+        node.threshold++;
+        if (!br.get_bit()) node.value++;
+      }
+      tmin = std::min<uint32_t>(node.value, node.threshold);
+    }
+    while (first >= 0) {   // extend the known prefix
+      const TagNode &node = tt.nodes[branch[first]];
+      if (node.value >= node.threshold) break;
+      tmin_first = node.value;
+      --first;
+    }
+    if (tt.nodes[leaf].value < t) return true;
+    if (t >= tmax) return false;
+  }
+}
+
 uchar tagtree_decode(TagTree &tt, BitReader &br, uint32_t threshold, uint64_t leaf) {
   int64_t branch[64];
   int nb = 0;

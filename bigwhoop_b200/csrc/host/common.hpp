@@ -248,6 +248,7 @@ void tagtree_encode_bits(TagTree &tt, RawBits &out, uint32_t threshold, uint64_t
 // the bits an estimating tagtree_encode would emit (the tree is left unchanged)
 void tagtree_estimate(const TagTree &tt, RawBits &out, uint32_t threshold, uint64_t leaf);
 uchar tagtree_decode(TagTree &tt, BitReader &br, uint32_t threshold, uint64_t leaf);
+bool tagtree_decode_until_known(TagTree &tt, BitReader &br, uint64_t leaf, uint32_t tmax);
 
 // ---- tier 2 and codestream (tier2.cpp, codestream.cpp) ------------------------------------------
 uchar t2_encode(bwc_codec *codec, Tile &tile);

@@ -1114,9 +1114,8 @@ uchar parse_packet(bwc_codec *codec, Tile &tile, Packet &pk, const uint8_t *cs, 
           tagtree_decode(pr.incl, br, (uint32_t)(q + 1), k);
           if (pr.incl.nodes[k].value <= q) {
             dz = 1;
-            uint32_t kk = 1;
-            while (tagtree_decode(pr.msbs, br, kk++, k))
-              if (kk > 255) return 1;   // no bit-plane count is this large: corrupt header
+            // no bit-plane count reaches 255: beyond it the header is corrupt
+            if (!tagtree_decode_until_known(pr.msbs, br, k, 255)) return 1;
             if (pr.msbs.nodes[k].value > sb.Kmax) return 1;   // more missing planes than exist
             cb.enc.Kmsbs = (uint8_t)pr.msbs.nodes[k].value;
           }
