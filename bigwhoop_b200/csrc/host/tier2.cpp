@@ -1160,6 +1160,7 @@ uchar parse_packet(bwc_codec *codec, Tile &tile, Packet &pk, const uint8_t *cs, 
           const uint32_t end = (cp[q] == 0) ? 0 : (uint32_t)cb.enc.L[cp[q] - 1];
           const uint32_t size = end - start;
           if (at + size > cs_len) return 1;
+          if (cb.chunks.empty()) cb.chunks.reserve(codec->control.nLayers);   // one allocation
           cb.chunks.emplace_back(at, size);
           at += size;
           pk.body_size += size;
