@@ -42,6 +42,7 @@ def load(precision="double"):
     L.rp_compress_full.restype = C.c_size_t
     L.rp_compress_full.argtypes = [vp]
     L.rp_set_precincts.argtypes = [u8p]
+    L.rp_set_kernels.argtypes = [u8p]
     for n in ("rp_stage_normalize", "rp_stage_dwt", "rp_stage_t1", "rp_dstage_t1",
               "rp_dstage_idwt", "rp_dstage_finish"):
         getattr(L, n).restype = C.c_int
@@ -99,7 +100,7 @@ class RefCompressor:
     """One reference compression, optionally run stage by stage."""
 
     def __init__(self, field, *, precision="double", decomp=None, cb=None, qm=-1, erres=False,
-                 rate="2", n_par=None, precincts=None):
+                 rate="2", n_par=None, precincts=None, kernels=None):
         self.L = load(precision)
         self.precision = precision
         f = np.ascontiguousarray(field)
@@ -119,10 +120,12 @@ class RefCompressor:
         self.out = np.zeros(f.nbytes + (1 << 16), dtype=np.uint8)
         rate_b = None if rate is None else rate.encode()
         self.L.rp_set_precincts(_u8arr(precincts))
+        self.L.rp_set_kernels(_u8arr(kernels))   # (x, y, z, t): 0 CDF 9/7, 1 LeGall 5/3
         try:
             self.h = self._open(f, dims, n_par, decomp, cb, qm, erres, rate_b)
         finally:
             self.L.rp_set_precincts(None)
+            self.L.rp_set_kernels(None)
         if not self.h:
             raise RuntimeError("reference rejected the configuration")
 

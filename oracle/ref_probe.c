@@ -85,6 +85,16 @@ void rp_set_precincts(const uint8 *p)
    else  rp_prec_set = 0;
 }
 
+/* wavelet kernels per axis (bwc_dwt_filter values) applied by the next rp_open_compress calls;
+ * NULL: defaults (CDF 9/7) */
+static uint8 rp_kern[4];
+static int   rp_kern_set = 0;
+void rp_set_kernels(const uint8 *k)
+{
+   if(k) { memcpy(rp_kern, k, 4); rp_kern_set = 1; }
+   else  rp_kern_set = 0;
+}
+
 rp_handle *rp_open_compress(void *field, uint64 nX, uint64 nY, uint64 nZ, uint64 nTS,
                             uint8 nPar, int data_prec, const uint8 *decomp, const uint8 *cb,
                             int qm, int erres, const char *rate, void *out)
@@ -97,6 +107,8 @@ rp_handle *rp_open_compress(void *field, uint64 nX, uint64 nY, uint64 nZ, uint64
    if(decomp) bwc_set_decomp(h->codec, decomp[0], decomp[1], decomp[2], decomp[3]);
    if(cb)     bwc_set_codeblocks(h->codec, cb[0], cb[1], cb[2], cb[3]);
    if(rp_prec_set) bwc_set_precincts(h->codec, rp_prec[0], rp_prec[1], rp_prec[2], rp_prec[3]);
+   if(rp_kern_set) set_kernels(h->codec, (bwc_dwt_filter)rp_kern[0], (bwc_dwt_filter)rp_kern[1],
+                               (bwc_dwt_filter)rp_kern[2], (bwc_dwt_filter)rp_kern[3]);
    if(qm >= 0) bwc_set_qm(h->codec, (uint8)qm);
    h->stream = bwc_init_stream(field, out, comp);
    if(rate)

@@ -141,6 +141,19 @@ static void lift_inverse(rs_float *w, int64_t len) {
   for (int64_t i = -3; i < len + 1; i += 2) w[i] -= L_ALPHA * (w[i - 1] + w[i + 1]);
 }
 
+/* LeGall 5/3 lifting, dwt.c:478-558: the predictor halves the neighbour sum, the update adds
+ * (sum + 2) / 4 -- the integer 5/3 rounding offset, applied here in floating point exactly as
+ * the reference does */
+static void lift_forward_53(rs_float *w, int64_t len) {
+  for (int64_t i = -1; i < len + 1; i += 2) w[i] -= (w[i - 1] + w[i + 1]) / 2;
+  for (int64_t i = 0; i < len; i += 2) w[i] += (w[i - 1] + w[i + 1] + 2) / 4;
+}
+
+static void lift_inverse_53(rs_float *w, int64_t len) {
+  for (int64_t i = -2; i < len + 1; i += 2) w[i] -= (w[i - 1] + w[i + 1] + 2) / 4;
+  for (int64_t i = -1; i < len; i += 2) w[i] += (w[i - 1] + w[i + 1]) / 2;
+}
+
 /* extent of the region transformed at `level` along an axis of n samples with `levels`
  * decompositions: the resolution box ceil((float)n / 2^min(level, levels))
  * (libbwc.c:1539-1548) */
@@ -152,7 +165,7 @@ static uint64_t level_extent(uint64_t n, int level, int levels) {
 /* transform every line along axis `a` of the region ext[] (forward: de-interleave lows first,
  * dwt.c:645-721; inverse: interleave first, dwt.c:170-272) */
 static void transform_axis(rs_float *work, const uint64_t dims[4], const uint64_t ext[4], int a,
-                           int forward, rs_float *line) {
+                           int forward, int kernel, rs_float *line) {
   const uint64_t stride[4] = {1, dims[0], dims[0] * dims[1], dims[0] * dims[1] * dims[2]};
   const int64_t len = (int64_t)ext[a];
   const int64_t half = (len + 1) / 2;
@@ -167,7 +180,7 @@ static void transform_axis(rs_float *work, const uint64_t dims[4], const uint64_
         if (forward) {
           for (int64_t i = 0; i < len; ++i) w[i] = base[i * stride[a]];
           extend(w, len);
-          lift_forward(w, len);
+          if (kernel == 1) lift_forward_53(w, len); else lift_forward(w, len);
           for (int64_t i = 0; i < len; ++i) {
             const int64_t dst = (i % 2 == 0) ? i / 2 : half + i / 2;
             base[dst * stride[a]] = w[i];
@@ -178,13 +191,14 @@ static void transform_axis(rs_float *work, const uint64_t dims[4], const uint64_
             w[i] = base[src * stride[a]];
           }
           extend(w, len);
-          lift_inverse(w, len);
+          if (kernel == 1) lift_inverse_53(w, len); else lift_inverse(w, len);
           for (int64_t i = 0; i < len; ++i) base[i * stride[a]] = w[i];
         }
       }
 }
 
-static void dwt(rs_float *work, const uint64_t dims[4], const uint8_t decomp[4], int forward) {
+static void dwt(rs_float *work, const uint64_t dims[4], const uint8_t decomp[4], int forward,
+                const uint8_t kernels[4]) {
   int n_levels = 0;
   for (int a = 0; a < 4; ++a)
     if (decomp[a] > n_levels) n_levels = decomp[a];
@@ -198,18 +212,31 @@ static void dwt(rs_float *work, const uint64_t dims[4], const uint8_t decomp[4],
     for (int a = 0; a < 4; ++a) ext[a] = level_extent(dims[a], level, decomp[a]);
     for (int q = 0; q < 4; ++q) {
       const int a = forward ? q : 3 - q; /* x, y, z, t forward; t, z, y, x inverse */
-      if (level < decomp[a] && ext[a] > 1) transform_axis(work, dims, ext, a, forward, line);
+      if (level < decomp[a] && ext[a] > 1)
+        transform_axis(work, dims, ext, a, forward, kernels[a], line);
     }
   }
   free(line);
 }
 
+static const uint8_t CDF97[4] = {0, 0, 0, 0};
+
 void rs_dwt_forward(rs_float *work, const uint64_t dims[4], const uint8_t decomp[4]) {
-  dwt(work, dims, decomp, 1);
+  dwt(work, dims, decomp, 1, CDF97);
 }
 
 void rs_dwt_inverse(rs_float *work, const uint64_t dims[4], const uint8_t decomp[4]) {
-  dwt(work, dims, decomp, 0);
+  dwt(work, dims, decomp, 0, CDF97);
+}
+
+void rs_dwt_forward_kernels(rs_float *work, const uint64_t dims[4], const uint8_t decomp[4],
+                            const uint8_t kernels[4]) {
+  dwt(work, dims, decomp, 1, kernels);
+}
+
+void rs_dwt_inverse_kernels(rs_float *work, const uint64_t dims[4], const uint8_t decomp[4],
+                            const uint8_t kernels[4]) {
+  dwt(work, dims, decomp, 0, kernels);
 }
 
 /* ---- coding tables ------------------------------------------------------------------------ */

@@ -47,6 +47,12 @@ void rs_denormalize(const rs_float *work, uint64_t n, rs_float pmin, rs_float pm
  * decomp[a] levels along axis a (dwt.c:1216-1724, :1738-2246) */
 void rs_dwt_forward(rs_float *work, const uint64_t dims[4], const uint8_t decomp[4]);
 void rs_dwt_inverse(rs_float *work, const uint64_t dims[4], const uint8_t decomp[4]);
+/* the same with a wavelet kernel per axis: 0 CDF 9/7, 1 LeGall 5/3 (dwt.c:478-558; the Haar
+ * kernel is not restated: the reference has no boundary extension for it, dwt.c:1259-1262) */
+void rs_dwt_forward_kernels(rs_float *work, const uint64_t dims[4], const uint8_t decomp[4],
+                            const uint8_t kernels[4]);
+void rs_dwt_inverse_kernels(rs_float *work, const uint64_t dims[4], const uint8_t decomp[4],
+                            const uint8_t kernels[4]);
 
 /* one codeblock: box in working-buffer coordinates and its subband's coding parameters */
 typedef struct {

@@ -46,6 +46,8 @@ def load(precision="double"):
     L.rs_denormalize.argtypes = [vp, u64, fl, fl, C.c_uint8, vp, C.c_int]
     L.rs_dwt_forward.argtypes = [vp, vp, vp]
     L.rs_dwt_inverse.argtypes = [vp, vp, vp]
+    L.rs_dwt_forward_kernels.argtypes = [vp, vp, vp, vp]
+    L.rs_dwt_inverse_kernels.argtypes = [vp, vp, vp, vp]
     L.rs_context_class.restype = C.c_int
     L.rs_context_class.argtypes = [C.c_uint32]
     L.rs_t1_encode.restype = C.c_int64
@@ -84,17 +86,28 @@ def denormalize(work, pmin, pmax, qm, out_dtype, precision="double"):
     return out
 
 
-def dwt_forward(work, dims, decomp, precision="double"):
+def dwt_forward(work, dims, decomp, precision="double", kernels=None):
+    """kernels: per axis (x, y, z, t), 0 CDF 9/7 (default), 1 LeGall 5/3"""
     dec = np.array(decomp, dtype=np.uint8)
-    load(precision).rs_dwt_forward(work.ctypes.data, np.asarray(dims, np.uint64).ctypes.data,
-                                   dec.ctypes.data)
+    d = np.asarray(dims, np.uint64)
+    if kernels is None:
+        load(precision).rs_dwt_forward(work.ctypes.data, d.ctypes.data, dec.ctypes.data)
+    else:
+        k = np.array(kernels, dtype=np.uint8)
+        load(precision).rs_dwt_forward_kernels(work.ctypes.data, d.ctypes.data, dec.ctypes.data,
+                                               k.ctypes.data)
     return work
 
 
-def dwt_inverse(work, dims, decomp, precision="double"):
+def dwt_inverse(work, dims, decomp, precision="double", kernels=None):
     dec = np.array(decomp, dtype=np.uint8)
-    load(precision).rs_dwt_inverse(work.ctypes.data, np.asarray(dims, np.uint64).ctypes.data,
-                                   dec.ctypes.data)
+    d = np.asarray(dims, np.uint64)
+    if kernels is None:
+        load(precision).rs_dwt_inverse(work.ctypes.data, d.ctypes.data, dec.ctypes.data)
+    else:
+        k = np.array(kernels, dtype=np.uint8)
+        load(precision).rs_dwt_inverse_kernels(work.ctypes.data, d.ctypes.data, dec.ctypes.data,
+                                               k.ctypes.data)
     return work
 
 
