@@ -406,12 +406,21 @@ static int t1_grid(const void *kernel_unused, size_t smem_per_block) {
 }
 
 // ---------------------------------------------------------------------------------------------
+static const char *kSingleTileError =
+    "o##########################################################o\n"
+    "| ERROR: this library compresses single-tile fields only   |\n"
+    "o##########################################################o\n";
+
 static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
   bwc_b200_engine *eng = codec->tile;
   if (!eng || eng->tiles.empty()) {
     warn("o##########################################################o\n"
          "| ERROR: bwc_create_compression has not been called        |\n"
          "o##########################################################o\n");
+    return 0;
+  }
+  if (eng->tiles.size() != 1) {
+    warn(kSingleTileError);
     return 0;
   }
   DeviceState *dv = device_state(codec);
@@ -921,6 +930,10 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
       warn("o##########################################################o\n"
            "| ERROR: bwc_create_compression has not been called        |\n"
            "o##########################################################o\n");
+      return 1;
+    }
+    if (codecs[i]->tile->tiles.size() != 1) {
+      warn(kSingleTileError);
       return 1;
     }
   }

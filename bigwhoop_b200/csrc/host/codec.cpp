@@ -867,12 +867,9 @@ static uchar bwc_create_compression_body(bwc_codec *const codec, bwc_stream *con
     }
   }
   c->bitrate = (float *)realloc(c->bitrate, c->nLayers * sizeof(float));
-  if (c->nTiles != 1) {
-    warn("o##########################################################o\n"
-         "| ERROR: this library codes single-tile codestreams only   |\n"
-         "o##########################################################o\n");
-    return 1;
-  }
+  // more than one tile: the geometry, rate control and codestream layout are built (and tested
+  // against the reference through bwc_b200_assemble_tiles_from_tier1); bwc_compress and
+  // bwc_b200_compress_batch refuse such codecs, the device path codes a single tile
   if (c->KernelX != bwc_dwt_9_7 || c->KernelY != bwc_dwt_9_7 || c->KernelZ != bwc_dwt_9_7 ||
       (c->KernelTS != bwc_dwt_9_7 && c->decompTS > 0 && info->nTS > 1)) {
     warn("o##########################################################o\n"

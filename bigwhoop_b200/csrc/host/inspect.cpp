@@ -95,6 +95,57 @@ static size_t bwc_b200_assemble_from_tier1_body(bwc_codec *const codec, bwc_stre
   return total;
 }
 
+static size_t assemble_tiles_body(bwc_codec *const codec, bwc_stream *const stream,
+                                  uint8 const *K, uint8 const *Z, uint64 const *L,
+                                  uint16 const *S, uint8 const *bytes,
+                                  uint64 const *byte_offsets, bwc_float const *minmax,
+                                  uint16 const *slopes) {
+  if (!codec || !codec->tile || codec->tile->tiles.empty()) return 0;
+  uint64_t g = 0, tp = 0, t = 0;
+  for (Tile &tile : codec->tile->tiles) {
+    for (size_t p = 0; p < tile.params.size(); ++p, ++tp) {
+      Parameter &par = tile.params[p];
+      par.pmin = minmax[2 * tp];
+      par.pmax = minmax[2 * tp + 1];
+      for (Codeblock &cb : par.codeblocks) {
+        CodedBlock &e = cb.enc;
+        e.K = K[g];
+        e.Z = Z[g];
+        e.Kmsbs = e.K ? (uint8_t)(par.subbands[cb.subband].Kmax - e.K) : 0;
+        for (int j = 0; j < e.Z; ++j) e.L[j] = (uint32_t)L[g * kMaxPasses + j];
+        for (int j = 0; j <= e.Z; ++j) e.S[j] = S[g * (kMaxPasses + 1) + j];
+        cb.data_off = byte_offsets[g];
+        ++g;
+      }
+    }
+    tile.slope_min = slopes[2 * t];
+    tile.slope_max = slopes[2 * t + 1];
+    ++t;
+  }
+  for (Tile &tile : codec->tile->tiles)
+    if (t2_encode(codec, tile)) return 0;
+  std::vector<uint8_t> blob;
+  std::vector<GatherPiece> pieces;
+  const uint64_t total = layout_codestream(codec, stream, blob, pieces);
+  if (!total) return 0;
+  uint8_t *out = (uint8_t *)stream->out;
+  for (const GatherPiece &pc : pieces)
+    std::memcpy(out + pc.dst, (pc.from_blob ? blob.data() : bytes) + pc.src, pc.size);
+  return total;
+}
+
+extern "C" size_t bwc_b200_assemble_tiles_from_tier1(bwc_codec *const codec,
+                                                     bwc_stream *const stream, uint8 const *K,
+                                                     uint8 const *Z, uint64 const *L,
+                                                     uint16 const *S, uint8 const *bytes,
+                                                     uint64 const *byte_offsets,
+                                                     bwc_float const *minmax,
+                                                     uint16 const *slopes) {
+  return guarded<size_t>(0, [&] {
+    return assemble_tiles_body(codec, stream, K, Z, L, S, bytes, byte_offsets, minmax, slopes);
+  });
+}
+
 extern "C" int bwc_b200_rate_features(bwc_codec *const codec, uint8 const layer, float *out) {
   if (!codec || !codec->tile || codec->tile->tiles.empty() || !out) return 1;
   const Tile &tile = codec->tile->tiles[0];

@@ -89,6 +89,16 @@ size_t bwc_b200_assemble_from_tier1(bwc_codec *const codec, bwc_stream *const st
                                     uint16 const *S, uint8 const *bytes,
                                     uint64 const *byte_offsets, bwc_float const *minmax,
                                     uint16 const slope_min, uint16 const slope_max);
+/* The same for a codec of one or more tiles (bwc_set_tiles): codeblocks of every tile in tile
+ * order, within a tile parameter by parameter; minmax = min, max per tile and parameter;
+ * slopes = slope minimum, maximum per tile.  bwc_compress codes single-tile fields only; this
+ * runs the host half of multi-tile coding (per-tile rate control, packets, the multi-tile
+ * codestream).  No counterpart in the reference. */
+size_t bwc_b200_assemble_tiles_from_tier1(bwc_codec *const codec, bwc_stream *const stream,
+                                          uint8 const *K, uint8 const *Z, uint64 const *L,
+                                          uint16 const *S, uint8 const *bytes,
+                                          uint64 const *byte_offsets, bwc_float const *minmax,
+                                          uint16 const *slopes);
 
 /* Device time of the stages of the last bwc_compress / bwc_decompress on this codec, in
  * milliseconds (CUDA events on the codec's stream): [0] upload, [1] fill+normalise, [2] wavelet,

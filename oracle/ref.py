@@ -43,6 +43,11 @@ def load(precision="double"):
     L.rp_compress_full.argtypes = [vp]
     L.rp_set_precincts.argtypes = [u8p]
     L.rp_set_kernels.argtypes = [u8p]
+    L.rp_set_tiles.argtypes = [C.POINTER(C.c_uint64)]
+    L.rp_select_tile.restype = C.c_int
+    L.rp_select_tile.argtypes = [vp, C.c_int]
+    L.rp_num_tiles.restype = u64
+    L.rp_num_tiles.argtypes = [vp]
     for n in ("rp_stage_normalize", "rp_stage_dwt", "rp_stage_t1", "rp_dstage_t1",
               "rp_dstage_idwt", "rp_dstage_finish"):
         getattr(L, n).restype = C.c_int
@@ -100,7 +105,7 @@ class RefCompressor:
     """One reference compression, optionally run stage by stage."""
 
     def __init__(self, field, *, precision="double", decomp=None, cb=None, qm=-1, erres=False,
-                 rate="2", n_par=None, precincts=None, kernels=None):
+                 rate="2", n_par=None, precincts=None, kernels=None, tiles=None):
         self.L = load(precision)
         self.precision = precision
         f = np.ascontiguousarray(field)
@@ -121,11 +126,15 @@ class RefCompressor:
         rate_b = None if rate is None else rate.encode()
         self.L.rp_set_precincts(_u8arr(precincts))
         self.L.rp_set_kernels(_u8arr(kernels))   # (x, y, z, t): 0 CDF 9/7, 1 LeGall 5/3
+        # tile sizes (x, y, z, t)
+        tl = None if tiles is None else (C.c_uint64 * 4)(*[int(v) for v in tiles])
+        self.L.rp_set_tiles(tl)
         try:
             self.h = self._open(f, dims, n_par, decomp, cb, qm, erres, rate_b)
         finally:
             self.L.rp_set_precincts(None)
             self.L.rp_set_kernels(None)
+            self.L.rp_set_tiles(None)
         if not self.h:
             raise RuntimeError("reference rejected the configuration")
 
@@ -197,6 +206,13 @@ class RefCompressor:
         nbytes = int(Ls[Z - 1]) if Z > 0 else 0
         return Codeblock(geom, K, Kmsbs, Z, Ls[:Z].copy(), Ss[:Z + 1].copy(),
                          bytes(data[:nbytes]) if with_data else b"", sb)
+
+    def num_tiles(self):
+        return int(self.L.rp_num_tiles(self.h))
+
+    def select_tile(self, t):
+        """stage functions and per-codeblock queries work on tile t from here on"""
+        assert self.L.rp_select_tile(self.h, t) == 0
 
     def tile_slopes(self):
         out = np.zeros(2, dtype=np.uint16)

@@ -36,6 +36,7 @@ typedef struct
    bwc_sample *work;       /* working buffer of one tile/parameter */
    uint64      work_len;
    char       *rate;       /* private copy: the reference tokenises it in place */
+   int         tile;       /* the tile the stage functions work on (rp_select_tile) */
 } rp_handle;
 
 /* ---- configuration ------------------------------------------------------------------- */
@@ -95,6 +96,26 @@ void rp_set_kernels(const uint8 *k)
    else  rp_kern_set = 0;
 }
 
+/* tile sizes per axis (bwc_set_tiles, bwc_tile_sizeof) applied by the next rp_open_compress
+ * calls; NULL: one tile */
+static uint64 rp_tiles[4];
+static int    rp_tiles_set = 0;
+void rp_set_tiles(const uint64 *t)
+{
+   if(t) { memcpy(rp_tiles, t, sizeof(rp_tiles)); rp_tiles_set = 1; }
+   else  rp_tiles_set = 0;
+}
+
+/* stage functions below work on tile t (0 until selected) */
+int rp_select_tile(rp_handle *h, int t)
+{
+   if(t < 0 || (uint64)t >= h->codec->control.nTiles) return 1;
+   h->tile = t;
+   return 0;
+}
+
+uint64 rp_num_tiles(rp_handle *h) { return h->codec->control.nTiles; }
+
 rp_handle *rp_open_compress(void *field, uint64 nX, uint64 nY, uint64 nZ, uint64 nTS,
                             uint8 nPar, int data_prec, const uint8 *decomp, const uint8 *cb,
                             int qm, int erres, const char *rate, void *out)
@@ -107,6 +128,8 @@ rp_handle *rp_open_compress(void *field, uint64 nX, uint64 nY, uint64 nZ, uint64
    if(decomp) bwc_set_decomp(h->codec, decomp[0], decomp[1], decomp[2], decomp[3]);
    if(cb)     bwc_set_codeblocks(h->codec, cb[0], cb[1], cb[2], cb[3]);
    if(rp_prec_set) bwc_set_precincts(h->codec, rp_prec[0], rp_prec[1], rp_prec[2], rp_prec[3]);
+   if(rp_tiles_set) bwc_set_tiles(h->codec, rp_tiles[0], rp_tiles[1], rp_tiles[2], rp_tiles[3],
+                                  bwc_tile_sizeof);
    if(rp_kern_set) set_kernels(h->codec, (bwc_dwt_filter)rp_kern[0], (bwc_dwt_filter)rp_kern[1],
                                (bwc_dwt_filter)rp_kern[2], (bwc_dwt_filter)rp_kern[3]);
    if(qm >= 0) bwc_set_qm(h->codec, (uint8)qm);
@@ -130,11 +153,11 @@ size_t rp_compress_full(rp_handle *h)
    return bwc_compress(h->codec, h->stream);
 }
 
-/* restatement of fill_buffer (libbwc.c:622-812) for tile 0 */
+/* restatement of fill_buffer (libbwc.c:622-812) for the selected tile */
 static void rp_fill(rp_handle *h, bwc_parameter *parameter, uint16 param_id)
 {
    bwc_gl_inf    *info = &h->codec->info;
-   bwc_tile_inf  *tile_info = &h->codec->tile[0].info;
+   bwc_tile_inf  *tile_info = &h->codec->tile[h->tile].info;
    bwc_param_inf *pi = &parameter->info;
    uint64 width  = pi->X1 - pi->X0, height = pi->Y1 - pi->Y0;
    uint64 depth  = pi->Z1 - pi->Z0, dt     = pi->TS1 - pi->TS0;
@@ -192,10 +215,10 @@ static int rp_ensure_work(rp_handle *h)
    return h->work ? 0 : 1;
 }
 
-/* fill + normalise parameter p of tile 0 into the working buffer */
+/* fill + normalise parameter p of the selected tile into the working buffer */
 int rp_stage_normalize(rp_handle *h, int p)
 {
-   bwc_parameter *parameter = &h->codec->tile[0].parameter[p];
+   bwc_parameter *parameter = &h->codec->tile[h->tile].parameter[p];
    if(rp_ensure_work(h)) return 1;
    memset(h->work, 0, h->work_len * sizeof(bwc_sample));
    rp_fill(h, parameter, (uint16)p);
@@ -205,17 +228,17 @@ int rp_stage_normalize(rp_handle *h, int p)
 
 int rp_stage_dwt(rp_handle *h, int p)
 {
-   return forward_wavelet_transform(h->codec, &h->codec->tile[0].parameter[p]);
+   return forward_wavelet_transform(h->codec, &h->codec->tile[h->tile].parameter[p]);
 }
 
 int rp_stage_t1(rp_handle *h, int p)
 {
-   return t1_encode(h->codec, &h->codec->tile[0], &h->codec->tile[0].parameter[p]);
+   return t1_encode(h->codec, &h->codec->tile[h->tile], &h->codec->tile[h->tile].parameter[p]);
 }
 
 int rp_stage_t2(rp_handle *h)
 {
-   return t2_encode(h->codec, &h->codec->tile[0]);
+   return t2_encode(h->codec, &h->codec->tile[h->tile]);
 }
 
 size_t rp_stage_assemble(rp_handle *h)
@@ -233,7 +256,7 @@ uint64 rp_copy_work(rp_handle *h, void *dst)
 /* parameter statistics after fill: min, max, alpha, beta (as double) */
 void rp_param_stats(rp_handle *h, int p, double *out4)
 {
-   bwc_parameter *parameter = &h->codec->tile[0].parameter[p];
+   bwc_parameter *parameter = &h->codec->tile[h->tile].parameter[p];
    out4[0] = parameter->info.parameter_min;
    out4[1] = parameter->info.parameter_max;
    out4[2] = parameter->control.alpha;
@@ -242,7 +265,7 @@ void rp_param_stats(rp_handle *h, int p, double *out4)
 
 uint64 rp_num_codeblocks(rp_handle *h, int p)
 {
-   return h->codec->tile[0].parameter[p].control.number_of_codeblocks;
+   return h->codec->tile[h->tile].parameter[p].control.number_of_codeblocks;
 }
 
 /* Codeblock c (tier-1 order) of parameter p:
@@ -252,7 +275,7 @@ uint64 rp_num_codeblocks(rp_handle *h, int p)
 int rp_codeblock(rp_handle *h, int p, uint64 c, uint64 *geom, int64 *meta, uint64 *L,
                  uint16 *S, uint8 *data, uint64 cap)
 {
-   bwc_parameter *parameter = &h->codec->tile[0].parameter[p];
+   bwc_parameter *parameter = &h->codec->tile[h->tile].parameter[p];
    bwc_cblk_access *a;
    bwc_encoded_cblk *e;
    uint64 n;
@@ -286,7 +309,7 @@ int rp_codeblock(rp_handle *h, int p, uint64 c, uint64 *geom, int64 *meta, uint6
  * dwt_gain (as double) */
 void rp_codeblock_subband(rp_handle *h, int p, uint64 c, double *out3)
 {
-   bwc_cblk_access *a = &h->codec->tile[0].parameter[p].access[c];
+   bwc_cblk_access *a = &h->codec->tile[h->tile].parameter[p].access[c];
    out3[0] = a->subband->control.qt_effective_step_size;
    out3[1] = a->subband->control.qt_step_size;
    out3[2] = a->subband->info.dwt_gain;
@@ -294,8 +317,8 @@ void rp_codeblock_subband(rp_handle *h, int p, uint64 c, double *out3)
 
 void rp_tile_slopes(rp_handle *h, uint16 *out2)
 {
-   out2[0] = h->codec->tile[0].control.slope_min;
-   out2[1] = h->codec->tile[0].control.slope_max;
+   out2[0] = h->codec->tile[h->tile].control.slope_min;
+   out2[1] = h->codec->tile[h->tile].control.slope_max;
 }
 
 /* copy of the public part of the codec: info and control (bitrate pointer excluded) */
@@ -351,23 +374,23 @@ int rp_decompress_full(rp_handle *h)
 
 int rp_dstage_t1(rp_handle *h, int p)
 {
-   bwc_parameter *parameter = &h->codec->tile[0].parameter[p];
+   bwc_parameter *parameter = &h->codec->tile[h->tile].parameter[p];
    if(rp_ensure_work(h)) return 1;
    memset(h->work, 0, h->work_len * sizeof(bwc_sample));
    parameter->data = h->work;
-   return t1_decode(h->codec, &h->codec->tile[0], parameter);
+   return t1_decode(h->codec, &h->codec->tile[h->tile], parameter);
 }
 
 int rp_dstage_idwt(rp_handle *h, int p)
 {
-   return inverse_wavelet_transform(h->codec, &h->codec->tile[0].parameter[p]);
+   return inverse_wavelet_transform(h->codec, &h->codec->tile[h->tile].parameter[p]);
 }
 
 /* restatement of denormalize_param (libbwc.c:1093-1176) and flush_buffer (:827-978) */
 int rp_dstage_finish(rp_handle *h, int p)
 {
    bwc_gl_inf    *info = &h->codec->info;
-   bwc_parameter *parameter = &h->codec->tile[0].parameter[p];
+   bwc_parameter *parameter = &h->codec->tile[h->tile].parameter[p];
    bwc_param_inf *pi = &parameter->info;
    uint64 width  = pi->X1 - pi->X0, height = pi->Y1 - pi->Y0;
    uint64 depth  = pi->Z1 - pi->Z0, dt     = pi->TS1 - pi->TS0;
@@ -402,7 +425,7 @@ int rp_dstage_finish(rp_handle *h, int p)
 /* decoder-side codeblock state after parsing: meta[0] = K (Kmax - Kmsbs), [1] = Kmsbs, [2] = Z */
 int rp_dcodeblock(rp_handle *h, int p, uint64 c, int64 *meta, uint64 *L)
 {
-   bwc_parameter *parameter = &h->codec->tile[0].parameter[p];
+   bwc_parameter *parameter = &h->codec->tile[h->tile].parameter[p];
    bwc_cblk_access *a;
    bwc_encoded_cblk *e;
    if(c >= parameter->control.number_of_codeblocks) return 1;

@@ -221,11 +221,11 @@ def test_create_decompression_rejects_truncated_codestream():
             C.CDLL(None).free(C.c_void_p(s))
 
 
-@pytest.mark.parametrize("case", ["two_tiles", "kernel_5_3", "kernel_haar", "no_quantisation"])
+@pytest.mark.parametrize("case", ["kernel_5_3", "kernel_haar", "no_quantisation"])
 def test_create_compression_rejects_configurations_off_the_accelerated_path(case):
-    """Multi-tile codestreams, the 5/3 and Haar kernels and bwc_qt_none are not on the
-    accelerated path: bwc_create_compression refuses them with return code 1 (the default
-    configuration of the same field is accepted)."""
+    """The 5/3 and Haar kernels and bwc_qt_none are not on the accelerated path:
+    bwc_create_compression refuses them with return code 1 (the default configuration of the
+    same field is accepted)."""
     f = np.zeros((16, 16, 16))
     out = np.zeros(1 << 16, np.uint8)
     L = C.CDLL(bwc.lib_path("double"))
@@ -244,9 +244,7 @@ def test_create_compression_rejects_configurations_off_the_accelerated_path(case
         s = L.bwc_init_stream(f.ctypes.data, out.ctypes.data, bwc.COMP)
         try:
             if configure:
-                if case == "two_tiles":
-                    L.bwc_set_tiles(c, 8, 16, 16, 1, 0)   # bwc_tile_sizeof: 8 x 16 x 16 tiles
-                elif case == "kernel_5_3":
+                if case == "kernel_5_3":
                     L.set_kernels(c, 1, 1, 1, 1)
                 elif case == "kernel_haar":
                     L.set_kernels(c, 2, 2, 2, 2)
@@ -304,3 +302,33 @@ def test_create_decompression_rejects_codestreams_off_the_accelerated_path(case)
         L.bwc_free_codec(d)
         C.CDLL(None).free(C.c_void_p(st))
     assert rc == (0 if case == "default" else 1), case
+
+
+def test_compress_refuses_multi_tile_fields(capfd):
+    """A codec of two tiles is set up (its host half is tested against the reference in
+    tests/test_host_parity.py), but bwc_compress, which codes single-tile fields on the device,
+    refuses it with return value 0 and a message, before touching the GPU."""
+    f = np.zeros((16, 16, 16))
+    out = np.zeros(1 << 16, np.uint8)
+    L = C.CDLL(bwc.lib_path("double"))
+    L.bwc_alloc_coder.restype = C.c_void_p
+    L.bwc_alloc_coder.argtypes = [C.c_uint64] * 4 + [C.c_uint8, C.c_int]
+    L.bwc_init_stream.restype = C.c_void_p
+    L.bwc_init_stream.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+    L.bwc_create_compression.restype = C.c_uint8
+    L.bwc_create_compression.argtypes = [C.c_void_p, C.c_void_p, C.c_char_p]
+    L.bwc_compress.restype = C.c_size_t
+    L.bwc_compress.argtypes = [C.c_void_p, C.c_void_p]
+    L.bwc_free_codec.argtypes = [C.c_void_p]
+    L.bwc_set_tiles.argtypes = [C.c_void_p] + [C.c_uint64] * 4 + [C.c_int]
+    c = L.bwc_alloc_coder(16, 16, 16, 1, 1, 8)
+    s = L.bwc_init_stream(f.ctypes.data, out.ctypes.data, bwc.COMP)
+    try:
+        L.bwc_set_tiles(c, 8, 16, 16, 1, 0)   # bwc_tile_sizeof: two 8 x 16 x 16 tiles
+        assert L.bwc_create_compression(c, s, C.create_string_buffer(b"2")) == 0
+        capfd.readouterr()
+        assert L.bwc_compress(c, s) == 0
+        assert "single-tile" in capfd.readouterr().err
+    finally:
+        L.bwc_free_codec(c)
+        C.CDLL(None).free(C.c_void_p(s))

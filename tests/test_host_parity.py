@@ -5,6 +5,8 @@ The reference's own tier-1 output (codeblock lengths, slopes, coded bytes) is fe
 library's tier-2 through bwc_b200_assemble_from_tier1; the codestream must be byte-identical to
 the one the reference assembles from the same data.
 """
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -206,3 +208,66 @@ def test_rate_control_in_small_pieces():
                        text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     assert "mismatch" not in r.stderr
+
+
+TILE_CASES = [
+    # shape, decomp, codeblocks, tile sizes (x, y, z, t), rate
+    ((32, 32, 32), (2, 2, 2, 0), (3, 3, 3, 0), (16, 16, 16, 1), "1,4"),
+    ((33, 47, 61), (2, 2, 2, 0), (4, 4, 4, 0), (32, 24, 20, 1), "2"),
+    ((8, 20, 24, 30), (2, 2, 2, 1), (3, 3, 3, 1), (16, 12, 10, 4), "0.5,4"),
+]
+
+
+@pytest.mark.parametrize("shape,decomp,cb,tiles,rate", TILE_CASES)
+def test_tier2_codestream_identical_with_tiles(shape, decomp, cb, tiles, rate):
+    """Multi-tile fields: the reference's tier-1 results of every tile, fed to this library's
+    host half (per-tile rate control, packets, the multi-tile codestream layout), give the
+    reference's codestream byte for byte.  (bwc_compress itself codes single-tile fields.)"""
+    ref = need_ref("double")
+    f = _field(shape, np.float64)
+    ref.reset_gain_lut("double")
+    bwc.reset_gain_state("double")
+    rc = ref.RefCompressor(f, decomp=decomp, cb=cb, rate=rate, tiles=tiles)
+    mc = bwc.Compressor(f, decomp=decomp, codeblocks=cb, rate=rate, tiles=tiles)
+    try:
+        nt = rc.num_tiles()
+        assert nt > 1
+        MP = ref.MAX_PASSES["double"]
+        K, Z, Ls, Ss, offs, mm, slopes = [], [], [], [], [], [], []
+        data = bytearray()
+        for t in range(nt):
+            rc.select_tile(t)
+            rc.normalize(); rc.dwt(); rc.t1()
+            for c in range(rc.num_codeblocks()):
+                cbk = rc.codeblock(c)
+                K.append(cbk.K); Z.append(cbk.Z)
+                l = np.zeros(MP, np.uint64); l[:cbk.Z] = cbk.L
+                s = np.zeros(MP + 1, np.uint16); s[:cbk.Z + 1] = cbk.S
+                Ls.append(l); Ss.append(s)
+                offs.append(len(data))
+                data += cbk.data
+            mm += list(rc.stats()[:2])
+            slopes += list(rc.tile_slopes())
+            rc.t2()
+        cs_ref = rc.assemble()
+        K = np.array(K, np.uint8); Z = np.array(Z, np.uint8)
+        Ls = np.concatenate(Ls); Ss = np.concatenate(Ss)
+        offs = np.array(offs, np.uint64); mm = np.array(mm, np.float64)
+        slopes = np.array(slopes, np.uint16)
+        buf = np.frombuffer(bytes(data) + b"\0" * 64, np.uint8).copy()
+        out = np.zeros(len(cs_ref) + 4096, np.uint8)
+        L = mc.L
+        L.bwc_b200_assemble_tiles_from_tier1.restype = C.c_size_t
+        L.bwc_b200_assemble_tiles_from_tier1.argtypes = [C.c_void_p] * 10
+        stream = L.bwc_init_stream(f.ctypes.data, out.ctypes.data, 0)
+        try:
+            n = L.bwc_b200_assemble_tiles_from_tier1(
+                mc.codec, stream, K.ctypes.data, Z.ctypes.data, Ls.ctypes.data, Ss.ctypes.data,
+                buf.ctypes.data, offs.ctypes.data, mm.ctypes.data, slopes.ctypes.data)
+        finally:
+            C.CDLL(None).free(C.c_void_p(stream))
+        assert n > 0
+        assert bytes(out[:n]) == cs_ref
+    finally:
+        rc.close()
+        mc.close()
