@@ -708,6 +708,12 @@ static uchar decompress_impl(bwc_codec *codec, bwc_stream *stream) {
     warn(kCsError);
     return 1;
   }
+  if (eng->tiles.size() != 1) {
+    warn("o##########################################################o\n"
+         "| ERROR: this library decodes single-tile codestreams only |\n"
+         "o##########################################################o\n");
+    return 1;
+  }
   DeviceState *dv = device_state(codec);
   if (!dv) return 1;
   cudaStream_t s = dv->stream;

@@ -664,7 +664,8 @@ uchar build_geometry(bwc_codec *codec) {
   // built: building it codeblock by codeblock would run for hours, or exhaust host memory
   // (about 2 KB a codeblock).  The bound, 2^21 codeblocks at the field's codeblock size, is
   // over ten times the codeblocks of the largest field whose compression fits a B200's memory
-  // (about 77 bytes of device memory a value, 32 x 32 x 16 codeblocks).
+  // (about 77 bytes of device memory a value, 32 x 32 x 16 codeblocks); likewise more than
+  // 65536 tiles.
   {
     const uint64_t n[4] = {info.nX, info.nY, info.nZ, info.nTS};
     const uint64_t tsz[4] = {c.tileSizeX, c.tileSizeY, c.tileSizeZ, c.tileSizeTS};
@@ -675,7 +676,7 @@ uchar build_geometry(bwc_codec *codec) {
       empty = empty || n[a] == 0 || tsz[a] == 0;
       cells *= std::ceil((double)n[a] / std::ldexp(1.0, cb[a] < 63 ? cb[a] : 63));
     }
-    if (empty || cells > (double)(1ull << 21)) {
+    if (empty || cells > (double)(1ull << 21) || c.nTiles > (1u << 16)) {
       warn(kMemError);
       return 1;
     }

@@ -289,12 +289,8 @@ uchar parse_main_header(bwc_codec *codec, bwc_stream *data, BitReader &br) {
           const uint32_t bits = (uint32_t)br.get_symbol(4);
           std::memcpy(&c.bitrate[l], &bits, 4);
         }
-        if (c.nTiles != 1) {
-          warn("o##########################################################o\n"
-               "| ERROR: this library decodes single-tile codestreams only |\n"
-               "o##########################################################o\n");
-          return 1;
-        }
+        // more than one tile: parsed here (tested against the reference's parser);
+        // bwc_decompress refuses such codecs, the device path decodes a single tile
         if (c.KernelX != bwc_dwt_9_7 || c.KernelY != bwc_dwt_9_7 || c.KernelZ != bwc_dwt_9_7 ||
             (c.KernelTS != bwc_dwt_9_7 && c.decompTS > 0 && info.nTS > 1)) {
           warn("o##########################################################o\n"

@@ -39,6 +39,22 @@ extern "C" int bwc_b200_subband_steps(bwc_codec *const codec, uint8 const param,
   return 0;
 }
 
+extern "C" int bwc_b200_parsed_codeblock_of_tile(bwc_codec *const codec, uint32 const tile,
+                                                 uint8 const param, uint64 const c,
+                                                 int64 *meta3, uint64 *L) {
+  if (!codec || !codec->tile || tile >= codec->tile->tiles.size()) return 1;
+  Tile &t = codec->tile->tiles[tile];
+  if (param >= t.params.size() || c >= t.params[param].codeblocks.size()) return 1;
+  const Parameter &par = t.params[param];
+  const Codeblock &cb = par.codeblocks[c];
+  meta3[0] = par.subbands[cb.subband].Kmax - cb.enc.Kmsbs;
+  meta3[1] = cb.enc.Kmsbs;
+  meta3[2] = cb.enc.Z;
+  if (L)
+    for (int j = 0; j < kMaxPasses; ++j) L[j] = cb.enc.L[j];
+  return 0;
+}
+
 extern "C" int bwc_b200_parsed_codeblock(bwc_codec *const codec, uint8 const param,
                                          uint64 const c, int64 *meta3, uint64 *L) {
   Parameter *par = param_of(codec, param);

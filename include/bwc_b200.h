@@ -84,6 +84,12 @@ int    bwc_b200_subband_steps(bwc_codec *const codec, uint8 const param, uint64 
                               double *out3);
 int    bwc_b200_parsed_codeblock(bwc_codec *const codec, uint8 const param, uint64 const c,
                                  int64 *meta3, uint64 *L);
+/* the same for codeblock c of parameter `param` in tile `tile` of a multi-tile codestream
+ * (bwc_create_decompression parses those; bwc_decompress decodes single-tile ones only).  No
+ * counterpart in the reference. */
+int    bwc_b200_parsed_codeblock_of_tile(bwc_codec *const codec, uint32 const tile,
+                                         uint8 const param, uint64 const c, int64 *meta3,
+                                         uint64 *L);
 size_t bwc_b200_assemble_from_tier1(bwc_codec *const codec, bwc_stream *const stream,
                                     uint8 const *K, uint8 const *Z, uint64 const *L,
                                     uint16 const *S, uint8 const *bytes,

@@ -267,6 +267,23 @@ class RefDecompressor:
         self.L.rp_copy_work(self.h, buf.ctypes.data)
         return buf
 
+    def num_tiles(self):
+        return int(self.L.rp_num_tiles(self.h))
+
+    def select_tile(self, t):
+        """codeblock queries and stages work on tile t from here on"""
+        assert self.L.rp_select_tile(self.h, t) == 0
+
+    def num_codeblocks(self, p=0):
+        return int(self.L.rp_num_codeblocks(self.h, p))
+
+    def codeblock_lengths(self, c, p=0):
+        """(K, Kmsbs, Z) and the truncation lengths of codeblock c as parsed"""
+        meta = np.zeros(3, dtype=np.int64)
+        Ls = np.zeros(MAX_PASSES[self.precision], dtype=np.uint64)
+        assert self.L.rp_dcodeblock(self.h, p, c, meta.ctypes.data, Ls.ctypes.data) == 0
+        return tuple(int(v) for v in meta), Ls
+
     def codeblock(self, c, p=0):
         """(K, Kmsbs, Z) of codeblock c as parsed from the codestream."""
         meta = np.zeros(3, dtype=np.int64)

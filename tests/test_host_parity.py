@@ -271,3 +271,51 @@ def test_tier2_codestream_identical_with_tiles(shape, decomp, cb, tiles, rate):
     finally:
         rc.close()
         mc.close()
+
+
+@pytest.mark.parametrize("shape,decomp,cb,tiles,rate", TILE_CASES)
+def test_parse_identical_with_tiles(shape, decomp, cb, tiles, rate):
+    """A multi-tile reference codestream parses to the reference parser's codeblocks, tile by
+    tile (missing bit planes, passes, truncation lengths); bwc_decompress itself then refuses
+    the codec (single-tile decoding on the device)."""
+    ref = need_ref("double")
+    f = _field(shape, np.float64)
+    ref.reset_gain_lut("double")
+    rc = ref.RefCompressor(f, decomp=decomp, cb=cb, rate=rate, tiles=tiles)
+    try:
+        cs = rc.compress()
+    finally:
+        rc.close()
+    rd = ref.RefDecompressor(cs, f.shape, f.dtype)
+    L = bwc.load("double")
+    L.bwc_b200_parsed_codeblock_of_tile.restype = C.c_int
+    L.bwc_b200_parsed_codeblock_of_tile.argtypes = [C.c_void_p, C.c_uint32, C.c_uint8,
+                                                    C.c_uint64, C.c_void_p, C.c_void_p]
+    buf = np.frombuffer(cs + b"\0" * 64, np.uint8).copy()
+    out = np.zeros(f.size, np.float64)
+    d = L.bwc_alloc_decoder()
+    st = L.bwc_init_stream(buf.ctypes.data, out.ctypes.data, bwc.DECOMP)
+    try:
+        assert L.bwc_create_decompression(d, st, 0) == 0
+        nt = rd.num_tiles()
+        assert nt > 1
+        meta = np.zeros(3, np.int64)
+        Lz = np.zeros(ref.MAX_PASSES["double"], np.uint64)
+        total = 0
+        for t in range(nt):
+            rd.select_tile(t)
+            for c in range(rd.num_codeblocks()):
+                (K, Kmsbs, Z), Lr = rd.codeblock_lengths(c)
+                assert L.bwc_b200_parsed_codeblock_of_tile(d, t, 0, c, meta.ctypes.data,
+                                                           Lz.ctypes.data) == 0
+                assert tuple(int(v) for v in meta) == (K, Kmsbs, Z), (t, c)
+                assert np.array_equal(Lz[:Z], Lr[:Z]), (t, c)
+                total += 1
+            assert L.bwc_b200_parsed_codeblock_of_tile(d, t, 0, rd.num_codeblocks(),
+                                                       meta.ctypes.data, None) == 1
+        assert total > 0
+        assert L.bwc_decompress(d, st) == 1
+    finally:
+        rd.close()
+        L.bwc_free_codec(d)
+        C.CDLL(None).free(C.c_void_p(st))
