@@ -229,6 +229,60 @@ void rs_dwt_inverse(rs_float *work, const uint64_t dims[4], const uint8_t decomp
   dwt(work, dims, decomp, 0, CDF97);
 }
 
+/* Forward transform of one tile's working buffer (dims: the tile's extent; origin: its first
+ * sample in field coordinates), dwt.c:1216-1724 with libbwc.c:1539-1548's resolution bounds.
+ * A level's region on an axis runs from ceil(origin / 2^k) to ceil((origin + n) / 2^k), k the
+ * level capped at the axis's decomposition count.  Where that start is odd (dwt.c:1393-1396)
+ * the line's first sample is a high-pass sample: the lifting runs one sample further into the
+ * extended buffer, and the flush (dwt.c:645-721) puts the lows w[0], w[2], ... first and the
+ * highs w[-1], w[1], ... after them. */
+static uint64_t level_bound(uint64_t v, int level, int levels) {
+  const int k = level < levels ? level : levels;
+  return (uint64_t)ceil((float)v / (float)(1u << k));
+}
+
+void rs_dwt_forward_tile(rs_float *work, const uint64_t dims[4], const uint64_t origin[4],
+                         const uint8_t decomp[4], const uint8_t kernels[4]) {
+  int n_levels = 0;
+  uint64_t maxlen = 1;
+  for (int a = 0; a < 4; ++a) {
+    if (decomp[a] > n_levels) n_levels = decomp[a];
+    if (dims[a] > maxlen) maxlen = dims[a];
+  }
+  rs_float *line = (rs_float *)calloc(maxlen + 2 * EXT + 2, sizeof(rs_float));
+  const uint64_t stride[4] = {1, dims[0], dims[0] * dims[1], dims[0] * dims[1] * dims[2]};
+  for (int level = 0; level < n_levels; ++level) {
+    uint64_t ext[4], r0[4];
+    for (int b = 0; b < 4; ++b) {
+      r0[b] = level_bound(origin[b], level, decomp[b]);
+      ext[b] = level_bound(origin[b] + dims[b], level, decomp[b]) - r0[b];
+    }
+    for (int a = 0; a < 4; ++a) {
+      if (!(level < decomp[a] && ext[a] > 1)) continue;
+      const int64_t len = (int64_t)ext[a];
+      const int odd = (int)(r0[a] % 2);
+      const int64_t half = odd ? len >> 1 : (len + 1) >> 1;
+      int o[3], k = 0;
+      for (int b = 0; b < 4; ++b)
+        if (b != a) o[k++] = b;
+      rs_float *B = line + EXT;   /* the line's samples at B[0..len) */
+      rs_float *w = B + odd;      /* the lifting's coordinates */
+      for (uint64_t i2 = 0; i2 < ext[o[2]]; ++i2)
+        for (uint64_t i1 = 0; i1 < ext[o[1]]; ++i1)
+          for (uint64_t i0 = 0; i0 < ext[o[0]]; ++i0) {
+            rs_float *base = work + i0 * stride[o[0]] + i1 * stride[o[1]] + i2 * stride[o[2]];
+            for (int64_t i = 0; i < len; ++i) B[i] = base[i * stride[a]];
+            extend(B, len);
+            if (kernels[a] == 1) lift_forward_53(w, len); else lift_forward(w, len);
+            for (int64_t i = 0; i < half; ++i) base[i * stride[a]] = w[2 * i];
+            for (int64_t j = 0; j < len - half; ++j)
+              base[(half + j) * stride[a]] = w[2 * j + (odd ? -1 : 1)];
+          }
+    }
+  }
+  free(line);
+}
+
 void rs_dwt_forward_kernels(rs_float *work, const uint64_t dims[4], const uint8_t decomp[4],
                             const uint8_t kernels[4]) {
   dwt(work, dims, decomp, 1, kernels);

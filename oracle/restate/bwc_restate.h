@@ -53,6 +53,10 @@ void rs_dwt_forward_kernels(rs_float *work, const uint64_t dims[4], const uint8_
                             const uint8_t kernels[4]);
 void rs_dwt_inverse_kernels(rs_float *work, const uint64_t dims[4], const uint8_t decomp[4],
                             const uint8_t kernels[4]);
+/* forward transform of one tile of a multi-tile field: dims = the tile's extent, origin = its
+ * first sample in field coordinates (odd region starts follow dwt.c:1393-1396, 645-721) */
+void rs_dwt_forward_tile(rs_float *work, const uint64_t dims[4], const uint64_t origin[4],
+                         const uint8_t decomp[4], const uint8_t kernels[4]);
 
 /* one codeblock: box in working-buffer coordinates and its subband's coding parameters */
 typedef struct {
