@@ -17,8 +17,11 @@ Under torchrun every rank compresses its own field (independent replicas, weak s
 time is the maximum over ranks.
 
 --impl reference times the reference's own CPU library (compiled from its sources into
-oracle/_ref) with all host threads on a bounded sample of the same workload (a 256^3 corner of
-the field, same settings), rank 0 only.
+oracle/_ref) with all host threads on the same field and settings, rank 0 only.
+
+cpu_baseline (ours) = the same reference library on the same full field with all host threads
+(plus one thread on the central 128^3 cube); its codestream and decompressed field are compared
+with this library's byte for byte and bit for bit ("parity_vs_reference").
 """
 from __future__ import annotations
 
@@ -155,81 +158,98 @@ def max_over_ranks(ws, v):
     return float(t.item())
 
 
-def sample_window(n):
-    """Central (n/2)^3 cube: it overlaps the constant quarter in the same 1/4 proportion as the
-    whole field and crosses the shock fronts like it."""
-    s = max(1, n // 2)
+def sample_window(n, frac=2):
+    """Central (n/frac)^3 cube: it overlaps the constant quarter in the same 1/4 proportion as
+    the whole field and crosses the shock fronts like it."""
+    s = max(1, n // frac)
     o = (n - s) // 2
     return slice(o, o + s), s
 
 
+def ref_compress_timed(field_np, prec, threads, rates=RATES, decomp=DECOMP, cb=CODEBLOCKS):
+    """One reference bwc_compress (set-up excluded from the time), gain table reset first."""
+    from oracle import ref
+    ref.set_threads(threads, prec)
+    ref.reset_gain_lut(prec)
+    rc = ref.RefCompressor(field_np, precision=prec, decomp=decomp, cb=cb, rate=rates)
+    try:
+        t0 = time.perf_counter()
+        cs = rc.compress()
+        dt = time.perf_counter() - t0
+    finally:
+        rc.close()
+    return cs, dt
+
+
 def cpu_baseline(field_np, a, threads=None):
-    """Reference CPU library on a bounded sample: the central 256^3 cube of the field."""
+    """The reference CPU library on the same full field and settings with all host threads
+    (compress and decompress timed), and with one thread on the central 128^3 cube.  Returns the
+    baseline object plus the reference's codestream and decompressed field for the parity
+    check."""
     from oracle import ref
     prec = "double" if a.dtype == "f64" else "single"
     threads = threads or os.cpu_count()
+    cs, dt = ref_compress_timed(field_np, prec, threads)
     ref.set_threads(threads, prec)
-    w, s = sample_window(a.size)
-    sub = np.ascontiguousarray(field_np[w, w, w])
-    ref.reset_gain_lut(prec)
-    rc = ref.RefCompressor(sub, precision=prec, decomp=DECOMP, cb=CODEBLOCKS, rate=RATES)
     t0 = time.perf_counter()
-    cs = rc.compress()
-    dt = time.perf_counter() - t0
-    rc.close()
-    t0 = time.perf_counter()
-    ref.decompress(cs, sub.shape, sub.dtype, prec)
+    dec = ref.decompress(cs, field_np.shape, field_np.dtype, prec)
     ddt = time.perf_counter() - t0
-    return {"value": sub.nbytes / dt / 1e9, "unit": "GB/s", "cores": threads,
+    w, s1 = sample_window(a.size, 4)
+    sub = np.ascontiguousarray(field_np[w, w, w])
+    _, dt1 = ref_compress_timed(sub, prec, 1)
+    ref.set_threads(threads, prec)
+    base = {"value": field_np.nbytes / dt / 1e9, "unit": "GB/s", "cores": threads,
             "kind": "reference",
-            "sample": f"central {s}^3 cube of the field ({sub.nbytes / 2**20:.0f} MiB), same "
-                      f"settings, one bwc_compress, {threads} OpenMP threads",
-            "decompress_GBps": sub.nbytes / ddt / 1e9}
+            "sample": f"the full field ({field_np.nbytes / 2**20:.0f} MiB), same settings, one "
+                      f"bwc_compress and one bwc_decompress, {threads} OpenMP threads",
+            "decompress_GBps": field_np.nbytes / ddt / 1e9,
+            "single_thread": {"value": sub.nbytes / dt1 / 1e9, "unit": "GB/s", "cores": 1,
+                              "sample": f"central {s1}^3 cube of the field, same settings"}}
+    return base, cs, dec
 
 
 def run_reference(a):
-    ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    """The reference's own CPU library (oracle/_ref, all host threads) on the same field and
+    settings as this library's arm: W untimed and K timed bwc_compress calls, rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from oracle import ref
     prec = "double" if a.dtype == "f64" else "single"
-    w, s = sample_window(a.size)
     try:
         import torch
         gpu = torch.cuda.is_available()
     except Exception:
         gpu = False
     if gpu:
-        # the same field as the GPU arm (generated on the device); its central cube to the host
-        field = make_field(a, "cuda")[w, w, w].cpu().numpy()
+        # the same field as the GPU arm, generated on the device, moved to the host
+        field = make_field(a, "cuda").cpu().numpy()
+        torch.cuda.empty_cache()
+        sample = "the full field"
     else:
-        # no GPU to evaluate the full-size generator quickly: a field of the sample's size
+        # no GPU to evaluate the full-size generator quickly: the central cube of the field
         from bigwhoop_b200 import fields
+        w, s = sample_window(a.size)
         dt = np.float64 if a.dtype == "f64" else np.float32
         field = fields.shock_field((s, s, s), 1, dtype=dt)
-    sub = np.ascontiguousarray(field)
+        sample = f"a {s}^3 field of the same generator (no GPU to generate the full field)"
+    field = np.ascontiguousarray(field)
     threads = os.cpu_count()
-    ref.set_threads(threads, prec)
     times = []
     for i in range(a.warmup + a.steps):
-        ref.reset_gain_lut(prec)
-        rc = ref.RefCompressor(sub, precision=prec, decomp=DECOMP, cb=CODEBLOCKS, rate=RATES)
-        t0 = time.perf_counter()
-        rc.compress()
-        t = time.perf_counter() - t0
-        rc.close()
+        _, t = ref_compress_timed(field, prec, threads)
         if i >= a.warmup:
             times.append(t)
     tt = float(np.mean(times))
-    v = sub.nbytes / tt / 1e9
+    v = field.nbytes / tt / 1e9
     line = {"metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": a.gpus, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": tt * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if a.dtype == "f64" else "f32",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": workload_name(a) + f" (reference sample: central {s}^3 cube)"},
+            "config": {"workload": workload_name(a), "codec_precision": prec,
+                       "rates_bpv": RATES},
             "cpu_baseline": {"value": v, "unit": "GB/s", "cores": threads, "kind": "reference",
-                             "sample": f"central {s}^3 cube, same settings, {threads} OpenMP "
-                                       f"threads"},
+                             "sample": f"{sample}, same settings, one bwc_compress per step, "
+                                       f"{threads} OpenMP threads"},
             "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -340,15 +360,15 @@ def run_ours(a):
         if os.path.exists(pk):
             peaks = json.load(open(pk))
         hbm = peaks.get("hbm_gbs", 6650.0)
-        # dominant kernel: tier-1 encoder (stage index 3); algorithmic bytes = one read of the
-        # wavelet coefficients + one write of the full-depth coded bytes
+        clk = clocks.summary()
+        sm_hz = (clk.get("sm_mhz") or peaks.get("sm_max_mhz") or 1965.0) * 1e6
         t1_ms = float(stage[3])
         s_bytes = 8 if prec == "double" else 4
         n_vals = field.numel()
-        alg_t1 = n_vals * s_bytes + 0
         dwt_ms = float(stage[2])
         # DWT algorithmic bytes: one read + one write of each level's region, all axes fused
         alg_dwt = sum(2 * s_bytes * n_vals / 8 ** l for l in range(4))
+        t1 = tier1_roofline(stage, dstage, sm_hz, prec)
         line = {
             "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": ws, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
@@ -366,19 +386,15 @@ def run_ours(a):
                           "tier1_download": round(float(stage[4]), 3),
                           "tier2_host": round(float(stage[5]), 3),
                           "assembly": round(float(stage[6]), 3)},
-            "roofline": {"bound": "hbm", "kernel": "t1_encode_kernel",
-                         "achieved": alg_t1 / (t1_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
-                         "frac": alg_t1 / (t1_ms * 1e-3) / 1e9 / hbm, "traffic": None,
-                         "note": "tier-1 is integer-issue bound; HBM fraction shown for the "
-                                 "coefficient read only",
-                         "peak_source": "measured" if peaks else "fallback"},
+            "roofline": t1["roofline"],
+            "tier1_kernels": t1["kernels"],
             "roofline_dwt": {"bound": "hbm", "achieved": alg_dwt / (dwt_ms * 1e-3) / 1e9,
                              "peak": hbm, "unit": "GB/s",
                              "frac": alg_dwt / (dwt_ms * 1e-3) / 1e9 / hbm},
             "quality": {"psnr_db": psnr, "max_abs_err": float(err.max()),
                         "codestream_bytes": len(cs), "bpv": len(cs) * 8 / field.numel(),
                         "device_and_host_codestreams_equal": cs == cs_dev},
-            "clocks": clocks.summary(),
+            "clocks": clk,
             # plus the rate model's forward pass (one launch for all layers) when it predicted
             "gpu_launches": launches + (1 if (rate_warm[:, 3] >= 0).any() else 0),
             "rate_control": {
@@ -392,12 +408,73 @@ def run_ours(a):
         if not a.no_batch and ws == 1:
             line["batch"] = batch_compare(prec)
         if not a.no_cpu_baseline and ws == 1:
-            line["cpu_baseline"] = cpu_baseline(host_in.numpy(), a)
+            base, cs_ref, dec_ref = cpu_baseline(host_in.numpy(), a)
+            line["cpu_baseline"] = base
+            rec_np = dec_out.numpy()
+            line["parity_vs_reference"] = {
+                "codestream_identical": cs_ref == cs_dev,
+                "codestream_bytes": [len(cs_dev), len(cs_ref)],
+                "decompression_bit_identical": bool(np.array_equal(
+                    rec_np.view(np.uint64 if rec_np.dtype == np.float64 else np.uint32),
+                    dec_ref.view(np.uint64 if dec_ref.dtype == np.float64 else np.uint32))),
+                "what": "this library's codestream of the full field (device-resident call) "
+                        "against the reference library's, and its decompression of that "
+                        "codestream against the reference's decompression"}
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
     return 0
+
+
+# Warp instructions issued per coded symbol by each tier-1 kernel, from the ncu capture named
+# beside it (instruction counts of the 256^3 bench field divided by its symbol count; the
+# figures do not depend on the field size).  The live part of the roofline is the symbol count
+# and each kernel's CUDA-event time in this run.
+T1_WARP_INSTR_PER_SYMBOL = {
+    "t1_model_kernel": (10.6, "profiles/t1_kernels_256cube_f64.md"),
+    "t1_mq_kernel": (44.0, "profiles/t1_kernels_256cube_f64.md"),
+}
+SMS = 148
+
+
+def tier1_roofline(stage, dstage, sm_hz, prec):
+    """Tier-1 against its bound, integer instruction issue: symbols per second per kernel and the
+    fraction of the GPU's warp-instruction issue slots (148 SMs x 4 schedulers x SM clock) the
+    kernel's instructions would fill over its measured time."""
+    sym = float(stage[8]) * 1e6 if len(stage) > 8 else 0.0
+    model_ms = float(stage[9]) if len(stage) > 9 else 0.0
+    t1_ms = float(stage[3])
+    kernels = {}
+    peak = SMS * 4 * sm_hz
+    for name, ms in (("t1_model_kernel", model_ms), ("t1_mq_kernel", t1_ms - model_ms)):
+        ipsym, src = T1_WARP_INSTR_PER_SYMBOL[name]
+        if ms <= 0 or sym <= 0:
+            continue
+        rate = ipsym * sym / (ms * 1e-3)
+        kernels[name] = {"ms": round(ms, 3), "symbols": sym,
+                         "Gsymbols_per_s": sym / (ms * 1e-3) / 1e9,
+                         "warp_instr_per_symbol": ipsym, "instr_source": src,
+                         "issue_frac": rate / peak}
+    kernels["t1_decode_kernel"] = {"ms": round(float(dstage[3]), 3) if len(dstage) > 3 else None}
+    dom = max((k for k in kernels if "issue_frac" in kernels[k]),
+              key=lambda k: kernels[k]["ms"], default=None)
+    if dom is None:
+        roof = {"bound": "int_issue", "achieved": None, "peak": peak / 1e12, "unit": "Twarp-instr/s",
+                "frac": None, "traffic": None}
+    else:
+        k = kernels[dom]
+        ach = k["warp_instr_per_symbol"] * sym / (k["ms"] * 1e-3)
+        roof = {"bound": "int_issue", "kernel": dom, "achieved": ach / 1e12, "peak": peak / 1e12,
+                "unit": "Twarp-instr/s", "frac": ach / peak, "traffic": None,
+                "symbols_per_s": sym / (k["ms"] * 1e-3),
+                "note": "tier-1 has no HBM or tensor bound: the MQ coder is one dependent chain "
+                        "per codeblock and the context modelling is scalar integer logic; the "
+                        "denominator is the GPU's warp-instruction issue rate at the sampled SM "
+                        "clock, the numerator the kernel's ncu-counted instructions per symbol "
+                        "times the symbols coded per second in this run",
+                "peak_source": "148 SMs x 4 issue slots x sampled SM clock"}
+    return {"roofline": roof, "kernels": kernels}
 
 
 def batch_compare(prec):

@@ -324,8 +324,8 @@ class Compressor:
         return n
 
     def timings(self):
-        out = np.zeros(9)
-        k = self.L.bwc_b200_last_timings(self.codec, out.ctypes.data, 9)
+        out = np.zeros(10)
+        k = self.L.bwc_b200_last_timings(self.codec, out.ctypes.data, 10)
         return out[:k]
 
     def close(self):
@@ -392,8 +392,8 @@ class Decompressor:
         return self.out
 
     def timings(self):
-        out = np.zeros(9)
-        k = self.L.bwc_b200_last_timings(self.codec, out.ctypes.data, 9)
+        out = np.zeros(10)
+        k = self.L.bwc_b200_last_timings(self.codec, out.ctypes.data, 10)
         return out[:k]
 
     def close(self):

@@ -132,7 +132,8 @@ struct DeviceState {
   bool dump_set = false, ddump_set = false;
   bwc_b200_stage_dump dump{};
   bwc_b200_decode_dump ddump{};
-  double timings[10] = {};   // stage times (ms); [8] tier-1 symbols coded (millions)
+  double timings[10] = {};   // stage times (ms); [8] tier-1 symbols coded (millions),
+                             // [9] tier-1 context modelling kernel (ms, part of [3])
 
   ~DeviceState() {
     DevBuf *all[] = {&order, &queue, &temp, &in, &work, &keys, &stats, &cbtab, &sbtab, &bytes, &scratch, &snaps, &dmse,
@@ -172,7 +173,7 @@ void free_engine(bwc_codec *codec) {
 
 // timing events of one stage sequence, released however the scope is left
 struct ScopedEvents {
-  cudaEvent_t e[4];
+  cudaEvent_t e[5];
   ScopedEvents() {
     for (auto &x : e) cudaEventCreate(&x);
   }
@@ -519,10 +520,10 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
     cudaMemcpyAsync(dv->order.p, order.data(), ncb * 4, cudaMemcpyHostToDevice, s);
     if (!cuda_ok(cudaStreamSynchronize(s), "tier-1 order")) return 0;
   }
-  float t_norm = 0, t_dwt = 0, t_t1 = 0;
+  float t_norm = 0, t_dwt = 0, t_t1 = 0, t_model = 0;
   for (int p = 0; p < info.nPar; ++p) {
     const ScopedEvents evs;
-    cudaEvent_t a = evs.e[0], b2 = evs.e[1], c2 = evs.e[2], d2 = evs.e[3];
+    cudaEvent_t a = evs.e[0], b2 = evs.e[1], c2 = evs.e[2], d2 = evs.e[3], m2 = evs.e[4];
     cudaEventRecord(a, s);
     launch_fill_minmax(src + (uint64_t)p * n * dsz, dsz == 8, n, dv->temp.as<bwc_float>(),
                        dv->keys.as<uint64_t>() + 2 * p, s);
@@ -558,7 +559,7 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
       cudaMemsetAsync(o.flags, 0, cbs[p].size() * 4, s);
       launch_t1_encode(dv->work.as<bwc_float>(), dv->cbtab.as<CbDev>() + cb_base[p],
                        (uint32_t)cbs[p].size(), dv->sbtab.as<SbDev>(), o, max_cols, s,
-                       dv->order.as<uint32_t>() + cb_base[p], dv->queue.as<uint32_t>());
+                       dv->order.as<uint32_t>() + cb_base[p], dv->queue.as<uint32_t>(), m2);
       unsigned long long used = 0;
       cudaMemcpyAsync(&used, dv->symused.p, 8, cudaMemcpyDeviceToHost, s);
       if (!cuda_ok(cudaStreamSynchronize(s), "tier-1 encoding")) return 0;
@@ -581,6 +582,7 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
     cudaEventElapsedTime(&x, a, b2); t_norm += x;
     cudaEventElapsedTime(&x, b2, c2); t_dwt += x;
     cudaEventElapsedTime(&x, c2, d2); t_t1 += x;
+    cudaEventElapsedTime(&x, c2, m2); t_model += x;
   }
 
   // tier-1 summary to the host
@@ -697,6 +699,7 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
   dv->timings[5] = std::chrono::duration<double, std::milli>(h1 - h0).count();
   dv->timings[6] = as;
   dv->timings[7] = up + t_norm + t_dwt + t_t1 + dl + dv->timings[5] + as;
+  dv->timings[9] = t_model;
   dv->dump_set = false;
   return total;
 }
@@ -1374,7 +1377,7 @@ extern "C" void bwc_b200_set_decode_dump(bwc_codec *const codec, bwc_b200_decode
 
 extern "C" int bwc_b200_last_timings(bwc_codec *const codec, double *out_ms, int n) {
   if (!codec || !codec->tile || !codec->tile->dev) return 0;
-  const int k = std::min(n, 9);
+  const int k = std::min(n, 10);
   for (int i = 0; i < k; ++i) out_ms[i] = codec->tile->dev->timings[i];
   return k;
 }

@@ -88,10 +88,12 @@ size_t t1_model_smem(uint32_t max_cols);
 // Each codeblock addresses its samples as work[base + x + y*sy + z*sz + t*st].  `order`
 // (optional, device) lists the codeblocks largest first: the MQ kernel's lanes take them in
 // that order, and with `queue` (a device counter, zeroed here) the modelling kernel runs
-// persistent and takes codeblocks from that work queue.
+// persistent and takes codeblocks from that work queue.  `after_model` (optional) is recorded
+// on `s` between the modelling and the MQ kernel.
 void launch_t1_encode(const bwc_float *work, const CbDev *cbs, uint32_t ncb, const SbDev *sbs,
                       const T1EncOut &out, uint32_t max_cols, cudaStream_t s,
-                      const uint32_t *order = nullptr, uint32_t *queue = nullptr);
+                      const uint32_t *order = nullptr, uint32_t *queue = nullptr,
+                      cudaEvent_t after_model = nullptr);
 
 // t1_decode.cu: decodes Z[c] passes of codeblock c from data + out_off (Lmax[c] bytes) and
 // writes the dequantised samples into the (zeroed) working buffer.

@@ -1054,7 +1054,7 @@ void load_tune_file_locked() {
 // warps lengthen the latency-bound MQ chains, and the longest chain sets the time.)
 void launch_t1_encode(const bwc_float *work, const CbDev *cbs, uint32_t ncb, const SbDev *sbs,
                       const T1EncOut &out, uint32_t max_cols, cudaStream_t s,
-                      const uint32_t *order, uint32_t *queue) {
+                      const uint32_t *order, uint32_t *queue, cudaEvent_t after_model) {
   if (!ncb) return;
   const size_t smem = t1_model_smem(max_cols);
   cudaFuncSetAttribute(t1_model_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1070,6 +1070,7 @@ void launch_t1_encode(const bwc_float *work, const CbDev *cbs, uint32_t ncb, con
   }
   t1_model_kernel<<<grid, kModelThreads, smem, s>>>(work, cbs, ncb, sbs, out, order, queue,
                                                     t1_model_stage_cap(max_cols));
+  if (after_model) cudaEventRecord(after_model, s);
   const uint32_t rule = mq_lanes_per_warp(ncb);
   uint32_t lanes = rule;
   bool tune = false;

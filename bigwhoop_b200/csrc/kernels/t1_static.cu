@@ -2,8 +2,7 @@
 // bwc_b200_t1_encode_codeblock_static.
 //
 // Who needs it: code that must not call cudaMalloc -- a caller working inside a framework whose
-// memory pool owns the device memory, a code path recorded into a stream capture, where an
-// allocation is not allowed, or a latency-bound service that cannot afford the implicit
+// memory pool owns the device memory, or a latency-bound service that cannot afford the implicit
 // synchronisation of an allocation.  Such a caller owns its inputs and outputs already; what it
 // cannot provide is this library's tier-1 working memory (bit planes, the symbol arena, coder
 // snapshots).  Here that working memory is one fixed static device array, sized for the largest
@@ -11,7 +10,9 @@
 // process exits.
 //
 // The kernels are the ones bwc_compress runs (t1_model_kernel, t1_mq_kernel through
-// launch_t1_encode); only where their scratch lives differs.
+// launch_t1_encode); only where their scratch lives differs.  The codeblock and subband records
+// reach the static area through a one-thread set-up kernel that takes them as arguments, so no
+// host memory is read after the call returns.
 #include <cstdio>
 #include <mutex>
 
@@ -71,6 +72,24 @@ unsigned char *static_area(int device) {
   return g_static_addr[device];
 }
 
+// Writes the call's codeblock and subband records into the static area and clears what must
+// start from zero: the symbol bump counter, the flags and the slope range (minimum 0xFFFF).
+// Planes, symbol chunks, snapshots and per-pass records are rewritten before they are read.
+__global__ void static_setup_kernel(unsigned char *base, CbDev cb, SbDev sb) {
+  *reinterpret_cast<CbDev *>(base + kOffCb) = cb;
+  *reinterpret_cast<SbDev *>(base + kOffSb) = sb;
+  *reinterpret_cast<unsigned long long *>(base + kOffUsed) = 0ull;
+  uint32_t *slopes = reinterpret_cast<uint32_t *>(base + kOffSlopes);
+  slopes[0] = 0xFFFF;
+  slopes[1] = 0;
+  *reinterpret_cast<uint32_t *>(base + kOffFlags) = 0;
+}
+
+// Copies the codeblock's flags to the caller's status word (device to device, no host copy).
+__global__ void static_status_kernel(const unsigned char *base, uint32_t *status) {
+  *status = *reinterpret_cast<const uint32_t *>(base + kOffFlags);
+}
+
 int reject(const char *why) {
   fprintf(stderr, "bwc_b200_t1_encode_codeblock_static: %s\n", why);
   return 1;
@@ -101,12 +120,27 @@ extern "C" int bwc_b200_t1_encode_codeblock_static(
              "(16384 samples)", (unsigned long long)ncols, kStaticMaxCols);
     return reject(msg);
   }
+  // An error left pending by the caller's own earlier CUDA calls would be reported after the
+  // launches below as if they had failed; refuse before queuing anything instead.
+  const cudaError_t pending = cudaPeekAtLastError();
+  if (pending != cudaSuccess) {
+    char msg[200];
+    snprintf(msg, sizeof msg, "a CUDA error is pending from earlier calls (%s); nothing queued",
+             cudaGetErrorString(pending));
+    return reject(msg);
+  }
   int device = 0;
   if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kMaxDevices)
     return reject("no usable current CUDA device");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (s) {
+    // the static area's address is the current device's: the stream must belong to it
+    int sdev = -1;
+    if (cudaStreamGetDevice(s, &sdev) != cudaSuccess) return reject("invalid stream");
+    if (sdev != device) return reject("the stream belongs to another device than the current one");
+  }
   unsigned char *base = static_area(device);
   if (!base) return 1;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
 
   CbDev cb{};
   cb.x0 = (uint32_t)box[0];
@@ -133,16 +167,16 @@ extern "C" int bwc_b200_t1_encode_codeblock_static(
   // significance-context class from the subband's high-pass axes (tier1.c:2416-2446)
   sb.cls = ((highband & 3) == 1) ? 1u : ((highband & 3) == 3) ? 2u : 0u;
   sb.erres = erres ? 1u : 0u;
-  const uint32_t slopes_init[2] = {0xFFFF, 0};
 
-  // The static area keeps the previous call's contents: the symbol counter, the slope range
-  // and the flags must start from zero (slope minimum from 0xFFFF); planes, symbol chunks,
-  // snapshots and per-pass records are rewritten before they are read.
-  cudaMemcpyAsync(base + kOffCb, &cb, sizeof cb, cudaMemcpyHostToDevice, s);
-  cudaMemcpyAsync(base + kOffSb, &sb, sizeof sb, cudaMemcpyHostToDevice, s);
-  cudaMemcpyAsync(base + kOffSlopes, slopes_init, sizeof slopes_init, cudaMemcpyHostToDevice, s);
-  cudaMemsetAsync(base + kOffUsed, 0, 8, s);
-  cudaMemsetAsync(base + kOffFlags, 0, 4, s);
+  // The static area keeps the previous call's contents; the set-up kernel writes this call's
+  // records and clears the counters before the tier-1 kernels run on the same stream.
+  static_setup_kernel<<<1, 1, 0, s>>>(base, cb, sb);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    fprintf(stderr, "bwc_b200_t1_encode_codeblock_static: set-up launch: %s\n",
+            cudaGetErrorString(e));
+    return 1;
+  }
 
   T1EncOut o;
   o.bytes = bytes;
@@ -162,8 +196,11 @@ extern "C" int bwc_b200_t1_encode_codeblock_static(
   o.pass_off = reinterpret_cast<uint64_t *>(base + kOffPoff);
   launch_t1_encode(coeffs, reinterpret_cast<const CbDev *>(base + kOffCb), 1,
                    reinterpret_cast<const SbDev *>(base + kOffSb), o, (uint32_t)ncols, s);
-  cudaMemcpyAsync(status, base + kOffFlags, 4, cudaMemcpyDeviceToDevice, s);
-  const cudaError_t e = cudaGetLastError();
+  e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    static_status_kernel<<<1, 1, 0, s>>>(base, status);
+    e = cudaGetLastError();
+  }
   if (e != cudaSuccess) {
     fprintf(stderr, "bwc_b200_t1_encode_codeblock_static: %s\n", cudaGetErrorString(e));
     return 1;

@@ -109,7 +109,9 @@ size_t bwc_b200_assemble_tiles_from_tier1(bwc_codec *const codec, bwc_stream *co
 /* Device time of the stages of the last bwc_compress / bwc_decompress on this codec, in
  * milliseconds (CUDA events on the codec's stream): [0] upload, [1] fill+normalise, [2] wavelet,
  * [3] tier-1, [4] download of tier-1 results, [5] tier-2 (host), [6] codestream gather and
- * download, [7] total.  Returns the number of entries written (at most n). */
+ * download, [7] total, [8] tier-1 symbols coded (millions, compression), [9] the tier-1 context
+ * modelling kernel alone (compression; the rest of [3] is the MQ coder).  Returns the number of
+ * entries written (at most n). */
 int    bwc_b200_last_timings(bwc_codec *const codec, double *out_ms, int n);
 
 /* Batched compression of n independently configured codecs (each set up with
@@ -185,11 +187,11 @@ int    bwc_b200_mlp_train(float *params, const float *X, const float *t, uint32 
  * reference API.
  *
  * For callers that cannot call cudaMalloc -- code that gets its device memory from a
- * framework's pool, code recorded into a stream capture, latency-bound services that cannot
- * take the synchronisation an allocation implies.  The caller passes device buffers it owns;
- * the library's own working memory (bit planes, symbol arena, coder snapshots) is one fixed
- * static device area of about 2.9 MB (double build; 1.5 MB single), held by every GPU that
- * loads the library until the process exits.
+ * framework's pool, latency-bound services that cannot take the synchronisation an
+ * allocation implies.  The caller passes device buffers it owns; the library's own working
+ * memory (bit planes, symbol arena, coder snapshots) is one fixed static device area of about
+ * 2.9 MB (double build; 1.5 MB single), held by every GPU that loads the library until the
+ * process exits.
  *
  *   coeffs          device pointer: wavelet coefficients of one parameter, nX x nY x nZ x nTS
  *                   bwc_float values, x fastest (the layout bwc_compress transforms into);
@@ -212,13 +214,15 @@ int    bwc_b200_mlp_train(float *params, const float *X, const float *t, uint32 
  *
  * Limit: at most 4096 stripe columns (width x ceil(height / 4) x depth x time steps, e.g. a
  * 32 x 32 x 16 codeblock); larger ones are rejected with a message on stderr and return 1.
- * Returns 0 once the work is queued on `stream`, 1 on rejected arguments or a CUDA error.
+ * Returns 0 once the work is queued on `stream`, 1 on rejected arguments or a CUDA error (an
+ * error already pending from the caller's earlier CUDA calls is refused before anything is
+ * queued).  `stream` must belong to the current device on every call.
  *
- * The static area is shared by every call on a device and keeps the last call's contents, so
- * calls that overlap on the GPU (different streams, or host threads without ordering) race
- * and corrupt each other; order them on one stream.  The first call on a device looks up the
- * area's device address (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture. */
+ * The static area is shared by every call on a device and keeps the last call's contents (each
+ * call clears what must start at zero), so calls that overlap on the GPU (different streams, or
+ * host threads without ordering) race and corrupt each other; order them on one stream.  The
+ * first call on a device looks up the area's device address (cudaGetSymbolAddress) with that
+ * device current; make that first call before any stream capture. */
 int    bwc_b200_t1_encode_codeblock_static(const bwc_float *coeffs, uint64 nX, uint64 nY,
                                            uint64 nZ, uint64 nTS, const uint64 *box,
                                            bwc_float qt_eff, double gain_step2, uint8 highband,

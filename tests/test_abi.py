@@ -15,7 +15,8 @@ from conftest import ROOT, need_ref
 from bigwhoop_b200 import bwc
 
 INCLUDE = os.path.join(ROOT, "include")
-REF_INC = "/root/reference/include/library/private"
+# the reference's private headers, copied there by the oracle's recipe (make -C oracle)
+REF_INC = os.path.join(ROOT, "oracle", "_ref", "include")
 
 
 def _declared_functions(header):

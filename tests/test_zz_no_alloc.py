@@ -1,11 +1,11 @@
 """bwc_b200_t1_encode_codeblock_static: tier-1 encoding of one codeblock with no allocation.
 
-Callers that cannot call cudaMalloc (device memory owned by a framework's pool, work recorded
-into a stream capture, services that cannot take an allocation's synchronisation) use this
-entry point with buffers they own; the library's working memory is a fixed static device area.
-Its results must equal what bwc_compress computes for the same codeblock -- bit for bit, as
-everywhere in tier-1 -- on two calls in a row (the static area keeps the previous call's
-contents).
+Callers that cannot call cudaMalloc (device memory owned by a framework's pool, services that
+cannot take an allocation's synchronisation) use this entry point with buffers they own; the
+library's working memory is a fixed static device area.  Its results must equal what
+bwc_compress computes for the same codeblock, and what the reference library computes for it
+(oracle/_ref) -- bit for bit, as everywhere in tier-1 -- on two calls in a row (the static area
+keeps the previous call's contents), with and without error resilience.
 
 This file is named so that pytest collects it last.
 """
@@ -14,6 +14,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
+from conftest import need_ref
 from parity import attach_stage_dump
 from bigwhoop_b200 import bwc, fields
 
@@ -32,17 +33,32 @@ def _entry(precision):
     return f
 
 
+@pytest.mark.parametrize("erres", [0, 1])
 @pytest.mark.parametrize("precision", ["double", "single"])
-def test_static_codeblock_encoder_matches_compress(gpu, precision):
+def test_static_codeblock_encoder_matches_compress(gpu, precision, erres):
     import torch
+    ref = need_ref(precision)
     dt = np.float64 if precision == "double" else np.float32
     mp = MAX_PASSES[precision]
     f = fields.shock_field((40, 48, 56), 5).astype(dt)
+    kw = dict(precision=precision, decomp=(3, 3, 3, 0), cb=(5, 5, 4, 0), rate="1,4",
+              erres=bool(erres))
+    # the reference's own tier-1 output of every codeblock
+    ref.reset_gain_lut(precision)
+    rc = ref.RefCompressor(f, **kw)
+    try:
+        rc.normalize()
+        rc.dwt()
+        rc.t1()
+        rcb = [rc.codeblock(k) for k in range(rc.num_codeblocks())]
+    finally:
+        rc.close()
     bwc.reset_gain_state(precision)
     c = bwc.Compressor(f, precision=precision, decomp=(3, 3, 3, 0), codeblocks=(5, 5, 4, 0),
-                       rate="1,4")
+                       rate="1,4", erres=bool(erres))
     try:
         ncb = c.num_codeblocks()
+        assert ncb == len(rcb)
         dump = attach_stage_dump(c, ncb, mp)
         c.compress()
         geoms, subs = [], []
@@ -73,7 +89,7 @@ def test_static_codeblock_encoder_matches_compress(gpu, precision):
             s2 = float(np.float32(st[1]) * np.float32(st[1])) if precision == "single" else st[1] * st[1]
             box = (C.c_uint64 * 8)(*[int(v) for v in g[:8]])
             data.fill_(0xAB)
-            rc = encode(coeffs.data_ptr(), *dims, box, st[0], st[2] * s2, int(g[8]), 0,
+            rc = encode(coeffs.data_ptr(), *dims, box, st[0], st[2] * s2, int(g[8]), erres,
                         K.data_ptr(), Z.data_ptr(), L.data_ptr(), S.data_ptr(), data.data_ptr(),
                         cap, status.data_ptr(), None)
             assert rc == 0
@@ -87,6 +103,11 @@ def test_static_codeblock_encoder_matches_compress(gpu, precision):
             n = int(m["L"][-1]) if z else 0
             got = bytes(data[:n].cpu().numpy())
             assert got == bytes(dump.data[m["offset"]:m["offset"] + n]), (rnd, k)
+            r = rcb[k]
+            assert (int(K.item()), z) == (r.K, r.Z), (rnd, k)
+            assert np.array_equal(L.cpu().numpy().view(np.uint32)[:z].astype(np.uint64), r.L), (rnd, k)
+            assert np.array_equal(S.cpu().numpy().view(np.uint16)[:z + 1], r.S), (rnd, k)
+            assert got == r.data, (rnd, k)
             checked += 1
     assert checked == 2 * ncb
 
