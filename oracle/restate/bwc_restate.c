@@ -415,7 +415,26 @@ static void transfer_byte(mq_enc *e) {
   }
 }
 
+/* optional record of every coded decision as one byte (context << 1 | decision) and of the
+ * decision count at the end of every pass (rs_set_symbol_trace) */
+static uint8_t *g_trace;
+static uint64_t g_trace_cap, g_trace_n;
+static uint64_t *g_trace_pass;
+
+void rs_set_symbol_trace(uint8_t *buf, uint64_t cap, uint64_t *pass_end) {
+  g_trace = buf;
+  g_trace_cap = cap;
+  g_trace_n = 0;
+  g_trace_pass = pass_end;
+}
+
+uint64_t rs_symbol_trace_count(void) { return g_trace_n; }
+
 static void mq_encode(mq_enc *e, int k, int bit) {
+  if (g_trace) {
+    if (g_trace_n < g_trace_cap) g_trace[g_trace_n] = (uint8_t)((k << 1) | bit);
+    g_trace_n++;
+  }
   mq_ctx *c = &e->ctx[k];
   const uint32_t p = QE[c->state];
   e->A -= p;
@@ -777,6 +796,7 @@ int64_t rs_t1_encode(const rs_float *work, const uint64_t dims[4], const rs_code
       snap[pass].t = e.t;
       snap[pass].L = e.L;
       dmse[pass] = mse;
+      if (g_trace && g_trace_pass) g_trace_pass[pass] = g_trace_n;
       pass++;
     }
   }

@@ -77,6 +77,13 @@ int64_t rs_t1_encode(const rs_float *work, const uint64_t dims[4], const rs_code
                      int erres, uint8_t *K, uint8_t *Z, uint64_t *L, uint16_t *S, uint8_t *bytes,
                      uint64_t cap);
 
+/* Records, during the following rs_t1_encode calls, every coded decision as one byte
+ * (context << 1 | decision) into buf (up to cap) and the running decision count at the end of
+ * every pass into pass_end[pass]; buf = NULL stops recording.  rs_symbol_trace_count returns
+ * the number of decisions seen since the last rs_set_symbol_trace. */
+void rs_set_symbol_trace(uint8_t *buf, uint64_t cap, uint64_t *pass_end);
+uint64_t rs_symbol_trace_count(void);
+
 /* decode_codeblock + cblkcopy_inverse (tier1.c:2624-2787, :767-931): decodes Z passes of a
  * codeblock with K significant bit planes from len bytes and writes the dequantised samples
  * into `work` (whose codeblock region must be zero).  Returns 0. */

@@ -53,6 +53,8 @@ def load(precision="double"):
     L.rs_context_class.argtypes = [C.c_uint32]
     L.rs_t1_encode.restype = C.c_int64
     L.rs_t1_encode.argtypes = [vp, vp, vp, C.c_int, vp, vp, vp, vp, vp, u64]
+    L.rs_set_symbol_trace.argtypes = [vp, u64, vp]
+    L.rs_symbol_trace_count.restype = u64
     L.rs_t1_decode.restype = C.c_int
     L.rs_t1_decode.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_int, vp, u64]
     _libs[precision] = L
@@ -135,6 +137,24 @@ def t1_encode(work, dims, cb, erres=False, precision="double"):
         raise RuntimeError("restated tier-1 encoder ran out of space")
     z = int(Z[0])
     return int(K[0]), z, Ls[:z].copy(), Ss[:z + 1].copy(), bytes(data[:nb])
+
+
+def t1_symbols(work, dims, cb, erres=False, precision="double"):
+    """The coded decisions of one codeblock in coding order, one byte each
+    (context << 1 | decision), and the decision count at the end of every pass."""
+    L = load(precision)
+    n = int((cb.x1 - cb.x0) * (cb.y1 - cb.y0) * (cb.z1 - cb.z0) * (cb.t1 - cb.t0))
+    cap = n * 80 + 4096
+    buf = np.zeros(cap, np.uint8)
+    ends = np.zeros(MAX_PASSES, np.uint64)
+    L.rs_set_symbol_trace(buf.ctypes.data, cap, ends.ctypes.data)
+    try:
+        K, Z, _, _, _ = t1_encode(work, dims, cb, erres, precision)
+        total = int(L.rs_symbol_trace_count())
+    finally:
+        L.rs_set_symbol_trace(None, 0, None)
+    assert total <= cap
+    return K, Z, buf[:total].copy(), ends[:Z].copy()
 
 
 def t1_decode(work, dims, cb, K, Z, data, erres=False, precision="double"):
