@@ -116,6 +116,28 @@ def build(jobs=None, force=False, precisions=("double", "single"), verbose=False
     return outputs
 
 
+def build_emu(precisions=("double", "single"), force=False):
+    """The host build of the tier-1 kernel bodies (csrc/emu/t1_emu.cu) for the CPU unit tests:
+    lib/emu/<precision>/libt1emu.so, a separate library that libbwc.so does not link."""
+    src = os.path.join(CSRC, "emu", "t1_emu.cu")
+    deps = [src] + _headers()
+    out = {}
+    for prec in precisions:
+        so = os.path.join(LIB, "emu", prec, "libt1emu.so")
+        os.makedirs(os.path.dirname(so), exist_ok=True)
+        if force or _stale(so, deps):
+            cmd = ([NVCC, "-O2", "-std=c++20", "-shared", "-Xcompiler", "-fPIC",
+                    "-Xcompiler", "-ffp-contract=off", "--expt-relaxed-constexpr"] + ARCH
+                   + PRECISIONS[prec] + ["-I", os.path.join(ROOT, "include"), "-I", CSRC,
+                                         "-I", CUDA_INC, src, "-o", so, "-lpthread"])
+            res = subprocess.run(cmd, capture_output=True, text=True)
+            if res.returncode != 0:
+                sys.stderr.write(" ".join(cmd) + "\n" + res.stdout + res.stderr)
+                raise RuntimeError("emu build failed")
+        out[prec] = so
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--jobs", type=int, default=None)
@@ -124,6 +146,8 @@ def main():
     a = ap.parse_args()
     for prec, so in build(a.jobs, a.force, verbose=a.verbose).items():
         print(prec, so)
+    for prec, so in build_emu(force=a.force).items():
+        print("emu", prec, so)
 
 
 if __name__ == "__main__":

@@ -366,7 +366,7 @@ static void build_tables(const Parameter &par, const FieldDims &dims, uchar erre
       d.out_cap = (uint32_t)std::min<uint64_t>(cap, 0xFFFFFFF0u);
       off += (cap + 15) & ~15ull;
       d.scratch_off = soff;
-      soff += (((uint64_t)ncols * (2 + kPrecBit + 1)) + 15) & ~15ull;
+      soff += t1_scratch_bytes(ncols);
     } else {
       d.out_off = 0;   // filled by the caller
       d.out_cap = 0;

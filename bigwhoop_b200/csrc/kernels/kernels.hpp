@@ -85,6 +85,8 @@ void launch_dwt_inverse(bwc_float *work, bwc_float *temp, const FieldDims &dims,
 // t1_encode.cu: context modelling (one CTA per codeblock, max_cols = largest number of stripe
 // columns of a codeblock) followed by MQ coding (one thread per codeblock).
 size_t t1_model_smem(uint32_t max_cols);
+// scratch bytes (bit planes) of one codeblock of ncols stripe columns
+uint64_t t1_scratch_bytes(uint64_t ncols);
 // Each codeblock addresses its samples as work[base + x + y*sy + z*sz + t*st].  `order`
 // (optional, device) lists the codeblocks largest first: the MQ kernel's lanes take them in
 // that order, and with `queue` (a device counter, zeroed here) the modelling kernel runs

@@ -5,38 +5,27 @@
 // encode_codeblock (tier1.c:2303-2588), the MQ coder (mq.c:85-127, :328-556, :587-759,
 // :1151-1175), slope2log and compute_convex_hull (tier1.c:2100-2267).
 //
-// Two kernels.
+// Two kernels, run one after the other on the stream.
 //
-// t1_model_kernel -- one CTA per codeblock.  Quantises the codeblock into bit planes (global
-// scratch), then runs every coding pass over all stripe columns of the codeblock at once and
-// writes the pass's (context, decision) symbols, in the reference's scan order, into the
-// codeblock's symbol stream.  Contexts only couple samples of the same slice, and within a pass
-// a column's outcome depends on its left and upper neighbours' state after the pass and on the
-// right and lower neighbours' state before it:
-//   * magnitude refinement: all contexts use pre-pass state;
-//   * cleanup: a sample's significance after the pass equals (significant | bit) for every
-//     sample the pass visits, so every neighbour's post-pass state is known in closed form;
-//   * significance propagation: a sample is visited only next to a significant sample, so
-//     significance spreads through the pass.  The CTA iterates "column outcome given the
-//     current estimates of its left/upper neighbours' outcomes" to a fixed point; the outcome
-//     is monotone in the neighbours' significance, so the iteration climbs from the pre-pass
-//     state to the sequential result, which is the unique fixed point (dependencies point
-//     backwards in scan order).
-// Each thread generates its columns' symbols once, into its own shared-memory slice; a
-// CTA-wide prefix sum of the counts places them in the pass's arena chunk, and each thread
-// copies its slice there (without the slices -- codeblocks over 4608 stripe columns -- the
-// symbols are counted first and written in a second run).  Per pass the kernel records the
-// symbol count and the distortion decrease.
+// t1_model_kernel -- one CTA of 256 threads per codeblock, persistent over a device work queue
+// (largest codeblocks first).  Quantises the codeblock into bit planes and writes every coding
+// pass's decisions (context << 1 | decision, one byte each, in the reference's scan order) into
+// the codeblock's symbol stream: passes back to back, each starting on a 16-byte boundary, in one
+// region of the shared arena reserved per codeblock for the worst case at its bit-plane count.
+// The body is t1_model.cuh (64-bit sample masks per thread; see there).  Codeblocks of more than
+// 4096 stripe columns run through t1_model_wide_kernel instead (one stripe column at a time per
+// thread, below), which writes the same stream.
 //
-// t1_mq_kernel -- one lane per codeblock.  Runs the MQ arithmetic coder over the codeblock's
-// symbol stream (the only part that is inherently sequential), records the coder state at the
-// end of every pass, terminates, derives the minimal truncation length of every pass, builds
-// the convex hull and the 16-bit log slopes.  A warp holds 1 to 32 codeblocks, each lane with
-// its own loop (mq_lanes_per_warp, or the autotuned count).
+// t1_mq_kernel -- one lane per codeblock, 1 to 32 codeblocks per warp.  Runs the MQ arithmetic
+// coder over the codeblock's stream (t1_mq.cuh: branch-free per decision except byte
+// transfers), records the coder state at the end of every pass, terminates, derives the minimal
+// truncation length of every pass, builds the convex hull and the 16-bit log slopes
+// (t1_common.cuh).
 //
-// Stripe-column state (shared memory, one byte each): lo = significance | sign << 4 (read by
-// neighbours), hi = visited-in-significance-pass | refined << 4 (owner only).  Bit planes: one
-// byte per stripe column per plane, the column's four bits in the low nibble, row 0 at bit 3.
+// t1_model_wide_kernel's stripe-column state (shared memory, one byte each): lo = significance |
+// sign << 4 (read by neighbours), hi = visited-in-significance-pass | refined << 4 (owner only).
+// Bit planes: one byte per stripe column per plane, the column's four bits in the low nibble,
+// row 0 at bit 3.
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
@@ -47,6 +36,8 @@
 
 #include "bwc_b200.h"
 #include "device_common.cuh"
+#include "t1_model.cuh"
+#include "t1_mq.cuh"
 #include "t1_tables.cuh"
 
 namespace bwcb {
@@ -372,7 +363,7 @@ __device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ wo
   __shared__ uint32_t s_wsum[kModelThreads / 32];
   __shared__ int64_t s_wsum64[kModelThreads / 32];
   __shared__ uint32_t s_K, s_ok;
-  __shared__ uint64_t s_base;
+  __shared__ uint64_t s_base, s_stream, s_pos;
   const int tid = threadIdx.x;
   const CbDev cb = cbs[c];
   const SbDev sb = sbs[cb.sb];
@@ -447,23 +438,29 @@ __device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ wo
       planes[(uint64_t)b * g.ncols + col] = (uint8_t)nib;
     }
   }
-  __syncthreads();   // planes and column states are read across threads from here on
   if (tid == 0) {
     out.K[c] = (uint8_t)K;
     out.Z[c] = (uint8_t)(3 * K - 2);
+    // the codeblock's stream, sized for the worst case at K planes; a full arena marks the
+    // codeblock for a retry with a larger one
+    const uint64_t need = t1::stream_bound(g.ncols, (uint32_t)K);
+    const uint64_t base = atomicAdd(out.sym_used, (unsigned long long)need);
+    s_ok = (base + need <= out.sym_cap) ? 1u : 0u;
+    s_stream = base;
+    s_pos = 0;
+    if (!s_ok) out.flags[c] |= 8u;
   }
-  // Every pass's symbols go to their own 16-byte aligned chunk of the shared arena, reserved
-  // once the pass's symbol count is known; a full arena marks the codeblock for a retry.
+  __syncthreads();   // planes and column states are read across threads from here on
+  if (!s_ok) return;
+  // Every pass's symbols go to the next 16-byte aligned chunk of the codeblock's stream, placed
+  // once the pass's symbol count is known.
   auto reserve = [&](uint32_t total) -> uint8_t * {
     if (tid == 0) {
-      const uint64_t need = ((uint64_t)total + 15) & ~15ull;
-      const uint64_t base = atomicAdd(out.sym_used, (unsigned long long)need);
-      s_ok = (base + need <= out.sym_cap) ? 1u : 0u;
-      s_base = base;
-      if (!s_ok) out.flags[c] |= 8u;
+      s_base = s_stream + s_pos;
+      s_pos += ((uint64_t)total + 15) & ~15ull;
     }
     __syncthreads();
-    return s_ok ? out.symbols + s_base : nullptr;
+    return out.symbols + s_base;
   };
   // a thread's staged symbols to their place in the pass's chunk; an overflowed slice (not
   // possible: a column yields at most 10 symbols a pass, and the slice holds 10 per column
@@ -637,11 +634,12 @@ __device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ wo
   }
 }
 
-// Kernel 1.  Without a queue, CTA i models codeblock order[i] (or i).  With a queue it is
-// persistent: every CTA takes the next position of the device work queue (an atomic counter
-// over `order`, largest codeblocks first) until the list is exhausted.
+// Modelling of codeblocks over 4096 stripe columns.  Without a queue, CTA i models codeblock
+// order[i] (or i).  With a queue it is persistent: every CTA takes the next position of the
+// device work queue (an atomic counter over `order`, largest codeblocks first) until the list is
+// exhausted.
 __global__ void __launch_bounds__(kModelThreads)
-    t1_model_kernel(const bwc_float *__restrict__ work, const CbDev *__restrict__ cbs,
+    t1_model_wide_kernel(const bwc_float *__restrict__ work, const CbDev *__restrict__ cbs,
                     uint32_t ncb, const SbDev *__restrict__ sbs, T1EncOut out,
                     const uint32_t *__restrict__ order, uint32_t *queue, uint32_t stage_cap) {
   if (!queue) {
@@ -661,127 +659,92 @@ __global__ void __launch_bounds__(kModelThreads)
   }
 }
 
-// ---- kernel 2: MQ coding, truncation lengths, convex hull ------------------------------------
+// ---- the CUDA block behind t1_model.cuh -----------------------------------------------------
 
-// MQ encoder state (mq.c:68-110)
-struct Mq {
-  uint32_t A, C, T;
-  int32_t t;
-  int32_t L;
+struct DevBlock {
+  int tid;
+  t1::ModelShared *sm;
+  __device__ __forceinline__ void sync() { __syncthreads(); }
+  __device__ __forceinline__ int sync_or(int v) { return __syncthreads_or(v); }
+  __device__ __forceinline__ uint32_t scan(uint32_t v, uint32_t *total) {
+    const int lane = tid & 31, w = tid >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) sm->wsum[w] = x;
+    __syncthreads();
+    uint32_t base = 0, tot = 0;
+#pragma unroll
+    for (int i = 0; i < t1::kModelBlock / 32; ++i) {
+      const uint32_t s = sm->wsum[i];
+      base += (i < w) ? s : 0u;
+      tot += s;
+    }
+    __syncthreads();
+    *total = tot;
+    return base + x - v;
+  }
+  __device__ __forceinline__ uint32_t reduce_max(uint32_t v) {
+    v = __reduce_max_sync(0xffffffffu, v);
+    if ((tid & 31) == 0) sm->wsum[tid >> 5] = v;
+    __syncthreads();
+    uint32_t m = 0;
+#pragma unroll
+    for (int i = 0; i < t1::kModelBlock / 32; ++i) m = max(m, sm->wsum[i]);
+    __syncthreads();
+    return m;
+  }
+  __device__ __forceinline__ void add(long long *p, long long v) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((tid & 31) == 0 && v) atomicAdd(reinterpret_cast<unsigned long long *>(p), (unsigned long long)v);
+  }
+  __device__ __forceinline__ unsigned long long reserve(unsigned long long *c, unsigned long long n) {
+    return atomicAdd(c, n);
+  }
+  __device__ __forceinline__ void copy16(uint8_t *dst, const uint8_t *src, uint32_t n16) {
+    for (uint32_t i = (uint32_t)tid; i < n16; i += t1::kModelBlock)
+      reinterpret_cast<uint4 *>(dst)[i] = reinterpret_cast<const uint4 *>(src)[i];
+  }
+  __device__ __forceinline__ void or_flag(uint32_t *f, uint32_t v) { atomicOr(f, v); }
 };
 
-struct ByteOut {
-  uint8_t *out;
-  uint32_t cap;
-  uint32_t flags;
-};
+constexpr size_t kModelSharedBytes = (sizeof(t1::ModelShared) + 15) & ~size_t(15);
 
-__device__ __forceinline__ void put_byte(const Mq &e, ByteOut &bo) {
-  if (e.L >= 0) {
-    if ((uint32_t)e.L < bo.cap) bo.out[e.L] = (uint8_t)e.T; else bo.flags |= 1u;
-  }
-}
-
-// transfer_byte (mq.c:85-127), due now (t == 0)
-__device__ __forceinline__ void mq_transfer(Mq &e, ByteOut &bo) {
-  if (e.T != 0xFF && (e.C & 0x8000000u)) {
-    e.T++;
-    e.C &= 0x7FFFFFFu;
-  }
-  put_byte(e, bo);
-  e.L++;
-  if (e.T == 0xFF) {
-    e.T = (e.C >> 20) & 0xFF;
-    e.C &= 0xFFFFFu;
-    e.t += 7;
-  } else {
-    e.T = (e.C >> 19) & 0xFF;
-    e.C &= 0x7FFFFu;
-    e.t += 8;
-  }
-}
-
-__device__ void mq_terminate(Mq &e, ByteOut &bo) {
-  // mq_termination (mq.c:706-759)
-  int n = 12 - e.t;
-  e.C <<= e.t;
-  e.t = 0;
-  while (n > 0) {
-    mq_transfer(e, bo);
-    n -= e.t;
-    e.C <<= e.t;
-    e.t = 0;
-  }
-  mq_transfer(e, bo);
-}
-
-// Minimal number of bytes that decode a pass correctly, from the coder state at its end and the
-// bytes emitted later (mq.c:587-675; the single-precision build uses 32-bit split arithmetic).
-// Bytes at or beyond `cap` read as zero (the reference's buffer is zero-filled past its data).
-__device__ int64_t truncation_length(uint32_t A, uint32_t C, int32_t t, uint32_t T, int64_t L,
-                                     const uint8_t *p, uint32_t cap, uint32_t *bad) {
-  auto b = [&](int64_t i) -> uint32_t { return (i >= 0 && i < (int64_t)cap) ? p[i] : 0u; };
-  int guard = 0;
-#ifdef BWC_SINGLE_PRECISION
-  int32_t CrFrac = (int32_t)((uint32_t)C << t);
-  int32_t CArFrac = (int32_t)((uint32_t)A << t) + CrFrac;
-  int32_t CrDec = (int32_t)T, CArDec = (int32_t)T;
-  CrDec += 0x01 & (CrFrac >> 27);
-  CArDec += 0x01 & (CArFrac >> 27);
-  CrFrac &= 0x7FFFFFF;
-  CArFrac &= 0x7FFFFFF;
-  int s = 8;
-  while ((CrDec > 0xff) || (CArDec <= 0xff)) {
-    if (++guard > 64) {
-      *bad = 1;
-      break;
+// Context modelling of codeblocks up to 4096 stripe columns.  Without a queue, CTA i models
+// codeblock order[i] (or i); with a queue it is persistent over the device work queue.
+__global__ void __launch_bounds__(t1::kModelBlock)
+    t1_model_kernel(const bwc_float *__restrict__ work, const CbDev *__restrict__ cbs,
+                    uint32_t ncb, const SbDev *__restrict__ sbs, T1EncOut out,
+                    const uint32_t *__restrict__ order, uint32_t *queue) {
+  extern __shared__ __align__(16) uint8_t smem16[];
+  t1::ModelShared &sm = *reinterpret_cast<t1::ModelShared *>(smem16);
+  uint8_t *stage = smem16 + kModelSharedBytes;
+  DevBlock blk{(int)threadIdx.x, &sm};
+  __shared__ uint32_t s_next;
+  for (;;) {
+    uint32_t i = blockIdx.x;
+    if (queue) {
+      if (threadIdx.x == 0) s_next = atomicAdd(queue, 1u);
+      __syncthreads();
+      i = s_next;
+      __syncthreads();   // every thread has read s_next before it is overwritten
     }
-    const int32_t buff = (L >= 0) ? (int32_t)b(L) : 0;
-    L++;
-    CrDec -= buff << (8 - s);
-    CArDec -= buff << (8 - s);
-    CrDec = (int32_t)((uint32_t)CrDec << s);
-    CArDec = (int32_t)((uint32_t)CArDec << s);
-    CrDec += CrFrac >> (27 - s);
-    CArDec += CArFrac >> (27 - s);
-    CrFrac = (int32_t)((uint32_t)CrFrac << s);
-    CArFrac = (int32_t)((uint32_t)CArFrac << s);
-    CrFrac &= 0x7FFFFFF;
-    CArFrac &= 0x7FFFFFF;
-    s = (buff == 0xFF) ? 7 : 8;
+    if (i >= ncb) return;
+    const uint32_t c = order ? order[i] : i;
+    const CbDev cb = cbs[c];
+    const SbDev sb = sbs[cb.sb];
+    t1::model_codeblock(blk, sm, stage, work, cb, sb, out, c, &dev::c_sig2ctx[0][0],
+                        dev::c_sig2xi, dev::c_xi2cont);
+    __syncthreads();   // shared memory is reused by the next codeblock
+    if (!queue) return;
   }
-#else
-  int64_t Cr = ((int64_t)T << 27) + ((int64_t)C << t);
-  int64_t CAr = ((int64_t)A << t) + Cr;
-  int s = 8;
-  while (((Cr >> 27) > 0xff) || ((CAr >> 27) <= 0xff)) {
-    if (++guard > 64) {
-      *bad = 1;
-      break;
-    }
-    const int64_t buff = (L >= 0) ? (int64_t)b(L) : 0;
-    L++;
-    Cr -= buff << (35 - s);
-    CAr -= buff << (35 - s);
-    Cr = (int64_t)((uint64_t)Cr << s);
-    CAr = (int64_t)((uint64_t)CAr << s);
-    s = (buff == 0xFF) ? 7 : 8;
-  }
-#endif
-  if (L > 0 && b(L - 1) == 0xFF) L--;
-  while (L > 1 && b(L - 2) == 0xFF && b(L - 1) == 0x7F) L -= 2;
-  return L;
 }
 
-__device__ uint16_t slope2log(double lambda) {
-  const uint64_t raw = (uint64_t)__double_as_longlong(lambda);
-  const uint64_t exponent = ((raw & 0x7FF0000000000000ull) >> 44) - 0x41F00ull;
-  const uint64_t mantissa = (raw & 0x000FFFFFFFFFFFFFull) >> 44;
-  const uint64_t r = (exponent + dev::c_frac2log[mantissa]) + 0x10000ull;
-  if (r > 0xFFFF) return 0xFFFF;
-  if (r < 2) return 2;
-  return (uint16_t)r;
-}
+// ---- MQ coding, truncation lengths, convex hull ----------------------------------------------
 
 __global__ void __launch_bounds__(kMqThreads) t1_mq_kernel(const CbDev *__restrict__ cbs,
                                                            uint32_t ncb,
@@ -789,8 +752,8 @@ __global__ void __launch_bounds__(kMqThreads) t1_mq_kernel(const CbDev *__restri
                                                            T1EncOut out, uint32_t lanes,
                                                            const uint32_t *__restrict__ order) {
   __shared__ uint32_t tbl[94];
-  // context states, [context][thread]: every lane of a warp hits its own bank
-  __shared__ uint32_t ctx_all[dev::kCtxTotal][kMqThreads];
+  // context slots, [context][thread]: every lane of a warp hits its own bank
+  __shared__ uint32_t slots[dev::kCtxTotal][kMqThreads];
   for (int i = threadIdx.x; i < 94; i += blockDim.x) tbl[i] = dev::c_mq_states[i];
   __syncthreads();
   // Lanes beyond `lanes`, past the last codeblock, or whose symbol stream did not fit the arena
@@ -798,179 +761,22 @@ __global__ void __launch_bounds__(kMqThreads) t1_mq_kernel(const CbDev *__restri
   const bool lane_used = threadIdx.x < lanes;
   const uint32_t slot = blockIdx.x * lanes + (lane_used ? threadIdx.x : 0u);
   const uint32_t c = (slot < ncb) ? (order ? order[slot] : slot) : ncb;
-  const uint32_t cc = (c < ncb) ? c : 0u;
-  const int K = (lane_used && c < ncb) ? out.K[c] : 0;
-  const bool live = (K != 0) && !(out.flags[cc] & 8u);
-  const CbDev cb = cbs[cc];
+  if (!lane_used || c >= ncb) return;
+  const int K = out.K[c];
+  if (K == 0 || (out.flags[c] & 8u)) return;
+  const CbDev cb = cbs[c];
   const SbDev sb = sbs[cb.sb];
-  const int Z = live ? out.Z[c] : 0;
-  // context slots hold their current state's table entry
-  uint32_t *ctx = &ctx_all[0][threadIdx.x];   // context k at ctx[k * kMqThreads]
-  for (int i = 0; i < dev::kCtxTotal; ++i)
-    ctx[i * kMqThreads] = tbl[dev::mq_initial_state(i)];
-  const uint32_t *pcount = out.pass_count + (uint64_t)cc * kMaxPasses;
-  const uint64_t *poff = out.pass_off + (uint64_t)cc * kMaxPasses;
-  uint64_t *snaps = out.snaps + (uint64_t)cc * kMaxPasses * 2;
-  int64_t *dmse = out.dmse + (uint64_t)cc * kMaxPasses;
-  ByteOut bo{out.bytes + cb.out_off, cb.out_cap, 0u};
-  Mq e{0x8000u, 0u, 0u, 12, -1};
-  auto snapshot = [&](int p) {
-    snaps[2 * p] = ((uint64_t)e.A << 48) | ((uint64_t)(e.T & 0xFF) << 40) |
-                   ((uint64_t)(uint8_t)e.t << 32) | (uint64_t)(uint32_t)e.C;
-    snaps[2 * p + 1] = (uint64_t)(int64_t)e.L;
-  };
-  if (!live) return;
-  // Each lane codes its codeblock on its own: passes in order, the state snapshot at the end of
-  // each.  A pass's symbols are read a 32-bit word (four symbols) at a time, two words ahead.
-  // Per symbol (mq_bit_encode, mq.c:478-556): the common case -- the more probable symbol with
-  // the interval staying >= 0x8000 -- is a subtraction and an addition; otherwise the context
-  // moves to its next state, the interval renormalises (a plain shift unless a byte falls due
-  // on the way, mq.c:85-127 then) and the coder state advances.  The next symbol's context
-  // entry is read while the current symbol is coded; a context the current symbol just changed
-  // overrides it.
-  auto code = [&](uint32_t sym, uint32_t ent, uint32_t nk, uint32_t &nent) {
-    const uint32_t pq = ent & 0xFFFF;
-    const uint32_t A1 = e.A - pq;
-    const bool is_mps = ((sym ^ (ent >> 16)) & 1) == 0;
-    if (is_mps && A1 >= 0x8000u) {
-      e.A = A1;
-      e.C += pq;
-      return;
-    }
-    const bool small = A1 < pq;
-    e.C += (is_mps != small) ? pq : 0u;
-    e.A = (is_mps == small) ? pq : A1;
-    const uint32_t k = sym >> 1;
-    const uint32_t ne = tbl[is_mps ? (ent >> 17) & 0x7F : (ent >> 24) & 0x7F];
-    ctx[k * kMqThreads] = ne;
-    if (nk == k) nent = ne;
-    int sh = __clz(e.A) - 16;   // shifts until A >= 0x8000 (at least one)
-    if (sh < e.t) {
-      e.A <<= sh;
-      e.C <<= sh;
-      e.t -= sh;
-      return;
-    }
-    do {   // shift up to each due transfer, transfer, continue
-      const int s1 = min(sh, e.t);
-      e.A <<= s1;
-      e.C <<= s1;
-      e.t -= s1;
-      sh -= s1;
-      if (e.t == 0) mq_transfer(e, bo);
-    } while (sh > 0);
-  };
-  for (int p = 0; p < Z; ++p) {
-    const uint32_t n = pcount[p];
-    if (n) {
-      // the pass's chunk holds at least (n + 3) / 4 words
-      const uint32_t *src = reinterpret_cast<const uint32_t *>(out.symbols + poff[p]);
-      const uint32_t nw = (n + 3) >> 2;
-      uint32_t w = src[0];
-      uint32_t wn = (nw > 1) ? src[1] : 0u;
-      uint32_t ent = ctx[((w & 0xFF) >> 1) * kMqThreads];
-      uint32_t left = n;
-      for (uint32_t q = 0; q < nw; ++q) {
-        const uint32_t wc = w;
-        w = wn;
-        wn = (q + 2 < nw) ? src[q + 2] : 0u;
-        const uint32_t cnt = min(left, 4u);
-        left -= cnt;
-#pragma unroll
-        for (int jj = 0; jj < 4; ++jj) {
-          if ((uint32_t)jj < cnt) {
-            const uint32_t sym = (wc >> (8 * jj)) & 0xFF;
-            const uint32_t nsym = (jj < 3) ? (wc >> (8 * (jj + 1))) & 0xFF : (w & 0xFF);
-            // past the pass's last symbol the next byte is padding: clamp its context index
-            const uint32_t nk = min(nsym >> 1, (uint32_t)dev::kCtxTotal - 1);
-            uint32_t nent = ctx[nk * kMqThreads];
-            code(sym, ent, nk, nent);
-            ent = nent;
-          }
-        }
-      }
-    }
-    snapshot(p);
-  }
-  mq_terminate(e, bo);
-  for (int i = 0; i < 16; ++i) {
-    const int64_t q = (int64_t)e.L + i;
-    if (q >= 0 && (uint64_t)q < bo.cap) bo.out[q] = 0;
-  }
-  // truncation lengths
-  uint32_t *Lout = out.L + (uint64_t)c * kMaxPasses;
-  uint32_t bad = 0;
-  for (int j = 0; j < Z; ++j) {
-    const uint64_t s0 = snaps[2 * j];
-    const int64_t Ls = (int64_t)snaps[2 * j + 1];
-    Lout[j] = (uint32_t)truncation_length((uint32_t)(s0 >> 48), (uint32_t)s0,
-                                          (int32_t)(int8_t)((s0 >> 32) & 0xFF),
-                                          (uint32_t)((s0 >> 40) & 0xFF), Ls, bo.out, bo.cap, &bad);
-  }
-  if (bad) bo.flags |= 4u;
-  // convex hull (scratch: slopes and hull stack overwrite the snapshots; dmse stays as it is,
-  // so the kernel can run again on the same symbol streams)
-  double *lambda = reinterpret_cast<double *>(snaps);
-  uint8_t *hull = reinterpret_cast<uint8_t *>(snaps + kMaxPasses + 1);
-  double scale0 = sb.gain_step2;
-  scale0 = dev::fmul(scale0, ldexp(1.0, 2 * K));
-  scale0 = dev::fdiv(scale0, 65536.0);
-  // distortion decrease of pass q in the reference's weighting: the weight is scale0 for the
-  // first plane and a quarter less per plane below (exact: powers of two, no subnormals);
-  // pass 0 codes plane K-1, passes 1-3 plane K-2, and so on
-  auto mse_of = [&](int q) -> double {
-    return dev::fmul(__ll2double_rn(dmse[q]), ldexp(scale0, -2 * ((q + 2) / 3)));
-  };
-  for (int i = 0; i <= Z; ++i) lambda[i] = 0.0;
-  for (int i = 0; i < Z; ++i) hull[i] = 0;
-  lambda[0] = 18446744073709551616.0;
-  int h = 0, hlast = 0;
-  for (int i = 0; i < Z; ++i) {
-    double dD = 0.0;
-    for (int q = hlast; q <= i; ++q) dD = dev::fadd(dD, mse_of(q));
-    uint64_t dL = (hlast > 0) ? (uint64_t)Lout[i] - Lout[hlast - 1] : (uint64_t)Lout[i];
-    if (dD > 0) {
-      while (dD >= dev::fmul(lambda[hlast], __ull2double_rn(dL))) {
-        lambda[hlast] = 0;
-        if (h == 0) {
-          // the reference would read below its hull stack here
-          bo.flags |= 2u;
-          break;
-        }
-        h--;
-        hlast = hull[h];
-        dD = 0.0;
-        for (int q = hlast; q <= i; ++q) dD = dev::fadd(dD, mse_of(q));
-        dL = (hlast > 0) ? (uint64_t)Lout[i] - Lout[hlast - 1] : (uint64_t)Lout[i];
-      }
-      h++;
-      hlast = i + 1;
-      hull[h] = (uint8_t)hlast;
-      if (dL == 0)
-        lambda[hlast] = (dD < 0) ? -1.0 : (dD == 0 ? 0.0 : 18446744073709551616.0);
-      else
-        lambda[hlast] = dev::fdiv(dD, __ull2double_rn(dL));
-    } else {
-      lambda[i + 1] = 0;
-    }
-  }
-  uint16_t *S = out.S + (uint64_t)c * (kMaxPasses + 1);
-  uint32_t smin = 0xFFFF, smax = 0;
-  for (int i = 0; i <= Z; ++i) {
-    uint16_t v;
-    if (lambda[i] < 0)
-      v = 1;
-    else if (lambda[i] == 0)
-      v = (i == Z) ? 1 : 0;
-    else
-      v = slope2log(lambda[i]);
-    S[i] = v;
-    if (v) {
-      smin = min(smin, (uint32_t)v);
-      smax = max(smax, (uint32_t)v);
-    }
-  }
-  if (Lout[Z - 1] > 0) {
+  const int Z = out.Z[c];
+  const uint64_t pbase = (uint64_t)c * kMaxPasses;
+  uint64_t *snaps = out.snaps + pbase * 2;
+  t1::MqState e{0x8000u, 0u, 0u, 12, -1};
+  t1::ByteSink bo{out.bytes + cb.out_off, cb.out_cap, 0u};
+  t1::mq_code_stream(e, bo, out.symbols + out.pass_off[pbase], out.pass_count + pbase, Z, tbl,
+                     &slots[0][threadIdx.x], kMqThreads, snaps);
+  uint32_t smin, smax;
+  t1::t1_finish(e, bo, K, Z, snaps, out.dmse + pbase, sb.gain_step2, out.L + pbase,
+                out.S + (uint64_t)c * (kMaxPasses + 1), &smin, &smax);
+  if (smax) {
     atomicMin(&out.slopes[2 * cb.slot], smin);
     atomicMax(&out.slopes[2 * cb.slot + 1], smax);
   }
@@ -979,8 +785,8 @@ __global__ void __launch_bounds__(kMqThreads) t1_mq_kernel(const CbDev *__restri
 
 }  // namespace
 
-// Per-thread symbol staging slice of the modelling kernel: 10 symbols for each of the thread's
-// columns plus 4 (a pass yields at most 10 per column -- cleanup in run mode: run, two
+// Per-thread symbol staging slice of the wide modelling kernel: 10 symbols for each of the
+// thread's columns plus 4 (a pass yields at most 10 per column -- cleanup in run mode: run, two
 // position, one sign, three samples of two -- and 4 segmentation symbols), kept while the
 // whole block's slices fit in 48 KB; 0 (count the symbols first, then write them) above that.
 uint32_t t1_model_stage_cap(uint32_t max_cols) {
@@ -989,8 +795,22 @@ uint32_t t1_model_stage_cap(uint32_t max_cols) {
   return ((size_t)cap * kModelThreads <= 48 * 1024) ? cap : 0u;
 }
 
-size_t t1_model_smem(uint32_t max_cols) {
+static size_t wide_smem(uint32_t max_cols) {
   return (size_t)max_cols * 3 + (size_t)kModelThreads * t1_model_stage_cap(max_cols);
+}
+
+// dynamic shared memory of the modelling kernel that runs for codeblocks of up to max_cols
+// stripe columns
+size_t t1_model_smem(uint32_t max_cols) {
+  if (max_cols <= t1::kModelMaxCols) return kModelSharedBytes + t1::kStageBytes;
+  return wide_smem(max_cols);
+}
+
+// scratch bytes of one codeblock of ncols stripe columns (bit planes of either modelling kernel)
+uint64_t t1_scratch_bytes(uint64_t ncols) {
+  const uint64_t wide = ncols * (2 + kPrecBit + 1);
+  const uint64_t narrow = t1::model_plane_bytes(ncols);
+  return ((wide > narrow ? wide : narrow) + 15) & ~15ull;
 }
 
 // Codeblocks per MQ warp, the rule used when the autotuner has no entry.  Each lane runs one
@@ -1057,19 +877,29 @@ void launch_t1_encode(const bwc_float *work, const CbDev *cbs, uint32_t ncb, con
                       const uint32_t *order, uint32_t *queue, cudaEvent_t after_model) {
   if (!ncb) return;
   const size_t smem = t1_model_smem(max_cols);
-  cudaFuncSetAttribute(t1_model_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const bool narrow = max_cols <= t1::kModelMaxCols;
+  if (narrow)
+    cudaFuncSetAttribute(t1_model_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  else
+    cudaFuncSetAttribute(t1_model_wide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   unsigned grid = ncb;
   if (queue) {
     // persistent: as many CTAs as fit on the GPU at once
     int dev = 0, sms = dev::kNumSMs, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, t1_model_kernel, kModelThreads, smem);
+    if (narrow)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, t1_model_kernel, t1::kModelBlock, smem);
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, t1_model_wide_kernel, kModelThreads, smem);
     grid = std::min<unsigned>(ncb, (unsigned)std::max(1, sms * std::max(1, per_sm)));
     cudaMemsetAsync(queue, 0, sizeof(uint32_t), s);
   }
-  t1_model_kernel<<<grid, kModelThreads, smem, s>>>(work, cbs, ncb, sbs, out, order, queue,
-                                                    t1_model_stage_cap(max_cols));
+  if (narrow)
+    t1_model_kernel<<<grid, t1::kModelBlock, smem, s>>>(work, cbs, ncb, sbs, out, order, queue);
+  else
+    t1_model_wide_kernel<<<grid, kModelThreads, smem, s>>>(work, cbs, ncb, sbs, out, order, queue,
+                                                           t1_model_stage_cap(max_cols));
   if (after_model) cudaEventRecord(after_model, s);
   const uint32_t rule = mq_lanes_per_warp(ncb);
   uint32_t lanes = rule;

@@ -30,6 +30,9 @@ CASES = [
     ("high_rate", (24, 24, 24), np.float64, "double", (2, 2, 2, 0), (3, 3, 3, 0), "32", {}),
     ("high_rate_single", (24, 24, 24), np.float32, "single", (2, 2, 2, 0), (3, 3, 3, 0), "16", {}),
     ("tiny", (3, 5, 7), np.float64, "double", (1, 1, 1, 0), (2, 2, 2, 0), "2", {}),
+    # 64 x 64 x 8 codeblocks (8192 stripe columns): the wide modelling kernel
+    ("wide_codeblocks", (32, 128, 128), np.float64, "double", (2, 2, 2, 0), (6, 6, 3, 0), "1,2", {}),
+    ("wide_codeblocks_single", (16, 128, 160), np.float32, "single", (1, 1, 1, 0), (6, 6, 3, 0), "4", {}),
 ]
 
 
