@@ -13,6 +13,7 @@
 #include <cstring>
 #include <vector>
 
+#include "../kernels/t1_dec.cuh"
 #include "../kernels/t1_model.cuh"
 #include "../kernels/t1_mq.cuh"
 
@@ -278,6 +279,45 @@ long long t1emu_encode(const bwc_float *work, const uint64_t *dims, const uint64
   }
   *flags = fl;
   return total;
+}
+
+// Tier-1 decoding of one codeblock with the decoder's kernel bodies on the host: Z passes of
+// `len` coded bytes into the zeroed working buffer `work` (dims x fastest), as bwc_decompress's
+// decode stage.  Codeblocks up to 4096 stripe columns.  Returns 0, or -1 on bad arguments.
+int t1emu_decode(bwc_float *work, const uint64_t *dims, const uint64_t *box, bwc_float qt_eff,
+                 int cls, int erres, int K, int Z, const uint8_t *bytes, uint32_t len) {
+  CbDev cb{};
+  cb.x0 = (uint32_t)box[0];
+  cb.y0 = (uint32_t)box[1];
+  cb.z0 = (uint32_t)box[2];
+  cb.t0 = (uint32_t)box[3];
+  cb.w = (uint32_t)(box[4] - box[0]);
+  cb.h = (uint32_t)(box[5] - box[1]);
+  cb.d = (uint32_t)(box[6] - box[2]);
+  cb.nt = (uint32_t)(box[7] - box[3]);
+  cb.base = 0;
+  cb.sy = dims[0];
+  cb.sz = dims[0] * dims[1];
+  cb.st = dims[0] * dims[1] * dims[2];
+  const uint32_t ncols = cb.w * ((cb.h + 3) / 4) * cb.d * cb.nt;
+  if (!ncols || ncols > kModelMaxCols) return -1;
+  const int ngroups = (int)((ncols + 15) / 16);
+  // the coded bytes, 16-byte aligned with zero padding after them
+  std::vector<uint8_t> hold((size_t)len + 96, 0);
+  uint8_t *data = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(hold.data()) + 15) & ~uintptr_t(15));
+  if (len) std::memcpy(data, bytes, len);
+  std::vector<u64> sig(ngroups), sgn(ngroups), pi(ngroups), del(ngroups), bits(ngroups);
+  std::vector<u64> planes((size_t)ngroups * (kPrecBit + 1), 0);
+  uint32_t slot[dev::kCtxTotal];
+  static DecTables tabs;
+  for (int i = 0; i < 256; ++i) dec_table_entry(tabs, i, &dev::h_sig2ctx[0][0], dev::h_sig2xi, dev::h_xi2cont);
+  const DecOut res = decode_seq(data, len, K, Z, erres != 0, cb.w, cb.h, ncols, cls, sig.data(),
+                                sgn.data(), pi.data(), del.data(), bits.data(), slot,
+                                dev::h_mq_states, tabs, planes.data());
+  for (int g = 0; g < ngroups; ++g)
+    dequant_group(g, ngroups, K, res, planes.data(), sgn[g], pi[g], cb, qt_eff, work, cb.w, cb.h,
+                  ncols);
+  return 0;
 }
 
 // 8x8 bit transpose as the kernels use it (for its unit test)

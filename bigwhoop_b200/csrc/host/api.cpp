@@ -370,8 +370,8 @@ static void build_tables(const Parameter &par, const FieldDims &dims, uchar erre
     } else {
       d.out_off = 0;   // filled by the caller
       d.out_cap = 0;
-      d.scratch_off = soff;   // elements of the magnitude scratch
-      soff += (uint64_t)ncols * 4;
+      d.scratch_off = soff;   // elements of the decode scratch
+      soff += t1_decode_scratch_elems(ncols);
     }
     cbs.push_back(d);
   }
@@ -814,7 +814,7 @@ static uchar decompress_impl(bwc_codec *codec, bwc_stream *stream) {
                         dv->Z.as<uint8_t>(), dv->lmax.as<uint32_t>(), c.error_resilience,
                         dv->mags.as<bwc_raw>(), dv->flags.as<uint32_t>(), state_cap,
                         big ? dv->scratch.as<uint16_t>() : nullptr, dv->counter.as<uint32_t>(),
-                        grid, s, dv->order.as<uint32_t>());
+                        grid, s, dv->order.as<uint32_t>(), mc);
     if (p == 0 && dv->ddump_set && dv->ddump.dequantized)
       cudaMemcpyAsync(dv->ddump.dequantized, dv->temp.p, n * sizeof(bwc_float), cudaMemcpyDeviceToHost, s);
     cudaEventRecord(b2, s);

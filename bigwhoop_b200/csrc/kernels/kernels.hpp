@@ -99,12 +99,16 @@ void launch_t1_encode(const bwc_float *work, const CbDev *cbs, uint32_t ncb, con
 
 // t1_decode.cu: decodes Z[c] passes of codeblock c from data + out_off (Lmax[c] bytes) and
 // writes the dequantised samples into the (zeroed) working buffer.
+// Codeblocks of up to 4096 stripe columns (max_cols) decode through the mask-based decoder,
+// larger ones through the column-state decoder (state_cap / gstate / grid apply to it only).
+// mags: decode scratch, t1_decode_scratch_elems(ncols) elements per codeblock at scratch_off.
 void launch_t1_decode_ex(bwc_float *work, const CbDev *cbs, uint32_t ncb,
                          const SbDev *sbs, const uint8_t *data, const uint8_t *K,
                          const uint8_t *Z, const uint32_t *Lmax, uchar erres, bwc_raw *mags,
                          uint32_t *flags, uint32_t state_cap, uint16_t *gstate,
                          uint32_t *work_counter, int grid, cudaStream_t s,
-                         const uint32_t *order = nullptr);
+                         const uint32_t *order, uint32_t max_cols);
+uint64_t t1_decode_scratch_elems(uint64_t ncols);
 
 // mlp.cu: the rate-control warm start's network (34 -> 64 -> 64 -> 1, FP32).
 constexpr int kMlpInputs = kRateFeatures;

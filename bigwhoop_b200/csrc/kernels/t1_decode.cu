@@ -4,11 +4,20 @@
 // decoder (mq.c:147-173, :846-1029), dequantisation cblkcopy_inverse (tier1.c:767-931).
 //
 // Decoding is inherently sequential inside a codeblock (every context depends on the bits just
-// decoded), so lane 0 walks the passes over the codeblock's column states held in shared memory
-// while the other lanes wait; the whole warp then reconstructs the samples in parallel:
-// value = (magnitude + 0.475 * 2^p) * step with p the first undecoded bit plane (one plane
-// lower for samples whose last pass was not reached), sign from the decoded sign bit.
+// decoded), so one lane walks the passes while the other lanes wait; the whole warp then
+// reconstructs the samples in parallel: value = (magnitude + 0.475 * 2^p) * step with p the
+// first undecoded bit plane (one plane lower for samples whose last pass was not reached), sign
+// from the decoded sign bit.
+//
+// t1_decode_kernel (codeblocks up to 4096 stripe columns): the decoder of t1_dec.cuh -- state as
+// 64-bit sample masks per 16 columns in shared memory, contexts from per-class tables, decoded
+// bits as one mask per plane and 16 columns in global memory, magnitudes rebuilt by bit
+// transposes.  t1_decode_wide_kernel (larger codeblocks): column states in shared memory and
+// magnitudes accumulated in global memory, one stripe column at a time.
+#include <algorithm>
+
 #include "device_common.cuh"
+#include "t1_dec.cuh"
 #include "t1_tables.cuh"
 
 namespace bwcb {
@@ -270,7 +279,7 @@ __device__ void dec_cu(MqDec &d, uint8_t *ctx, uint16_t *state, bwc_raw *mag, co
 }
 
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
-    t1_decode_kernel(bwc_float *__restrict__ work, const CbDev *__restrict__ cbs,
+    t1_decode_wide_kernel(bwc_float *__restrict__ work, const CbDev *__restrict__ cbs,
                      uint32_t ncb, const SbDev *__restrict__ sbs, const uint8_t *__restrict__ data,
                      const uint8_t *__restrict__ Kin, const uint8_t *__restrict__ Zin,
                      const uint32_t *__restrict__ Lmax, uint32_t erres, bwc_raw *mags,
@@ -384,19 +393,95 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
   }
 }
 
+// ---- codeblocks up to 4096 stripe columns ---------------------------------------------------
+
+constexpr int kDecWarps = 4;
+
+struct DecWarpShared {
+  t1::u64 sig[256], sgn[256], pi[256], del[256], bits[256];
+  uint32_t slot[dev::kCtxTotal + 1];
+};
+
+__global__ void __launch_bounds__(kDecWarps * 32)
+    t1_decode_kernel(bwc_float *__restrict__ work, const CbDev *__restrict__ cbs, uint32_t ncb,
+                     const SbDev *__restrict__ sbs, const uint8_t *__restrict__ data,
+                     const uint8_t *__restrict__ Kin, const uint8_t *__restrict__ Zin,
+                     const uint32_t *__restrict__ Lmax, uint32_t erres, bwc_raw *mags,
+                     uint32_t *flags, uint32_t *work_counter, const uint32_t *__restrict__ order) {
+  __shared__ t1::DecTables tabs;
+  __shared__ uint32_t tbl[94];
+  __shared__ DecWarpShared wsh[kDecWarps];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x)
+    t1::dec_table_entry(tabs, i, &dev::c_sig2ctx[0][0], dev::c_sig2xi, dev::c_xi2cont);
+  for (int i = threadIdx.x; i < 94; i += blockDim.x) tbl[i] = dev::c_mq_states[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  DecWarpShared &ws = wsh[wib];
+  for (;;) {
+    uint32_t c = 0;
+    if (lane == 0) c = atomicAdd(work_counter, 1u);
+    c = __shfl_sync(0xffffffffu, c, 0);
+    if (c >= ncb) break;
+    if (order) c = order[c];   // the queue position's codeblock (largest coded length first)
+    const CbDev cb = cbs[c];
+    const SbDev sb = sbs[cb.sb];
+    const uint32_t ncols = cb.w * ((cb.h + 3) >> 2) * cb.d * cb.nt;
+    if (ncols > t1::kModelMaxCols) {
+      if (lane == 0) flags[c] |= 4u;
+      continue;
+    }
+    const int ngroups = (int)((ncols + 15) >> 4);
+    const int K = Kin[c], Z = Zin[c];
+    t1::u64 *planes = reinterpret_cast<t1::u64 *>(mags + cb.scratch_off);
+    int r0 = 0, r1 = 0, r2 = K;
+    if (lane == 0) {
+      const t1::DecOut res =
+          t1::decode_seq(data + cb.out_off, Lmax[c], K, Z, erres != 0, cb.w, cb.h, ncols,
+                         (int)sb.cls, ws.sig, ws.sgn, ws.pi, ws.del, ws.bits, ws.slot, tbl, tabs,
+                         planes);
+      r0 = res.bitplane;
+      r1 = res.cpass;
+      r2 = res.pmin;
+    }
+    t1::DecOut res;
+    res.bitplane = __shfl_sync(0xffffffffu, r0, 0);
+    res.cpass = __shfl_sync(0xffffffffu, r1, 0);
+    res.pmin = __shfl_sync(0xffffffffu, r2, 0);
+    __syncwarp();
+    for (int g = lane; g < ngroups; g += 32)
+      t1::dequant_group(g, ngroups, K, res, planes, ws.sgn[g], ws.pi[g], cb, sb.qt_eff, work, cb.w,
+                        cb.h, ncols);
+    __syncwarp();
+  }
+}
+
 }  // namespace
+
+// decode scratch (elements of bwc_raw) of one codeblock of ncols stripe columns: its decoded
+// bit planes (one 64-bit mask per 16 columns and plane), or the wide kernel's magnitudes
+uint64_t t1_decode_scratch_elems(uint64_t ncols) { return ((ncols + 15) / 16) * 64; }
 
 void launch_t1_decode_ex(bwc_float *work, const CbDev *cbs, uint32_t ncb,
                          const SbDev *sbs, const uint8_t *data, const uint8_t *K,
                          const uint8_t *Z, const uint32_t *Lmax, uchar erres, bwc_raw *mags,
                          uint32_t *flags, uint32_t state_cap, uint16_t *gstate,
                          uint32_t *work_counter, int grid, cudaStream_t s,
-                         const uint32_t *order) {
+                         const uint32_t *order, uint32_t max_cols) {
+  if (max_cols <= t1::kModelMaxCols) {
+    int dev = 0, sms = dev::kNumSMs, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, t1_decode_kernel, kDecWarps * 32, 0);
+    const unsigned g = (unsigned)std::max(1, sms * std::max(1, per_sm));
+    t1_decode_kernel<<<g, kDecWarps * 32, 0, s>>>(work, cbs, ncb, sbs, data, K, Z, Lmax, erres,
+                                                 mags, flags, work_counter, order);
+    return;
+  }
   const size_t smem = 32 * kWarpsPerBlock + (size_t)state_cap * sizeof(uint16_t) * kWarpsPerBlock;
-  cudaFuncSetAttribute(t1_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  t1_decode_kernel<<<grid, kWarpsPerBlock * 32, smem, s>>>(work, cbs, ncb, sbs, data, K, Z,
-                                                            Lmax, erres, mags, flags, state_cap,
-                                                            gstate, work_counter, order);
+  cudaFuncSetAttribute(t1_decode_wide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  t1_decode_wide_kernel<<<grid, kWarpsPerBlock * 32, smem, s>>>(work, cbs, ncb, sbs, data, K, Z,
+                                                                Lmax, erres, mags, flags, state_cap,
+                                                                gstate, work_counter, order);
 }
 
 }  // namespace bwcb

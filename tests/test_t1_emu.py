@@ -161,3 +161,76 @@ def test_kernel_logic_matches_restatement(case, precision):
         box = (x0, y0, z0, t0, min(dims[0], x0 + 32), min(dims[1], y0 + 23), min(dims[2], z0 + 9), 1)
     qt = 1.0 / 8.0 if precision == "double" else 1.0 / 4.0
     _compare(L, rs, work, dims, list(box), qt, 0.37, hb, erres, precision)
+
+
+# ---- decoder -----------------------------------------------------------------------------------
+
+def emu_decode(L, work, dims, box, qt_eff, cls, erres, K, Z, data):
+    L.t1emu_decode.restype = C.c_int
+    fl = C.c_double if work.dtype == np.float64 else C.c_float
+    L.t1emu_decode.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, fl, C.c_int, C.c_int, C.c_int,
+                               C.c_int, C.c_char_p, C.c_uint32]
+    d = np.asarray(dims, np.uint64)
+    b = np.asarray(box, np.uint64)
+    rc = L.t1emu_decode(work.ctypes.data, d.ctypes.data, b.ctypes.data, qt_eff, cls, int(erres),
+                        int(K), int(Z), bytes(data), len(data))
+    assert rc == 0
+
+
+@pytest.mark.parametrize("name", sorted(INDEX))
+def test_decoder_logic_matches_golden(name):
+    """Every codeblock of the golden codestream decoded by the decoder's kernel bodies gives the
+    reference's dequantised field (its hash is stored in the fixture)."""
+    import hashlib
+    meta = INDEX[name]
+    g = dict(np.load(os.path.join(GOLDEN, name + ".npz")))
+    precision = meta["precision"]
+    rs = restated(precision)
+    L = emu(precision)
+    f = g["field"]
+    dims = rs.dims_of(f.shape)
+    work = np.zeros(f.size, np.float64 if precision == "double" else np.float32)
+    for c in range(meta["codeblocks_n"]):
+        K, Z = int(g["dK"][c]), int(g["dZ"][c])
+        if Z == 0:
+            continue
+        geo = g["geom"][c]
+        cls = rs.load(precision).rs_context_class(int(geo[8]))
+        lo = int(g["cb_offsets"][c])
+        n = int(g["L"][c][Z - 1])
+        emu_decode(L, work, dims, [int(v) for v in geo[:8]], g["subband"][c][0], cls,
+                   meta["erres"], K, Z, g["cb_data"][lo:lo + n])
+    assert hashlib.sha256(work.tobytes()).hexdigest() == meta["dequantized_sha"]
+
+
+@pytest.mark.parametrize("precision", ["double", "single"])
+@pytest.mark.parametrize("case", CASES, ids=[str(i) for i in range(len(CASES))])
+def test_decoder_logic_matches_restatement_at_every_truncation(case, precision):
+    """Codeblocks truncated after every kind of pass (significance, refinement, cleanup), as the
+    quality layers cut them, decode like the restated decoder."""
+    rs = restated(precision)
+    L = emu(precision)
+    from bigwhoop_b200 import fields
+    shape, box, hb, erres = case
+    f = fields.shock_field(shape, 78)
+    dims = rs.dims_of(shape)
+    work, _ = rs.fill_normalize(f, 62 if precision == "double" else 30, precision)
+    rs.dwt_forward(work, dims, (1, 1, 1, 0), precision)
+    if len(box) == 4:
+        x0, y0, z0, t0 = box
+        box = (x0, y0, z0, t0, min(dims[0], x0 + 32), min(dims[1], y0 + 23), min(dims[2], z0 + 9), 1)
+    box = list(box)
+    qt = 1.0 if precision == "double" else 1.0 / 4.0
+    cls = rs.load(precision).rs_context_class(int(hb))
+    cb = rs.make_codeblock(box, qt, 0.37, hb, precision)
+    K, Z, Ls, _, data = rs.t1_encode(work, dims, cb, erres, precision)
+    assert Z > 6
+    dt = np.float64 if precision == "double" else np.float32
+    for z in sorted({1, 2, 3, 4, 5, Z // 3, Z // 2, Z - 2, Z - 1, Z}):
+        n = int(Ls[z - 1])
+        ours = np.zeros(int(np.prod(dims)), dt)
+        theirs = np.zeros_like(ours)
+        emu_decode(L, ours, dims, box, qt, cls, erres, K, z, data[:n])
+        rs.t1_decode(theirs, dims, cb, K, z, data[:n], erres, precision)
+        assert np.array_equal(ours.view(np.uint64 if dt == np.float64 else np.uint32),
+                              theirs.view(np.uint64 if dt == np.float64 else np.uint32)), z
