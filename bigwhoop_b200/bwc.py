@@ -264,7 +264,7 @@ class Compressor:
 
     def __init__(self, field=None, *, precision="double", rate="2", decomp=None, codeblocks=None,
                  precincts=None, qm=None, erres=False, n_par=None, device_ptr=None,
-                 out=None, tiles=None):
+                 out=None, tiles=None, kernels=None):
         self.L = load(precision)
         self.precision = precision
         if device_ptr is not None:
@@ -299,6 +299,8 @@ class Compressor:
             self.L.bwc_set_qm(self.codec, qm)
         if tiles is not None:   # tile sizes (x, y, z, t); bwc_compress codes one tile only
             self.L.bwc_set_tiles(self.codec, *[int(v) for v in tiles], 0)
+        if kernels is not None:   # wavelet per axis (x, y, z, t): 0 CDF 9/7, 1 LeGall 5/3
+            self.L.set_kernels(self.codec, *[int(v) for v in kernels])
         if out is None:
             # not zero-filled: compress() reads back only the bytes the library wrote
             self.out = np.empty(nbytes + (1 << 16), dtype=np.uint8)

@@ -308,6 +308,9 @@ static DwtPlan make_plan(const bwc_gl_ctrl &c, const Parameter &par) {
   DwtPlan plan{};
   plan.levels = c.nDecomp;
   const uint8_t dec[4] = {c.decompX, c.decompY, c.decompZ, c.decompTS};
+  const uint8_t kern[4] = {(uint8_t)c.KernelX, (uint8_t)c.KernelY, (uint8_t)c.KernelZ,
+                           (uint8_t)c.KernelTS};
+  for (int a = 0; a < 4; ++a) plan.kern[a] = (kern[a] == bwc_dwt_5_3) ? 1 : 0;
   for (int l = 0; l < c.nDecomp; ++l) {
     const Box &b = par.res[c.nDecomp - l].box;
     const uint64_t e[4] = {b.X1 - b.X0, b.Y1 - b.Y0, b.Z1 - b.Z0, b.TS1 - b.TS0};

@@ -179,6 +179,17 @@ static bwc_codec *alloc_codec() {
   return codec;
 }
 
+namespace bwcb {
+bool unsupported_kernel(const bwc_gl_ctrl &c, const bwc_gl_inf &info) {
+  const int kern[4] = {(int)c.KernelX, (int)c.KernelY, (int)c.KernelZ, (int)c.KernelTS};
+  const uint8_t dec[4] = {c.decompX, c.decompY, c.decompZ, c.decompTS};
+  const uint64_t n[4] = {info.nX, info.nY, info.nZ, info.nTS};
+  for (int a = 0; a < 4; ++a)
+    if (dec[a] > 0 && n[a] > 1 && kern[a] != bwc_dwt_9_7 && kern[a] != bwc_dwt_5_3) return true;
+  return false;
+}
+}  // namespace bwcb
+
 extern "C" bwc_stream *bwc_init_stream(void *const inpbuf, void *const outbuf, bwc_mode const mode) {
   bwc_stream *s = (bwc_stream *)calloc(1, sizeof(bwc_stream));
   if (!s) {
@@ -871,10 +882,10 @@ static uchar bwc_create_compression_body(bwc_codec *const codec, bwc_stream *con
   // more than one tile: the geometry, rate control and codestream layout are built (and tested
   // against the reference through bwc_b200_assemble_tiles_from_tier1); bwc_compress and
   // bwc_b200_compress_batch refuse such codecs, the device path codes a single tile
-  if (c->KernelX != bwc_dwt_9_7 || c->KernelY != bwc_dwt_9_7 || c->KernelZ != bwc_dwt_9_7 ||
-      (c->KernelTS != bwc_dwt_9_7 && c->decompTS > 0 && info->nTS > 1)) {
+  if (unsupported_kernel(*c, *info)) {
     warn("o##########################################################o\n"
-         "| ERROR: this library implements the CDF 9/7 wavelet only  |\n"
+         "| ERROR: this library implements the CDF 9/7 and LeGall    |\n"
+         "|        5/3 wavelets only                                 |\n"
          "o##########################################################o\n");
     return 1;
   }

@@ -291,10 +291,10 @@ uchar parse_main_header(bwc_codec *codec, bwc_stream *data, BitReader &br) {
         }
         // more than one tile: parsed here (tested against the reference's parser);
         // bwc_decompress refuses such codecs, the device path decodes a single tile
-        if (c.KernelX != bwc_dwt_9_7 || c.KernelY != bwc_dwt_9_7 || c.KernelZ != bwc_dwt_9_7 ||
-            (c.KernelTS != bwc_dwt_9_7 && c.decompTS > 0 && info.nTS > 1)) {
+        if (unsupported_kernel(c, info)) {
           warn("o##########################################################o\n"
-               "| ERROR: this library implements the CDF 9/7 wavelet only  |\n"
+               "| ERROR: this library implements the CDF 9/7 and LeGall    |\n"
+               "|        5/3 wavelets only                                 |\n"
                "o##########################################################o\n");
           return 1;
         }

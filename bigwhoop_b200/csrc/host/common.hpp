@@ -289,4 +289,9 @@ R guarded(R on_error, F &&body) noexcept {
   return on_error;
 }
 
+// true when an axis that the transform decomposes (levels > 0, more than one sample) uses a
+// wavelet kernel this library does not implement: Haar (the reference has no boundary extension
+// for it, dwt.c:1259-1262, so it cannot transform such a field) or a value outside the enum
+bool unsupported_kernel(const bwc_gl_ctrl &c, const bwc_gl_inf &info);
+
 }  // namespace bwcb

@@ -1,6 +1,12 @@
-// Multi-level separable CDF 9/7 lifting transform, forward and inverse
-// (dwt.c:354-466 lifting, :286-342 boundary extension, :645-789 de-/interleave,
-// :1216-2246 level/axis drivers).
+// Multi-level separable CDF 9/7 and LeGall 5/3 lifting transforms, forward and inverse
+// (dwt.c:354-466 9/7 lifting, :478-558 5/3 lifting, :286-342 boundary extension, :645-789
+// de-/interleave, :1216-2246 level/axis drivers).
+//
+// Fields whose every transformed axis uses the 9/7 kernel take the fused paths below.  A field
+// with a 5/3 axis is transformed axis by axis in place (dwt_axis_kernel): each block holds whole
+// lines in shared memory with an 8-sample reflected extension on both sides and lifts them over
+// the extended range exactly as the reference lifts its extended line buffers, for either
+// kernel.
 //
 // Each level's spatial axes are transformed by one fused pass, reading one field-sized buffer
 // and writing the other: the z-streaming kernel (dwt_stream_fwd_kernel) for large forward 3D
@@ -618,6 +624,108 @@ __global__ void __launch_bounds__(kZThreads, 1)
   }
 }
 
+// ---- one axis in place, any kernel ---------------------------------------------------------
+constexpr int kExt = 8;   // reflected samples on each side of a line (the liftings read at most 6)
+// LeGall 5/3 lifting constants of the reference (dwt.c:478-558): halving and (sum + 2) / 4
+constexpr bwc_float kTwo = (bwc_float)2, kFour = (bwc_float)4;
+
+// Lines of length `len` along an axis of element stride `sa` (the region's extent on that axis),
+// TX of them side by side along the companion axis (extent ec, stride sc); blockIdx enumerates
+// x tiles, then the two remaining axes (extent e1 with stride s1, then stride s2).  Forward: load
+// the line, extend, lift, store lows first (a line starting at an odd coordinate, `odd`, lifts
+// one sample further into the extension and takes its lows from w[0], w[2], ... and highs from
+// w[-1], w[1], ...).  Inverse: load interleaved, extend, lift, store in natural order.
+template <bool kFwd>
+__global__ void __launch_bounds__(256) dwt_axis_kernel(bwc_float *__restrict__ work, int len,
+                                                       int odd, int kern, uint64_t sa, int TX,
+                                                       uint32_t ec, uint64_t sc, uint32_t e1,
+                                                       uint64_t s1, uint64_t s2, uint32_t ntx) {
+  extern __shared__ unsigned char smem_raw[];
+  bwc_float *sm = reinterpret_cast<bwc_float *>(smem_raw);
+  const int rows = len + 2 * kExt + 2;   // line positions -kExt-1 .. len+kExt
+  const uint32_t tile = blockIdx.x % ntx;
+  const uint64_t rest = blockIdx.x / ntx;
+  const uint64_t i1 = rest % e1, i2 = rest / e1;
+  const uint32_t c0 = tile * (uint32_t)TX;
+  const int tw = (int)((ec - c0) < (uint32_t)TX ? (ec - c0) : (uint32_t)TX);
+  bwc_float *base = work + (uint64_t)c0 * sc + i1 * s1 + i2 * s2;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  // B[q] of line x at sm[(q + kExt + 1) * TX + x]; the lifting's w = B + odd
+  auto B = [&](int q, int x) -> bwc_float & { return sm[(q + kExt + 1) * TX + x]; };
+  const int half = kFwd ? (odd ? (len >> 1) : ((len + 1) >> 1)) : ((len + 1) >> 1);
+  for (int q = tid; q < len * TX; q += nth) {
+    const int i = q / TX, x = q - i * TX;
+    if (x >= tw) continue;
+    const bwc_float v = base[(uint64_t)x * sc + (uint64_t)i * sa];
+    if (kFwd) {
+      B(i, x) = v;
+    } else {
+      // coefficient i of the stored line is interleaved back to position j
+      const int j = (i < half) ? 2 * i : 2 * (i - half) + 1;
+      B(j, x) = v;
+    }
+  }
+  __syncthreads();
+  // whole-point symmetric extension, reflected as often as needed (dwt.c:286-342)
+  for (int q = tid; q < 2 * kExt * TX; q += nth) {
+    const int k = q / TX, x = q - k * TX;
+    if (x >= tw) continue;
+    const int e = (k < kExt) ? -(k + 1) : len - 1 + (k - kExt + 1);
+    int j = e;
+    while (j < 0 || j > len - 1) j = (j < 0) ? -j : 2 * (len - 1) - j;
+    B(e, x) = B(j, x);
+  }
+  __syncthreads();
+  // one lifting step over w[i], i = i0, i0 + 2, ... < i1
+  auto step = [&](int i0, int i1e, auto fn) {
+    const int cnt = (i1e - i0 + 1) / 2;
+    for (int q = tid; q < cnt * TX; q += nth) {
+      const int k = q / TX, x = q - k * TX;
+      if (x >= tw) continue;
+      const int i = i0 + 2 * k + odd;
+      B(i, x) = fn(B(i, x), B(i - 1, x), B(i + 1, x));
+    }
+    __syncthreads();
+  };
+  using dev::fadd;
+  using dev::fdiv;
+  using dev::fmul;
+  using dev::fsub;
+  if (kern == 1) {
+    if (kFwd) {
+      step(-1, len + 1, [](bwc_float v, bwc_float a, bwc_float b) { return fsub(v, fdiv(fadd(a, b), kTwo)); });
+      step(0, len, [](bwc_float v, bwc_float a, bwc_float b) { return fadd(v, fdiv(fadd(fadd(a, b), kTwo), kFour)); });
+    } else {
+      step(-2, len + 1, [](bwc_float v, bwc_float a, bwc_float b) { return fsub(v, fdiv(fadd(fadd(a, b), kTwo), kFour)); });
+      step(-1, len, [](bwc_float v, bwc_float a, bwc_float b) { return fadd(v, fdiv(fadd(a, b), kTwo)); });
+    }
+  } else {
+    if (kFwd) {
+      step(-3, len + 3, [](bwc_float v, bwc_float a, bwc_float b) { return fadd(v, fmul(kAlpha, fadd(a, b))); });
+      step(-2, len + 2, [](bwc_float v, bwc_float a, bwc_float b) { return fadd(v, fmul(kBeta, fadd(a, b))); });
+      step(-1, len + 1, [](bwc_float v, bwc_float a, bwc_float b) { return fmul(kKappaH, fadd(v, fmul(kGamma, fadd(a, b)))); });
+      step(0, len, [](bwc_float v, bwc_float a, bwc_float b) { return fmul(kKappaL, fadd(v, fmul(kDelta, fadd(a, b)))); });
+    } else {
+      step(-4, len + 4, [](bwc_float v, bwc_float a, bwc_float b) { return fsub(fmul(kKappaH, v), fmul(kDelta, fadd(a, b))); });
+      step(-5, len + 3, [](bwc_float v, bwc_float a, bwc_float b) { return fsub(fmul(kKappaL, v), fmul(kGamma, fadd(a, b))); });
+      step(-4, len + 2, [](bwc_float v, bwc_float a, bwc_float b) { return fsub(v, fmul(kBeta, fadd(a, b))); });
+      step(-3, len + 1, [](bwc_float v, bwc_float a, bwc_float b) { return fsub(v, fmul(kAlpha, fadd(a, b))); });
+    }
+  }
+  for (int q = tid; q < len * TX; q += nth) {
+    const int i = q / TX, x = q - i * TX;
+    if (x >= tw) continue;
+    bwc_float v;
+    if (kFwd) {
+      // lows first: w[0], w[2], ...; then the highs
+      v = (i < half) ? B(2 * i + odd, x) : B(2 * (i - half) + (odd ? -1 : 1) + odd, x);
+    } else {
+      v = B(i, x);
+    }
+    base[(uint64_t)x * sc + (uint64_t)i * sa] = v;
+  }
+}
+
 // dst = src over the box [0, e0) x [0, e1) x [0, e2) x [0, e3) of the buffer
 __global__ void __launch_bounds__(256) copy_region_kernel(const bwc_float *__restrict__ src,
                                                           bwc_float *__restrict__ dst,
@@ -713,6 +821,37 @@ void level_pass(const bwc_float *src, bwc_float *dst, const FieldDims &d, const 
   k<<<(unsigned)blocks, kFusedThreads, smem, s>>>(src, dst, g);
 }
 
+// one axis of a level's region in place with dwt_axis_kernel
+template <bool kFwd>
+void axis_pass(bwc_float *work, const FieldDims &d, const uint64_t *e, int a, int kern, int odd,
+               cudaStream_t s) {
+  const int len = (int)e[a];
+  if (len <= 1) return;
+  const uint64_t st[4] = {1, d.width, d.width * d.height, d.width * d.height * d.depth};
+  const int c = (a == 0) ? 1 : 0;
+  int o[2], k = 0;
+  for (int b = 0; b < 4; ++b)
+    if (b != a && b != c) o[k++] = b;
+  const size_t line_bytes = (size_t)(len + 2 * kExt + 2) * sizeof(bwc_float);
+  int TX = (int)std::min<size_t>(32, std::max<size_t>(1, (96 * 1024) / line_bytes));
+  TX = (int)std::min<uint64_t>((uint64_t)TX, std::max<uint64_t>(1, e[c]));
+  const uint32_t ntx = (uint32_t)((e[c] + TX - 1) / TX);
+  const uint64_t blocks = (uint64_t)ntx * e[o[0]] * e[o[1]];
+  if (!blocks) return;
+  const size_t smem = line_bytes * TX;
+  auto kf = dwt_axis_kernel<kFwd>;
+  cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kf<<<(unsigned)blocks, 256, smem, s>>>(work, len, odd, kern, st[a], TX, (uint32_t)e[c], st[c],
+                                         (uint32_t)e[o[0]], st[o[0]], st[o[1]], ntx);
+}
+
+bool uses_axis_path(const DwtPlan &plan) {
+  for (int l = 0; l < plan.levels; ++l)
+    for (int a = 0; a < 4; ++a)
+      if ((plan.axis_on[l] >> a & 1) && plan.kern[a] != 0) return true;
+  return false;
+}
+
 }  // namespace
 
 // Forward: `temp` holds the normalised field on entry; the coefficients end in `work`.  Even
@@ -725,6 +864,14 @@ void launch_dwt_forward(bwc_float *work, bwc_float *temp, const FieldDims &dims,
   const uint64_t full[4] = {dims.width, dims.height, dims.depth, dims.dt};
   if (plan.levels == 0) {
     copy_region(temp, work, dims, full, s);
+    return;
+  }
+  if (uses_axis_path(plan)) {
+    // axis by axis in place (x, y, z, t per level), each with its own kernel
+    copy_region(temp, work, dims, full, s);
+    for (int l = 0; l < plan.levels; ++l)
+      for (int a = 0; a < 4; ++a)
+        if (plan.axis_on[l] >> a & 1) axis_pass<true>(work, dims, plan.ext[l], a, plan.kern[a], 0, s);
     return;
   }
   for (int l = 0; l < plan.levels; ++l) {
@@ -747,6 +894,14 @@ void launch_dwt_inverse(bwc_float *work, bwc_float *temp, const FieldDims &dims,
                         const DwtPlan &plan, cudaStream_t s) {
   const uint64_t full[4] = {dims.width, dims.height, dims.depth, dims.dt};
   if (plan.levels == 0) {
+    copy_region(temp, work, dims, full, s);
+    return;
+  }
+  if (uses_axis_path(plan)) {
+    // axis by axis in place (t, z, y, x per level, coarsest level first), then to `work`
+    for (int l = plan.levels - 1; l >= 0; --l)
+      for (int a = 3; a >= 0; --a)
+        if (plan.axis_on[l] >> a & 1) axis_pass<false>(temp, dims, plan.ext[l], a, plan.kern[a], 0, s);
     copy_region(temp, work, dims, full, s);
     return;
   }

@@ -67,13 +67,15 @@ void launch_normalize(bwc_float *work, uint64_t n, const uint64_t *minmax_keys, 
 void launch_denormalize(const bwc_float *work, uint64_t n, bwc_float pmin, bwc_float pmax,
                         uint8_t Qm, void *dst, bool dst_double, cudaStream_t s);
 
-// dwt.cu: the multi-level separable 9/7 transform of one parameter.
+// dwt.cu: the multi-level separable transform (CDF 9/7 or LeGall 5/3 per axis) of one parameter.
 // level_ext[l] = extents (x, y, z, t) of the region transformed at level l; axis_on[l] bit a
 // set when axis a is transformed at level l.
+// kern[a]: the axis's wavelet kernel, 0 CDF 9/7, 1 LeGall 5/3.
 struct DwtPlan {
   int levels;
   uint64_t ext[16][4];
   uint8_t axis_on[16];
+  uint8_t kern[4];
 };
 // Forward: `temp` holds the normalised field on entry, the coefficients end in `work`;
 // inverse: `temp` holds the coefficients, the field ends in `work`.  `temp` is scratch after.

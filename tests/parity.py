@@ -63,14 +63,15 @@ def attach_stage_dump(comp: bwc.Compressor, ncb: int, max_passes: int) -> StageD
 
 
 def compare_stages(f, ref, *, precision="double", decomp=None, cb=None, rate="2", qm=None,
-                   erres=False, precincts=None):
+                   erres=False, precincts=None, kernels=None):
     """Compress ``f`` with both libraries, stage by stage.  Returns a dict of mismatch counts
     (all zero on parity) plus both codestreams."""
     mp = ref.MAX_PASSES[precision]
     ref.reset_gain_lut(precision)
     bwc.reset_gain_state(precision)
     rc = ref.RefCompressor(f, precision=precision, decomp=decomp, cb=cb, rate=rate,
-                           qm=-1 if qm is None else qm, erres=erres, precincts=precincts)
+                           qm=-1 if qm is None else qm, erres=erres, precincts=precincts,
+                           kernels=kernels)
     try:
         rc.normalize()
         a = rc.work()
@@ -84,7 +85,7 @@ def compare_stages(f, ref, *, precision="double", decomp=None, cb=None, rate="2"
     finally:
         rc.close()
     mc = bwc.Compressor(f, precision=precision, decomp=decomp, codeblocks=cb, rate=rate, qm=qm,
-                        erres=erres, precincts=precincts)
+                        erres=erres, precincts=precincts, kernels=kernels)
     try:
         assert mc.num_codeblocks() == ncb
         dump = attach_stage_dump(mc, ncb, mp)

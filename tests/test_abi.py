@@ -222,11 +222,11 @@ def test_create_decompression_rejects_truncated_codestream():
             C.CDLL(None).free(C.c_void_p(s))
 
 
-@pytest.mark.parametrize("case", ["kernel_5_3", "kernel_haar", "no_quantisation"])
-def test_create_compression_rejects_configurations_off_the_accelerated_path(case):
-    """The 5/3 and Haar kernels and bwc_qt_none are not on the accelerated path:
-    bwc_create_compression refuses them with return code 1 (the default configuration of the
-    same field is accepted)."""
+@pytest.mark.parametrize("case", ["kernel_haar", "no_quantisation", "kernel_5_3"])
+def test_create_compression_accepts_5_3_and_refuses_haar_and_no_quantisation(case):
+    """The LeGall 5/3 kernel is accepted; the Haar kernel and bwc_qt_none are refused by
+    bwc_create_compression with return code 1 (the default configuration of the same field is
+    accepted)."""
     f = np.zeros((16, 16, 16))
     out = np.zeros(1 << 16, np.uint8)
     L = C.CDLL(bwc.lib_path("double"))
@@ -252,18 +252,20 @@ def test_create_compression_rejects_configurations_off_the_accelerated_path(case
                 else:
                     L.set_quant_style(c, 0)
             rc = L.bwc_create_compression(c, s, C.create_string_buffer(b"2"))
-            assert rc == (1 if configure else 0), (case, configure)
+            refused = configure and case != "kernel_5_3"
+            assert rc == (1 if refused else 0), (case, configure)
         finally:
             L.bwc_free_codec(c)
             C.CDLL(None).free(C.c_void_p(s))
 
 
-@pytest.mark.parametrize("case", ["default", "kernel_5_3"])
-def test_create_decompression_rejects_codestreams_off_the_accelerated_path(case):
-    """A reference codestream made with the 5/3 kernel is refused by bwc_create_decompression
-    (return code 1) instead of being decoded as 9/7.  The reference's own bwc_compress crashes
-    (segmentation fault, some runs) with the Haar kernel or without quantisation on this input,
-    so no such codestream is made here; the header checks for them are the same."""
+@pytest.mark.parametrize("case", ["default", "kernel_5_3", "kernel_haar_in_header"])
+def test_create_decompression_checks_the_wavelet_of_the_codestream(case):
+    """Reference codestreams made with the 9/7 and the 5/3 kernel are accepted by
+    bwc_create_decompression; one whose header names the Haar kernel is refused (return code
+    1).  The reference's own bwc_compress crashes (segmentation fault, some runs) with the Haar
+    kernel or without quantisation on this input, so the Haar header is made by rewriting the
+    kernel byte of the 5/3 codestream's SGC marker."""
     need_ref("double")
     from oracle import ref
     from bigwhoop_b200 import fields
@@ -283,7 +285,7 @@ def test_create_decompression_rejects_codestreams_off_the_accelerated_path(case)
     c = R.bwc_alloc_coder(16, 16, 16, 1, 1, 8)
     s = R.bwc_init_stream(f.ctypes.data, out.ctypes.data, bwc.COMP)
     try:
-        if case == "kernel_5_3":
+        if case != "default":
             R.set_kernels(c, 1, 1, 1, 1)
         assert R.bwc_create_compression(c, s, C.create_string_buffer(b"4")) == 0
         n = R.bwc_compress(c, s)
@@ -293,6 +295,12 @@ def test_create_decompression_rejects_codestreams_off_the_accelerated_path(case)
         C.CDLL(None).free(C.c_void_p(s))
     cs = np.zeros(n + 64, np.uint8)
     cs[:n] = out[:n]
+    if case == "kernel_haar_in_header":
+        # the kernel byte (x << 6 | y << 4 | z << 2 | t) of the SGC marker: 5/3 everywhere is
+        # 0x55; Haar everywhere is 0xAA
+        pos = bytes(cs[:256]).find(b"\x55")
+        assert pos > 0
+        cs[pos] = 0xAA
     L = _lib()
     rec = np.zeros(f.size, np.float64)
     d = L.bwc_alloc_decoder()
@@ -302,7 +310,7 @@ def test_create_decompression_rejects_codestreams_off_the_accelerated_path(case)
     finally:
         L.bwc_free_codec(d)
         C.CDLL(None).free(C.c_void_p(st))
-    assert rc == (0 if case == "default" else 1), case
+    assert rc == (1 if case == "kernel_haar_in_header" else 0), case
 
 
 def test_compress_refuses_multi_tile_fields(capfd):

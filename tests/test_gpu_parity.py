@@ -49,6 +49,32 @@ def test_stage_and_codestream_parity(gpu, case):
     assert n_bit_diffs(out, out_ref) == 0
 
 
+KERNEL_CASES = [
+    # id, shape, precision, decomp, codeblocks, rate, kernels (x, y, z, t): 0 CDF 9/7, 1 LeGall 5/3
+    ("legall_3d", (40, 36, 44), "double", (3, 3, 3, 0), (4, 4, 4, 0), "1,4", (1, 1, 1, 1)),
+    ("legall_mixed", (33, 47, 61), "double", (2, 3, 2, 0), (5, 5, 4, 0), "0.5,2", (1, 0, 1, 1)),
+    ("legall_single", (24, 40, 32), "single", (2, 2, 2, 0), (4, 4, 4, 0), "2,8", (0, 1, 1, 1)),
+    ("legall_4d", (6, 20, 16, 24), "double", (2, 2, 2, 1), (3, 3, 3, 1), "1,4", (1, 1, 1, 1)),
+    ("legall_line", (1, 1, 300), "double", (4, 0, 0, 0), (6, 0, 0, 0), "2", (1, 1, 1, 1)),
+]
+
+
+@pytest.mark.parametrize("case", KERNEL_CASES, ids=[c[0] for c in KERNEL_CASES])
+def test_legall_5_3_parity(gpu, case):
+    """The LeGall 5/3 kernel, alone and mixed with 9/7 per axis: stage by stage, codestream and
+    decompression against the reference."""
+    _, shape, precision, decomp, cb, rate, kernels = case
+    ref = need_ref(precision)
+    dt = np.float64 if precision == "double" else np.float32
+    f = fields.spectral_field(shape, 15).astype(dt)
+    rep, cs, cs_ref = compare_stages(f, ref, precision=precision, decomp=decomp, cb=cb, rate=rate,
+                                     kernels=kernels)
+    assert rep == dict(normalized=0, transformed=0, codeblocks=0, flags=0, codestream=0), rep
+    out = bwc.decompress_array(cs, precision)
+    out_ref = ref.decompress(cs_ref, f.shape, f.dtype, precision)
+    assert n_bit_diffs(out, out_ref) == 0
+
+
 def test_many_precincts(gpu):
     """16^3 precincts over 8^3 codeblocks: many packets per resolution, stage by stage and the
     decompressed field."""
