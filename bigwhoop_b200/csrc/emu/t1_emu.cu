@@ -227,7 +227,7 @@ long long t1emu_encode(const bwc_float *work, const uint64_t *dims, const uint64
   std::vector<uint8_t> planes(model_plane_bytes(ncols) + 64, 0);
   const uint64_t arena_cap = stream_bound(ncols, kPrecBit + 1);
   std::vector<uint8_t> arena(arena_cap + 256, 0);
-  unsigned long long used = 0;
+  unsigned long long used[2] = {0, 0};   // arena bytes reserved, decisions coded
   std::vector<uint64_t> snaps(2 * kMaxPasses + 16, 0);
   std::vector<int64_t> dm(kMaxPasses, 0);
   std::vector<uint32_t> pc(kMaxPasses, 0);
@@ -247,7 +247,7 @@ long long t1emu_encode(const bwc_float *work, const uint64_t *dims, const uint64
   o.dmse = dm.data();
   o.symbols = arena.data();
   o.sym_cap = arena_cap;
-  o.sym_used = &used;
+  o.sym_used = used;
   o.pass_count = pc.data();
   o.pass_off = po.data();
 

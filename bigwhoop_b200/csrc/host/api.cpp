@@ -512,7 +512,7 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
     total_samples += (uint64_t)allcb[i].w * ((allcb[i].h + 3) / 4) * 4 * allcb[i].d * allcb[i].nt;
   uint64_t arena = std::max<uint64_t>(1 << 20, total_samples * (kPrecBit + 1) * 9 / 8);
   if (!dv->pcount.ensure(ncb * kMaxPasses * 4) || !dv->poff.ensure(ncb * kMaxPasses * 8) ||
-      !dv->symused.ensure(8) || !dv->order.ensure(ncb * 4) || !dv->queue.ensure(4))
+      !dv->symused.ensure(16) || !dv->order.ensure(ncb * 4) || !dv->queue.ensure(4))
     return 0;
   {
     std::vector<uint32_t> order;
@@ -558,17 +558,18 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
       if (!dv->symbols.ensure(arena + 256)) return 0;
       o.symbols = dv->symbols.as<uint8_t>();
       o.sym_cap = dv->symbols.cap - 256;   // slack for the MQ kernel's read-ahead
-      cudaMemsetAsync(dv->symused.p, 0, 8, s);
+      cudaMemsetAsync(dv->symused.p, 0, 16, s);
       cudaMemsetAsync(o.flags, 0, cbs[p].size() * 4, s);
       launch_t1_encode(dv->work.as<bwc_float>(), dv->cbtab.as<CbDev>() + cb_base[p],
                        (uint32_t)cbs[p].size(), dv->sbtab.as<SbDev>(), o, max_cols, s,
                        dv->order.as<uint32_t>() + cb_base[p], dv->queue.as<uint32_t>(), m2);
-      unsigned long long used = 0;
-      cudaMemcpyAsync(&used, dv->symused.p, 8, cudaMemcpyDeviceToHost, s);
+      unsigned long long cnt[2] = {0, 0};
+      cudaMemcpyAsync(cnt, dv->symused.p, 16, cudaMemcpyDeviceToHost, s);
       if (!cuda_ok(cudaStreamSynchronize(s), "tier-1 encoding")) return 0;
+      const unsigned long long used = cnt[0];
       if (p == 0) dv->timings[8] = 0;
       if (used <= o.sym_cap) {
-        dv->timings[8] += (double)used * 1e-6;
+        dv->timings[8] += (double)cnt[1] * 1e-6;
         break;
       }
       if (attempt >= 3) {
@@ -1023,7 +1024,7 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
       !bs->L.ensure(ncb * kMaxPasses * 4) || !bs->S.ensure(ncb * (kMaxPasses + 1) * 2) ||
       !bs->flags.ensure(ncb * 4) || !bs->slopes.ensure(8 * nf) ||
       !bs->pcount.ensure(ncb * kMaxPasses * 4) || !bs->poff.ensure(ncb * kMaxPasses * 8) ||
-      !bs->symused.ensure(8) || !bs->order.ensure(ncb * 4) || !bs->queue.ensure(4))
+      !bs->symused.ensure(16) || !bs->order.ensure(ncb * 4) || !bs->queue.ensure(4))
     return 1;
   const std::vector<uint32_t> order = work_order(allcb, allsb, 0, ncb);
   // Inputs in pageable host memory go through a page-locked staging area: several host threads
@@ -1192,7 +1193,7 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
     if (!bs->symbols.ensure(arena + 256)) return 1;
     o.symbols = bs->symbols.as<uint8_t>();
     o.sym_cap = bs->symbols.cap - 256;
-    cudaMemsetAsync(bs->symused.p, 0, 8, s);
+    cudaMemsetAsync(bs->symused.p, 0, 16, s);
     cudaMemsetAsync(bs->flags.p, 0, ncb * 4, s);
     launch_t1_encode(bs->work.as<bwc_float>(), bs->cbtab.as<CbDev>(), (uint32_t)ncb,
                      bs->sbtab.as<SbDev>(), o, max_cols, s, bs->order.as<uint32_t>(),

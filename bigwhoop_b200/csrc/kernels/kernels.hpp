@@ -50,7 +50,8 @@ struct T1EncOut {
   int64_t *dmse;         // scratch: [ncb * kMaxPasses] distortion decrease per pass
   uint8_t *symbols;      // scratch: symbol arena
   uint64_t sym_cap;      //   its capacity in bytes
-  unsigned long long *sym_used;   // bump counter (zeroed by the caller)
+  unsigned long long *sym_used;   // [0] bump counter of the arena (bytes reserved), [1] decisions
+                                  // coded (both zeroed by the caller)
   uint32_t *pass_count;  // scratch: [ncb * kMaxPasses] symbols per pass
   uint64_t *pass_off;    // scratch: [ncb * kMaxPasses] arena offset of each pass's symbols
 };

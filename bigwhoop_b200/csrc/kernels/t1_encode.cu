@@ -363,7 +363,7 @@ __device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ wo
   __shared__ uint32_t s_wsum[kModelThreads / 32];
   __shared__ int64_t s_wsum64[kModelThreads / 32];
   __shared__ uint32_t s_K, s_ok;
-  __shared__ uint64_t s_base, s_stream, s_pos;
+  __shared__ uint64_t s_base, s_stream, s_pos, s_decisions;
   const int tid = threadIdx.x;
   const CbDev cb = cbs[c];
   const SbDev sb = sbs[cb.sb];
@@ -448,6 +448,7 @@ __device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ wo
     s_ok = (base + need <= out.sym_cap) ? 1u : 0u;
     s_stream = base;
     s_pos = 0;
+    s_decisions = 0;
     if (!s_ok) out.flags[c] |= 8u;
   }
   __syncthreads();   // planes and column states are read across threads from here on
@@ -458,6 +459,7 @@ __device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ wo
     if (tid == 0) {
       s_base = s_stream + s_pos;
       s_pos += ((uint64_t)total + 15) & ~15ull;
+      s_decisions += total;
     }
     __syncthreads();
     return out.symbols + s_base;
@@ -632,6 +634,7 @@ __device__ __forceinline__ void model_codeblock(const bwc_float *__restrict__ wo
       pass++;
     }
   }
+  if (tid == 0) atomicAdd(out.sym_used + 1, (unsigned long long)s_decisions);
 }
 
 // Modelling of codeblocks over 4096 stripe columns.  Without a queue, CTA i models codeblock

@@ -341,6 +341,7 @@ T1_HD void model_codeblock(Blk &blk, ModelShared &sm, uint8_t *stage, const bwc_
   uint64_t *poff = out.pass_off + (uint64_t)c * kMaxPasses;
   int64_t *dmse = out.dmse + (uint64_t)c * kMaxPasses;
   int pass = 0;
+  unsigned long long decisions = 0;   // the codeblock's coded decisions (block-uniform)
 
   auto load_plane = [&](int b) -> u64 {
     if (b < 0 || t >= nthr) return 0ull;
@@ -381,6 +382,7 @@ T1_HD void model_codeblock(Blk &blk, ModelShared &sm, uint8_t *stage, const bwc_
       dmse[pass] = *ds;
     }
     pos += 16ull * n16;
+    decisions += total;
     ++pass;
   };
 
@@ -561,6 +563,7 @@ T1_HD void model_codeblock(Blk &blk, ModelShared &sm, uint8_t *stage, const bwc_
     for (int i = 0; i < 5; ++i) P[i] = P[i + 1];
     P[5] = load_plane(b - 7);
   }
+  if (t == 0) blk.reserve(out.sym_used + 1, decisions);
 }
 
 }  // namespace t1

@@ -41,8 +41,9 @@ constexpr uint64_t kOffSnaps = round256(kOffArena + kArenaBytes);
 constexpr uint64_t kOffDmse = round256(kOffSnaps + 16ull * kMaxPasses);
 constexpr uint64_t kOffPcount = round256(kOffDmse + 8ull * kMaxPasses);
 constexpr uint64_t kOffPoff = round256(kOffPcount + 4ull * kMaxPasses);
-constexpr uint64_t kOffUsed = round256(kOffPoff + 8ull * kMaxPasses);   // symbol bump counter
-constexpr uint64_t kOffSlopes = kOffUsed + 8;                            // slope min / max
+constexpr uint64_t kOffUsed = round256(kOffPoff + 8ull * kMaxPasses);   // arena bump counter,
+                                                                         // decisions coded
+constexpr uint64_t kOffSlopes = kOffUsed + 16;                           // slope min / max
 constexpr uint64_t kOffFlags = kOffSlopes + 8;                           // codeblock flags
 constexpr uint64_t kOffCb = round256(kOffFlags + 4);
 constexpr uint64_t kOffSb = round256(kOffCb + sizeof(CbDev));
@@ -78,7 +79,8 @@ unsigned char *static_area(int device) {
 __global__ void static_setup_kernel(unsigned char *base, CbDev cb, SbDev sb) {
   *reinterpret_cast<CbDev *>(base + kOffCb) = cb;
   *reinterpret_cast<SbDev *>(base + kOffSb) = sb;
-  *reinterpret_cast<unsigned long long *>(base + kOffUsed) = 0ull;
+  reinterpret_cast<unsigned long long *>(base + kOffUsed)[0] = 0ull;
+  reinterpret_cast<unsigned long long *>(base + kOffUsed)[1] = 0ull;
   uint32_t *slopes = reinterpret_cast<uint32_t *>(base + kOffSlopes);
   slopes[0] = 0xFFFF;
   slopes[1] = 0;
