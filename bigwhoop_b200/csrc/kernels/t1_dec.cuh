@@ -154,6 +154,17 @@ T1_HD uint32_t dec_bit(MqDec &d, uint32_t *slot, const uint32_t *tbl) {
 
 // ---- the sequential decoder ----------------------------------------------------------------
 
+// bit i set when nibble i of m is not zero
+T1_HD uint32_t nib_any(u64 m) {
+  m = (m | (m >> 1));
+  m = (m | (m >> 2)) & kRow0;
+  m = (m | (m >> 3)) & 0x0303030303030303ull;
+  m = (m | (m >> 6)) & 0x000F000F000F000Full;
+  m = (m | (m >> 12)) & 0x000000FF000000FFull;
+  m = (m | (m >> 24)) & 0xFFFFull;
+  return (uint32_t)m;
+}
+
 struct DecOut {
   int bitplane;   // first plane not decoded completely (the reference's `bitplane`)
   int cpass;      // pass reached in it (0 when it was not started)
@@ -204,7 +215,7 @@ T1_HD DecOut decode_seq(const uint8_t *bytes, uint32_t Lmax, int K, int Z, bool 
       }
       if (b < res.pmin) res.pmin = b;
       const int kind = i;
-      uint32_t x = 0, js = 0;   // cursor of column 16g
+      uint32_t gx = 0, gj = 0;   // cursor (x, stripe) of column 16g
       for (int g = 0; g < ngroups; ++g) {
         u64 S = sig[g], G = sgn[g], P = pi[g], D = del[g], Bt = bits[g];
         const int c0 = 16 * g;
@@ -224,9 +235,50 @@ T1_HD DecOut decode_seq(const uint8_t *bytes, uint32_t Lmax, int K, int Z, bool 
           UsW = window(sgn, c0 - Wi, ngroups);
           DsW = window(sgn, c0 + Wi, ngroups);
         }
-        for (int ci = 0; ci < 16; ++ci) {
+        // valid samples of the group (rows below a partial last stripe do not exist)
+        const uint32_t ncg = ((int)ncols - c0 < 16) ? (uint32_t)((int)ncols - c0) : 16u;
+        u64 VALID = (ncg == 16) ? ~0ull : ((1ull << (4 * ncg)) - 1ull);
+        if (rem) VALID = col_masks(g, W, nstripes, nfull, rem, ncols).valid;
+        // the columns that can need a decision in this pass: significance propagation visits
+        // insignificant samples next to significant ones (a column that becomes significant
+        // adds its right neighbour below); refinement the significant, unvisited samples;
+        // cleanup the insignificant, unvisited ones
+        uint32_t work;
+        uint32_t candcols = 0;
+        if (kind == 0) {
+          candcols = nib_any(~S & VALID);
+          if (wide) {
+            const uint32_t sigcols = nib_any(S);
+            const uint32_t ud = nib_any(((Uw | ULw | URw) & kRow3) | ((Dw | DLw | DRw) & kRow0));
+            const uint32_t nbc = sigcols | (sigcols << 1) | (sigcols >> 1) | (Lb ? 1u : 0u) |
+                                 (Rb ? 0x8000u : 0u) | ud;
+            work = candcols & nbc & 0xFFFFu;
+          } else {
+            work = candcols;
+          }
+        } else if (kind == 1) {
+          work = nib_any(S & ~P & VALID);
+        } else {
+          work = nib_any(~S & ~P & VALID);
+        }
+        while (work) {
+          const int ci = ctz64(work);
+          work &= work - 1u;
           const int col = c0 + ci;
-          if (col >= (int)ncols) break;
+          uint32_t x, js;
+          if (wide) {
+            x = gx + (uint32_t)ci;
+            js = gj;
+            if (x >= W) {
+              x -= W;
+              js = (gj + 1 == nstripes) ? 0u : gj + 1;
+            }
+          } else {
+            const uint32_t xx = gx + (uint32_t)ci;
+            x = xx % W;
+            js = (gj + xx / W) % nstripes;
+          }
+          const uint32_t own0 = (uint32_t)(S >> (4 * ci)) & 0xFu;
           const bool full = js < nfull;
           const uint32_t rows = full ? 4u : rem;
           const uint32_t vm = (1u << rows) - 1u;
@@ -372,10 +424,14 @@ T1_HD DecOut decode_seq(const uint8_t *bytes, uint32_t Lmax, int K, int Z, bool 
               }
             }
           }
-          if (++x == W) {
-            x = 0;
-            if (++js == nstripes) js = 0;
-          }
+          if (kind == 0 && ci < 15 && (((uint32_t)(S >> (4 * ci)) & 0xFu) != own0))
+            work |= candcols & (2u << ci);   // the right neighbour may now be visited
+        }
+        // cursor of the next group
+        gx += 16;
+        while (gx >= W) {
+          gx -= W;
+          if (++gj == nstripes) gj = 0;
         }
         if (kind == 2) {
           // the plane's decoded bits are final; the next significance pass starts unvisited

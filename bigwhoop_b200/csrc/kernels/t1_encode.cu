@@ -817,15 +817,14 @@ uint64_t t1_scratch_bytes(uint64_t ncols) {
 }
 
 // Codeblocks per MQ warp, the rule used when the autotuner has no entry.  Each lane runs one
-// codeblock's coder, a long dependent chain, so a warp is latency-bound and its lanes diverge
-// (symbol kinds, byte transfers, pass ends); fewer lanes per warp waste less, until the warps'
-// instructions saturate the schedulers.  Measured on B200 (FP64, 32x32x16 codeblocks): 1030
-// codeblocks code fastest at 1 per warp, 8192 at 4 per warp, i.e. at about three warps per
-// scheduler (148 SMs x 4).
+// codeblock's coder, a long dependent chain; the per-decision code is straight-line, so the lanes
+// of a warp stay converged and a warp codes up to 32 chains for the cost of one.  The rule packs
+// codeblocks until there is about one warp per scheduler (148 SMs x 4), where each chain's
+// latency, not the issue rate, sets the time.
 uint32_t mq_lanes_per_warp(uint32_t ncb) {
-  const uint32_t target_warps = (uint32_t)dev::kNumSMs * 4 * 3;
+  const uint32_t target_warps = (uint32_t)dev::kNumSMs * 4;
   uint32_t lanes = 1;
-  while (lanes < 32 && ncb / (lanes * 2) >= target_warps) lanes *= 2;
+  while (lanes < 32 && ncb / lanes > target_warps) lanes *= 2;
   return lanes;
 }
 

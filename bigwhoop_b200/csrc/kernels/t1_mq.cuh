@@ -44,10 +44,72 @@ T1_HD Chunk load_chunk(const uint8_t *p) {
   return c;
 }
 
+// One decision of the MQ coder (mq_bit_encode, mq.c:478-556), written as straight-line code:
+// every branch of the reference's coder is a select, the context's new state is stored under a
+// predicate, and the byte transfer that falls due during the renormalising shift (at most one in
+// all but the rarest cases) is computed unconditionally and kept under a predicate.  Only a
+// renormalisation long enough to need a second transfer (an interval of at most 0xFF, i.e. a
+// less probable symbol in one of the most skewed states) takes a branch.
+//   ent: the entry of the decision's context; on return the entry of the next decision's
+//        context: nk == k and the state moved ? the new entry : nent (read before this decision)
+T1_HD void mq_code_one(MqState &e, ByteSink &bo, uint32_t sym, uint32_t &ent, uint32_t nk,
+                       uint32_t nent, uint32_t *slot, int stride, const uint32_t *tbl) {
+  const uint32_t k = sym >> 1;
+  const uint32_t em = tbl[(ent >> 17) & 0x7F], el = tbl[(ent >> 24) & 0x7F];
+  const uint32_t qe = ent & 0xFFFFu;
+  const uint32_t A1 = e.A - qe;
+  const bool is_mps = ((sym ^ (ent >> 16)) & 1u) == 0u;
+  const bool keep = is_mps != (A1 < qe);   // the interval keeps its upper part
+  const uint32_t An = keep ? A1 : qe;
+  e.C += keep ? qe : 0u;
+  const bool ren = An < 0x8000u;
+  const uint32_t ne = is_mps ? em : el;
+  if (ren) slot[k * stride] = ne;
+  ent = (ren && nk == k) ? ne : nent;
+  const int sh = clz32(An) - 16;   // 0 without renormalisation
+  e.A = An << sh;
+  // shift up to the transfer point
+  const int s1 = sh < e.ct ? sh : e.ct;
+  e.C <<= s1;
+  e.ct -= s1;
+  const int rem = sh - s1;
+  // transfer_byte (mq.c:85-127) when it fell due
+  const bool tr = e.ct == 0;
+  const uint32_t carry = (e.T != 0xFFu) ? ((e.C >> 27) & 1u) : 0u;
+  const uint32_t T1 = e.T + carry;
+  const uint32_t C1 = carry ? (e.C & 0x7FFFFFFu) : e.C;
+  if (tr && (uint32_t)e.L < bo.cap) bo.out[e.L] = (uint8_t)T1;
+  if (tr && e.L >= 0 && (uint32_t)e.L >= bo.cap) bo.flags |= 1u;
+  const bool ff = T1 == 0xFFu;
+  const uint32_t T2 = (C1 >> (ff ? 20 : 19)) & 0xFFu;
+  const uint32_t C2 = C1 & (ff ? 0xFFFFFu : 0x7FFFFu);
+  e.T = tr ? T2 : e.T;
+  e.C = tr ? C2 : e.C;
+  e.ct = tr ? (ff ? 7 : 8) : e.ct;
+  e.L += tr ? 1 : 0;
+  if (rem < e.ct) {
+    e.C <<= rem;
+    e.ct -= rem;
+  } else {
+    int r = rem;
+    do {   // further transfers fall due: shift up to each, transfer, continue
+      const int s2 = r < e.ct ? r : e.ct;
+      e.C <<= s2;
+      e.ct -= s2;
+      r -= s2;
+      if (e.ct == 0) mq_transfer(e, bo);
+    } while (r > 0);
+  }
+}
+
+T1_HD uint32_t chunk_sym(const Chunk &c, int j) { return (c.w[j >> 2] >> (8 * (j & 3))) & 0xFFu; }
+
 // Codes Z passes of the stream at `src` (pcount[p] decisions in pass p), records the coder state
 // at every pass end in snaps, and leaves the coder unterminated in `e`.  `slot` holds the 19
 // context slots at a stride of `stride` words, `tbl` the 94-entry state table.  The stream must
-// be readable 32 bytes past its end.
+// be readable 32 bytes past its end.  Full chunks of 16 decisions are coded without guards, so
+// that consecutive decisions' independent work overlaps; a pass's last, partial chunk is coded
+// decision by decision.
 T1_HD void mq_code_stream(MqState &e, ByteSink &bo, const uint8_t *src, const uint32_t *pcount,
                           int Z, const uint32_t *tbl, uint32_t *slot, int stride,
                           uint64_t *snaps) {
@@ -66,56 +128,34 @@ T1_HD void mq_code_stream(MqState &e, ByteSink &bo, const uint8_t *src, const ui
       next_count = (p + 1 < Z) ? pcount[p + 1] : 0u;
       continue;
     }
-    const uint32_t cnt = left < 16u ? left : 16u;
     // chunks follow each other through the passes (a pass's last chunk is padded), so the
     // stream is fetched in order, two chunks ahead
     const Chunk c = cur;
     cur = nxt;
     nxt = load_chunk(fetch);
     fetch += 16;
-    uint32_t ent = slot[((c.w[0] & 0xFF) >> 1) * stride];
+    uint32_t ent = slot[(chunk_sym(c, 0) >> 1) * stride];
+    if (left >= 16u) {
 #pragma unroll
-    for (int jj = 0; jj < 16; ++jj) {
-      if ((uint32_t)jj < cnt) {
+      for (int jj = 0; jj < 16; ++jj) {
+        const uint32_t sym = chunk_sym(c, jj);
+        const uint32_t nk = (jj < 15) ? (chunk_sym(c, jj + 1) >> 1) : 0xFFu;
+        const uint32_t nent = (jj < 15) ? slot[nk * stride] : 0u;
+        mq_code_one(e, bo, sym, ent, nk, nent, slot, stride, tbl);
+      }
+      left -= 16u;
+    } else {
+      for (uint32_t jj = 0; jj < left; ++jj) {
         const uint32_t sym = (c.w[jj >> 2] >> (8 * (jj & 3))) & 0xFFu;
-        const uint32_t k = sym >> 1;
         uint32_t nk = 0xFFu, nent = 0u;
-        if (jj < 15 && (uint32_t)(jj + 1) < cnt) {
+        if (jj + 1 < left) {
           nk = ((c.w[(jj + 1) >> 2] >> (8 * ((jj + 1) & 3))) & 0xFFu) >> 1;
           nent = slot[nk * stride];
         }
-        const uint32_t em = tbl[(ent >> 17) & 0x7F], el = tbl[(ent >> 24) & 0x7F];
-        const uint32_t qe = ent & 0xFFFFu;
-        const uint32_t A1 = e.A - qe;
-        const bool mps = ((sym ^ (ent >> 16)) & 1u) == 0u;
-        const bool keep = mps != (A1 < qe);
-        const uint32_t An = keep ? A1 : qe;
-        e.C += keep ? qe : 0u;
-        if (An < 0x8000u) {
-          const uint32_t ne = mps ? em : el;
-          slot[k * stride] = ne;
-          if (nk == k) nent = ne;
-          int sh = clz32(An) - 16;
-          e.A = An << sh;
-          if (sh < e.ct) {
-            e.C <<= sh;
-            e.ct -= sh;
-          } else {
-            do {   // shift up to each due transfer, transfer, continue
-              const int s1 = sh < e.ct ? sh : e.ct;
-              e.C <<= s1;
-              e.ct -= s1;
-              sh -= s1;
-              if (e.ct == 0) mq_transfer(e, bo);
-            } while (sh > 0);
-          }
-        } else {
-          e.A = An;
-        }
-        ent = nent;
+        mq_code_one(e, bo, sym, ent, nk, nent, slot, stride, tbl);
       }
+      left = 0;
     }
-    left -= cnt;
   }
 }
 
