@@ -283,6 +283,58 @@ void rs_dwt_forward_tile(rs_float *work, const uint64_t dims[4], const uint64_t 
   free(line);
 }
 
+/* Inverse transform of one tile's working buffer, dwt.c:1738-2246 with the region bounds of
+ * rs_dwt_forward_tile: levels coarsest first, axes t, z, y, x.  fill_inverse_buffer
+ * (dwt.c:170-272) puts a line's lows at B[0], B[2], ... and its highs at B[1], B[3], ... whatever
+ * the region's start; the buffer is extended like any line; where the start is odd the
+ * lifting runs on B + 1, and buffer_flush_inverse (dwt.c:735-789) writes w[-1], w[0], ... =
+ * B[0], B[1], ... back in order.
+ * Where the start is odd and the length odd, the fill leaves B[len - 1] unwritten (the line's
+ * last high lands on B[len], which the extension overwrites) and the reference lifts whatever its
+ * per-thread line buffer held there from the previous line, so its output then depends on its
+ * OpenMP schedule.  Here that sample is zero, as in a fresh buffer. */
+void rs_dwt_inverse_tile(rs_float *work, const uint64_t dims[4], const uint64_t origin[4],
+                         const uint8_t decomp[4], const uint8_t kernels[4]) {
+  int n_levels = 0;
+  uint64_t maxlen = 1;
+  for (int a = 0; a < 4; ++a) {
+    if (decomp[a] > n_levels) n_levels = decomp[a];
+    if (dims[a] > maxlen) maxlen = dims[a];
+  }
+  rs_float *line = (rs_float *)calloc(maxlen + 2 * EXT + 2, sizeof(rs_float));
+  const uint64_t stride[4] = {1, dims[0], dims[0] * dims[1], dims[0] * dims[1] * dims[2]};
+  for (int level = n_levels - 1; level >= 0; --level) {
+    uint64_t ext[4], r0[4];
+    for (int b = 0; b < 4; ++b) {
+      r0[b] = level_bound(origin[b], level, decomp[b]);
+      ext[b] = level_bound(origin[b] + dims[b], level, decomp[b]) - r0[b];
+    }
+    for (int a = 3; a >= 0; --a) {
+      if (!(level < decomp[a] && ext[a] > 1)) continue;
+      const int64_t len = (int64_t)ext[a];
+      const int odd = (int)(r0[a] % 2);
+      const int64_t half = odd ? len >> 1 : (len + 1) >> 1;
+      int o[3], k = 0;
+      for (int b = 0; b < 4; ++b)
+        if (b != a) o[k++] = b;
+      rs_float *B = line + EXT;
+      rs_float *w = B + odd;
+      for (uint64_t i2 = 0; i2 < ext[o[2]]; ++i2)
+        for (uint64_t i1 = 0; i1 < ext[o[1]]; ++i1)
+          for (uint64_t i0 = 0; i0 < ext[o[0]]; ++i0) {
+            rs_float *base = work + i0 * stride[o[0]] + i1 * stride[o[1]] + i2 * stride[o[2]];
+            if (odd && (len & 1)) B[len - 1] = 0;
+            for (int64_t i = 0; i < half; ++i) B[2 * i] = base[i * stride[a]];
+            for (int64_t i = 0; i < len - half; ++i) B[2 * i + 1] = base[(half + i) * stride[a]];
+            extend(B, len);
+            if (kernels[a] == 1) lift_inverse_53(w, len); else lift_inverse(w, len);
+            for (int64_t i = 0; i < len; ++i) base[i * stride[a]] = B[i];
+          }
+    }
+  }
+  free(line);
+}
+
 void rs_dwt_forward_kernels(rs_float *work, const uint64_t dims[4], const uint8_t decomp[4],
                             const uint8_t kernels[4]) {
   dwt(work, dims, decomp, 1, kernels);

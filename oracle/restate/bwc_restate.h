@@ -58,6 +58,10 @@ void rs_dwt_inverse_kernels(rs_float *work, const uint64_t dims[4], const uint8_
 void rs_dwt_forward_tile(rs_float *work, const uint64_t dims[4], const uint64_t origin[4],
                          const uint8_t decomp[4], const uint8_t kernels[4]);
 
+/* its inverse (the reference's odd-start inverse: lows at B[0], B[2], ..., lifting on B + 1) */
+void rs_dwt_inverse_tile(rs_float *work, const uint64_t dims[4], const uint64_t origin[4],
+                         const uint8_t decomp[4], const uint8_t kernels[4]);
+
 /* one codeblock: box in working-buffer coordinates and its subband's coding parameters */
 typedef struct {
   uint64_t x0, y0, z0, t0;

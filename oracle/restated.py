@@ -49,6 +49,7 @@ def load(precision="double"):
     L.rs_dwt_forward_kernels.argtypes = [vp, vp, vp, vp]
     L.rs_dwt_inverse_kernels.argtypes = [vp, vp, vp, vp]
     L.rs_dwt_forward_tile.argtypes = [vp, vp, vp, vp, vp]
+    L.rs_dwt_inverse_tile.argtypes = [vp, vp, vp, vp, vp]
     L.rs_context_class.restype = C.c_int
     L.rs_context_class.argtypes = [C.c_uint32]
     L.rs_t1_encode.restype = C.c_int64
@@ -163,6 +164,17 @@ def t1_decode(work, dims, cb, K, Z, data, erres=False, precision="double"):
     rc = L.rs_t1_decode(work.ctypes.data, np.asarray(dims, np.uint64).ctypes.data, C.byref(cb),
                         int(erres), int(K), int(Z), buf.ctypes.data, len(data))
     assert rc == 0
+    return work
+
+
+def dwt_inverse_tile(work, dims, origin, decomp, precision="double", kernels=(0, 0, 0, 0)):
+    """inverse transform of one tile: dims its extent, origin its first sample (x, y, z, t)"""
+    d = np.asarray(dims, np.uint64)
+    o = np.asarray(origin, np.uint64)
+    dec = np.array(decomp, dtype=np.uint8)
+    k = np.array(kernels, dtype=np.uint8)
+    load(precision).rs_dwt_inverse_tile(work.ctypes.data, d.ctypes.data, o.ctypes.data,
+                                        dec.ctypes.data, k.ctypes.data)
     return work
 
 

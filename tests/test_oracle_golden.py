@@ -244,3 +244,96 @@ def test_restated_tile_transform_matches_reference(shape, precision, decomp, til
         assert odd_starts > 0
     finally:
         rc.close()
+
+
+TILE_INV_CASES = [
+    # tile sizes multiples of 2^levels: every region of every tile starts at an even coordinate
+    ((26, 30, 27), "double", (3, 3, 3, 0), (16, 16, 8, 1), (0, 0, 0, 0)),
+    ((26, 30, 27), "single", (2, 2, 2, 0), (12, 8, 16, 1), (0, 0, 0, 0)),
+    ((20, 18, 22), "double", (2, 2, 2, 0), (8, 12, 4, 1), (1, 0, 1, 0)),
+    ((8, 20, 24, 30), "double", (2, 2, 2, 1), (16, 12, 8, 4), None),
+    # tiles starting at odd coordinates
+    ((26, 30, 27), "double", (3, 3, 3, 0), (13, 15, 9, 1), (0, 0, 0, 0)),
+    ((20, 18, 22), "double", (2, 2, 2, 0), (7, 9, 11, 1), (1, 0, 1, 0)),
+]
+
+
+def _tiles(dims, tiles):
+    counts = [-(-dims[a] // tiles[a]) for a in range(4)]
+    for t in range(int(np.prod(counts))):
+        idx, r = [], t
+        for a in range(4):
+            idx.append(r % counts[a])
+            r //= counts[a]
+        origin = [idx[a] * tiles[a] for a in range(4)]
+        yield t, origin, [min(tiles[a], dims[a] - origin[a]) for a in range(4)]
+
+
+def _all_even(origin, ext, decomp):
+    """every level region of the tile starts at an even coordinate and none has an odd length
+    starting at an odd coordinate (where the reference reads an unwritten buffer sample)"""
+    import math
+    for a in range(4):
+        for lv in range(decomp[a]):
+            r0 = math.ceil(np.float32(origin[a]) / np.float32(2 ** lv))
+            if r0 % 2:
+                return False
+    return True
+
+
+@pytest.mark.parametrize("shape,precision,decomp,tiles,kernels", TILE_INV_CASES)
+def test_restated_tile_inverse_matches_reference(shape, precision, decomp, tiles, kernels):
+    """The inverse transform of the tiles of a multi-tile reference codestream, by the
+    restatement as by the reference library's own inverse transform stage, bit for bit, for every
+    tile whose level regions all start at even coordinates (all tiles of the aligned tilings)."""
+    ref = need_ref(precision)
+    rs = restated(precision)
+    from bigwhoop_b200 import fields
+    dt = np.float64 if precision == "double" else np.float32
+    f = fields.spectral_field(shape, 9).astype(dt)
+    dims = tuple(reversed(shape)) + (1,) * (4 - len(shape))
+    cb = (2, 2, 2, 1) if len(shape) == 4 else (2, 2, 2, 0)
+    ref.reset_gain_lut(precision)
+    cs = ref.compress(f, precision=precision, decomp=decomp, cb=cb, rate="4", kernels=kernels,
+                      tiles=tiles)
+    kernels = (0, 0, 0, 0) if kernels is None else kernels
+    rd = ref.RefDecompressor(cs, f.shape, f.dtype, precision=precision)
+    checked = 0
+    try:
+        assert rd.num_tiles() > 1
+        for t, origin, ext in _tiles(dims, tiles):
+            if not _all_even(origin, ext, decomp):
+                continue
+            n = int(np.prod(ext))
+            rd.select_tile(t)
+            rd.t1()
+            deq = rd.work()[:n].copy()
+            rd.idwt()
+            rec = rd.work()[:n].copy()
+            rs.dwt_inverse_tile(deq, ext, origin, decomp, precision, kernels=kernels)
+            u = np.uint64 if precision == "double" else np.uint32
+            assert np.array_equal(deq.view(u), rec.view(u)), (t, origin, ext)
+            checked += 1
+    finally:
+        rd.close()
+    assert checked >= 1
+
+
+def test_reference_tile_inverse_depends_on_its_thread_count():
+    """Documents why tiles starting at odd coordinates are not compared with the reference's
+    decompression: its inverse transform of an odd-length line starting at an odd coordinate lifts
+    a sample of its per-thread line buffer that the fill did not write, so its output changes
+    with the number of OpenMP threads (this library and the restatement use zero there)."""
+    ref = need_ref("double")
+    from bigwhoop_b200 import fields
+    f = fields.spectral_field((26, 30, 27), 9)
+    ref.reset_gain_lut("double")
+    cs = ref.compress(f, decomp=(3, 3, 3, 0), cb=(2, 2, 2, 0), rate="4", tiles=(13, 15, 9, 1))
+    outs = []
+    try:
+        for th in (1, 3):
+            ref.set_threads(th, "double")
+            outs.append(ref.decompress(cs, f.shape, f.dtype))
+    finally:
+        ref.set_threads(os.cpu_count() or 1, "double")
+    assert np.count_nonzero(outs[0].view(np.uint64) != outs[1].view(np.uint64)) > 0
