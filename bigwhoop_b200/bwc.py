@@ -297,7 +297,7 @@ class Compressor:
             self.L.bwc_set_codeblocks(self.codec, *codeblocks)
         if qm is not None:
             self.L.bwc_set_qm(self.codec, qm)
-        if tiles is not None:   # tile sizes (x, y, z, t); bwc_compress codes one tile only
+        if tiles is not None:   # tile sizes (x, y, z, t)
             self.L.bwc_set_tiles(self.codec, *[int(v) for v in tiles], 0)
         if kernels is not None:   # wavelet per axis (x, y, z, t): 0 CDF 9/7, 1 LeGall 5/3
             self.L.set_kernels(self.codec, *[int(v) for v in kernels])
@@ -379,8 +379,9 @@ class Decompressor:
         if hdr["nPar"] > 1:
             self.shape = (hdr["nPar"],) + self.shape
         self.dtype = np.float64 if hdr["data_prec"] == 8 else np.float32
-        # decompression writes every value of the field
-        self.out = np.empty(self.shape, dtype=self.dtype) if out is None else out
+        # zero-filled: a tiling in time leaves time steps unwritten (the reference writes each
+        # tile's time steps from the field's first one)
+        self.out = np.zeros(self.shape, dtype=self.dtype) if out is None else out
         self.codec = self.L.bwc_alloc_decoder()
         outp = self.out.ctypes.data if hasattr(self.out, "ctypes") else self.out
         self.stream = self.L.bwc_init_stream(self.cs.ctypes.data, outp, DECOMP)

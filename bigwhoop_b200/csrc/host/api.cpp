@@ -314,9 +314,11 @@ static DwtPlan make_plan(const bwc_gl_ctrl &c, const Parameter &par) {
   for (int l = 0; l < c.nDecomp; ++l) {
     const Box &b = par.res[c.nDecomp - l].box;
     const uint64_t e[4] = {b.X1 - b.X0, b.Y1 - b.Y0, b.Z1 - b.Z0, b.TS1 - b.TS0};
+    const uint64_t o[4] = {b.X0, b.Y0, b.Z0, b.TS0};
     for (int a = 0; a < 4; ++a) {
       plan.ext[l][a] = e[a];
       if (l < dec[a] && e[a] > 1) plan.axis_on[l] |= (uint8_t)(1 << a);
+      if (o[a] & 1) plan.odd[l] |= (uint8_t)(1 << a);
     }
   }
   return plan;
@@ -410,10 +412,47 @@ static int t1_grid(const void *kernel_unused, size_t smem_per_block) {
 }
 
 // ---------------------------------------------------------------------------------------------
-static const char *kSingleTileError =
-    "o##########################################################o\n"
-    "| ERROR: this library compresses single-tile fields only   |\n"
-    "o##########################################################o\n";
+// One tile of one parameter: the unit the device pipeline runs through (a single-tile field has
+// one unit per parameter).  Tiles are taken in tile order, within a tile parameter by parameter,
+// as the reference codes them (libbwc.c:3231-3358).
+struct TileUnit {
+  uint32_t tile, param;
+  FieldDims dims;      // the tile's extent
+  uint64_t n;          // samples of the tile
+  BoxMap map;          // where the tile's samples sit in the user's field
+  bool whole;          // the tile is the whole field (contiguous)
+};
+
+// The tiles of a codec as units.  A tile's samples are read from (and written back to) the
+// field at X0 + nX * (Y0 + y + nY * (Z0 + z + nZ * t)) + the parameter's offset, with t counted
+// from the field's first time step, not the tile's (the reference's fill_buffer and
+// flush_buffer, libbwc.c:727-729 and :870-875, index with t, not TS0 + t).
+static std::vector<TileUnit> tile_units(const bwc_codec *codec) {
+  const bwc_gl_inf &info = codec->info;
+  std::vector<TileUnit> units;
+  const std::vector<Tile> &tiles = codec->tile->tiles;
+  const bool single = tiles.size() == 1;
+  for (const Tile &tile : tiles) {
+    for (uint32_t p = 0; p < (uint32_t)info.nPar; ++p) {
+      TileUnit u;
+      u.tile = tile.index;
+      u.param = p;
+      u.dims = FieldDims{tile.box.nx(), tile.box.ny(), tile.box.nz(), tile.box.nt()};
+      u.n = tile.box.size();
+      const uint64_t po = info.nX * info.nY * info.nZ * info.nTS * (uint64_t)p;
+      u.map.w = u.dims.width;
+      u.map.h = u.dims.height;
+      u.map.d = u.dims.depth;
+      u.map.sy = info.nX;
+      u.map.sz = info.nX * info.nY;
+      u.map.st = info.nX * info.nY * info.nZ;
+      u.map.base = po + tile.box.X0 + info.nX * (tile.box.Y0 + info.nY * tile.box.Z0);
+      u.whole = single;
+      units.push_back(u);
+    }
+  }
+  return units;
+}
 
 static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
   bwc_b200_engine *eng = codec->tile;
@@ -423,20 +462,18 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
          "o##########################################################o\n");
     return 0;
   }
-  if (eng->tiles.size() != 1) {
-    warn(kSingleTileError);
-    return 0;
-  }
   DeviceState *dv = device_state(codec);
   if (!dv) return 0;
   cudaStream_t s = dv->stream;
   bwc_gl_ctrl &c = codec->control;
   bwc_gl_inf &info = codec->info;
-  Tile &tile = eng->tiles[0];
-  const uint64_t n = tile.box.size();
   const size_t dsz = (info.data_prec == bwc_precision_double) ? 8 : 4;
   const uint64_t in_bytes = info.nX * info.nY * info.nZ * info.nTS * (uint64_t)info.nPar * dsz;
-  const FieldDims dims{tile.box.nx(), tile.box.ny(), tile.box.nz(), tile.box.nt()};
+  const std::vector<TileUnit> units = tile_units(codec);
+  const size_t nu = units.size();
+  const size_t ntiles = eng->tiles.size();
+  uint64_t nmax = 0;
+  for (const TileUnit &u : units) nmax = std::max(nmax, u.n);
 
   cudaEventRecord(dv->ev[0], s);
   const uint8_t *src = (const uint8_t *)stream->inp;
@@ -450,54 +487,61 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
   }
   cudaEventRecord(dv->ev[1], s);
 
-  // tables and output regions of every parameter
-  std::vector<std::vector<CbDev>> cbs(info.nPar);
-  std::vector<std::vector<SbDev>> sbs(info.nPar);
-  std::vector<uint64_t> cb_base(info.nPar + 1, 0), byte_base(info.nPar + 1, 0),
-      scr_base(info.nPar + 1, 0), sb_base(info.nPar + 1, 0);
+  // tables and output regions of every unit; a codeblock's slope range goes to its tile's slot
+  std::vector<std::vector<CbDev>> cbs(nu);
+  std::vector<std::vector<SbDev>> sbs(nu);
+  std::vector<uint64_t> cb_base(nu + 1, 0), byte_base(nu + 1, 0), scr_base(nu + 1, 0),
+      sb_base(nu + 1, 0);
   uint32_t max_cols = 0;
-  for (int p = 0; p < info.nPar; ++p) {
+  for (size_t ui = 0; ui < nu; ++ui) {
+    const TileUnit &u = units[ui];
     uint64_t bt, st;
     uint32_t mc;
-    build_tables(tile.params[p], dims, c.error_resilience, true, cbs[p], sbs[p], &bt, &st, &mc);
+    build_tables(eng->tiles[u.tile].params[u.param], u.dims, c.error_resilience, true, cbs[ui],
+                 sbs[ui], &bt, &st, &mc);
     max_cols = std::max(max_cols, mc);
-    cb_base[p + 1] = cb_base[p] + cbs[p].size();
-    byte_base[p + 1] = byte_base[p] + bt;
-    scr_base[p + 1] = scr_base[p] + st;
-    sb_base[p + 1] = sb_base[p] + sbs[p].size();
-    for (CbDev &d : cbs[p]) {
-      d.out_off += byte_base[p];
-      d.scratch_off += scr_base[p];
-      d.sb += (uint32_t)sb_base[p];
+    cb_base[ui + 1] = cb_base[ui] + cbs[ui].size();
+    byte_base[ui + 1] = byte_base[ui] + bt;
+    scr_base[ui + 1] = scr_base[ui] + st;
+    sb_base[ui + 1] = sb_base[ui] + sbs[ui].size();
+    for (CbDev &d : cbs[ui]) {
+      d.out_off += byte_base[ui];
+      d.scratch_off += scr_base[ui];
+      d.sb += (uint32_t)sb_base[ui];
+      d.slot = u.tile;
     }
   }
-  const uint64_t ncb = cb_base[info.nPar];
+  const uint64_t ncb = cb_base[nu];
   std::vector<CbDev> allcb;
   std::vector<SbDev> allsb;
-  for (int p = 0; p < info.nPar; ++p) {
-    allcb.insert(allcb.end(), cbs[p].begin(), cbs[p].end());
-    allsb.insert(allsb.end(), sbs[p].begin(), sbs[p].end());
+  for (size_t ui = 0; ui < nu; ++ui) {
+    allcb.insert(allcb.end(), cbs[ui].begin(), cbs[ui].end());
+    allsb.insert(allsb.end(), sbs[ui].begin(), sbs[ui].end());
   }
-  if (!dv->work.ensure(n * sizeof(bwc_float)) || !dv->temp.ensure(n * sizeof(bwc_float)) ||
-      !dv->keys.ensure(16 * info.nPar) ||
-      !dv->stats.ensure(4 * sizeof(bwc_float) * info.nPar) ||
+  if (!dv->work.ensure(nmax * sizeof(bwc_float)) || !dv->temp.ensure(nmax * sizeof(bwc_float)) ||
+      !dv->keys.ensure(16 * nu) || !dv->stats.ensure(4 * sizeof(bwc_float) * nu) ||
       !dv->cbtab.ensure(sizeof(CbDev) * ncb) || !dv->sbtab.ensure(sizeof(SbDev) * allsb.size()) ||
-      !dv->bytes.ensure(byte_base[info.nPar]) || !dv->scratch.ensure(scr_base[info.nPar]) ||
+      !dv->bytes.ensure(byte_base[nu]) || !dv->scratch.ensure(scr_base[nu]) ||
       !dv->snaps.ensure(ncb * kMaxPasses * 16) || !dv->dmse.ensure(ncb * kMaxPasses * 8) ||
       !dv->K.ensure(ncb) || !dv->Z.ensure(ncb) || !dv->L.ensure(ncb * kMaxPasses * 4) ||
       !dv->S.ensure(ncb * (kMaxPasses + 1) * 2) || !dv->flags.ensure(ncb * 4) ||
-      !dv->slopes.ensure(8) || !dv->counter.ensure(4 * info.nPar))
+      !dv->slopes.ensure(8 * ntiles) || !dv->counter.ensure(4 * nu))
     return 0;
   cudaMemcpyAsync(dv->cbtab.p, allcb.data(), sizeof(CbDev) * ncb, cudaMemcpyHostToDevice, s);
   cudaMemcpyAsync(dv->sbtab.p, allsb.data(), sizeof(SbDev) * allsb.size(), cudaMemcpyHostToDevice, s);
   {
-    const uint32_t init[2] = {0xFFFF, 0};
-    cudaMemcpyAsync(dv->slopes.p, init, 8, cudaMemcpyHostToDevice, s);
+    std::vector<uint32_t> init(2 * ntiles);
+    for (size_t t = 0; t < ntiles; ++t) {
+      init[2 * t] = 0xFFFF;
+      init[2 * t + 1] = 0;
+    }
+    cudaMemcpyAsync(dv->slopes.p, init.data(), 8 * ntiles, cudaMemcpyHostToDevice, s);
+    if (!cuda_ok(cudaStreamSynchronize(s), "tier-1 tables")) return 0;   // `init` dies here
   }
   cudaMemsetAsync(dv->flags.p, 0, ncb * 4, s);
-  cudaMemsetAsync(dv->counter.p, 0, 4 * info.nPar, s);
-  cudaMemsetAsync(dv->keys.p, 0, 16 * info.nPar, s);
-  for (int p = 0; p < info.nPar; ++p) cudaMemsetAsync(dv->keys.as<uint64_t>() + 2 * p, 0xFF, 8, s);
+  cudaMemsetAsync(dv->counter.p, 0, 4 * nu, s);
+  cudaMemsetAsync(dv->keys.p, 0, 16 * nu, s);
+  for (size_t ui = 0; ui < nu; ++ui) cudaMemsetAsync(dv->keys.as<uint64_t>() + 2 * ui, 0xFF, 8, s);
 
   if (t1_model_smem(max_cols) > 200 * 1024) {
     warn("o##########################################################o\n"
@@ -506,7 +550,7 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
     return 0;
   }
   // symbol arena: sized for about 1.1 symbols per sample and bit plane; a full arena is
-  // detected per codeblock and the parameter is coded again with a larger one
+  // detected per codeblock and the unit is coded again with a larger one
   uint64_t total_samples = 0;
   for (uint64_t i = 0; i < ncb; ++i)
     total_samples += (uint64_t)allcb[i].w * ((allcb[i].h + 3) / 4) * 4 * allcb[i].d * allcb[i].nt;
@@ -516,58 +560,64 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
     return 0;
   {
     std::vector<uint32_t> order;
-    for (int p = 0; p < info.nPar; ++p) {
-      const std::vector<uint32_t> o = work_order(allcb, allsb, cb_base[p], cbs[p].size());
+    for (size_t ui = 0; ui < nu; ++ui) {
+      const std::vector<uint32_t> o = work_order(allcb, allsb, cb_base[ui], cbs[ui].size());
       order.insert(order.end(), o.begin(), o.end());
     }
     cudaMemcpyAsync(dv->order.p, order.data(), ncb * 4, cudaMemcpyHostToDevice, s);
     if (!cuda_ok(cudaStreamSynchronize(s), "tier-1 order")) return 0;
   }
   float t_norm = 0, t_dwt = 0, t_t1 = 0, t_model = 0;
-  for (int p = 0; p < info.nPar; ++p) {
+  dv->timings[8] = 0;
+  for (size_t ui = 0; ui < nu; ++ui) {
+    const TileUnit &u = units[ui];
+    Tile &tile = eng->tiles[u.tile];
     const ScopedEvents evs;
     cudaEvent_t a = evs.e[0], b2 = evs.e[1], c2 = evs.e[2], d2 = evs.e[3], m2 = evs.e[4];
     cudaEventRecord(a, s);
-    launch_fill_minmax(src + (uint64_t)p * n * dsz, dsz == 8, n, dv->temp.as<bwc_float>(),
-                       dv->keys.as<uint64_t>() + 2 * p, s);
-    launch_normalize(dv->temp.as<bwc_float>(), n, dv->keys.as<uint64_t>() + 2 * p, c.Qm,
-                     dv->stats.as<bwc_float>() + 4 * p, s);
-    if (p == 0 && dv->dump_set && dv->dump.normalized)
-      cudaMemcpyAsync(dv->dump.normalized, dv->temp.p, n * sizeof(bwc_float), cudaMemcpyDeviceToHost, s);
+    if (u.whole)
+      launch_fill_minmax(src + (uint64_t)u.param * u.n * dsz, dsz == 8, u.n,
+                         dv->temp.as<bwc_float>(), dv->keys.as<uint64_t>() + 2 * ui, s);
+    else
+      launch_fill_minmax_box(src, dsz == 8, u.n, u.map, dv->temp.as<bwc_float>(),
+                             dv->keys.as<uint64_t>() + 2 * ui, s);
+    launch_normalize(dv->temp.as<bwc_float>(), u.n, dv->keys.as<uint64_t>() + 2 * ui, c.Qm,
+                     dv->stats.as<bwc_float>() + 4 * ui, s);
+    if (ui == 0 && dv->dump_set && dv->dump.normalized)
+      cudaMemcpyAsync(dv->dump.normalized, dv->temp.p, u.n * sizeof(bwc_float), cudaMemcpyDeviceToHost, s);
     cudaEventRecord(b2, s);
-    launch_dwt_forward(dv->work.as<bwc_float>(), dv->temp.as<bwc_float>(), dims,
-                       make_plan(c, tile.params[p]), s);
-    if (p == 0 && dv->dump_set && dv->dump.transformed)
-      cudaMemcpyAsync(dv->dump.transformed, dv->work.p, n * sizeof(bwc_float), cudaMemcpyDeviceToHost, s);
+    launch_dwt_forward(dv->work.as<bwc_float>(), dv->temp.as<bwc_float>(), u.dims,
+                       make_plan(c, tile.params[u.param]), s);
+    if (ui == 0 && dv->dump_set && dv->dump.transformed)
+      cudaMemcpyAsync(dv->dump.transformed, dv->work.p, u.n * sizeof(bwc_float), cudaMemcpyDeviceToHost, s);
     cudaEventRecord(c2, s);
     T1EncOut o;
     o.bytes = dv->bytes.as<uint8_t>();
-    o.K = dv->K.as<uint8_t>() + cb_base[p];
-    o.Z = dv->Z.as<uint8_t>() + cb_base[p];
-    o.L = dv->L.as<uint32_t>() + cb_base[p] * kMaxPasses;
-    o.S = dv->S.as<uint16_t>() + cb_base[p] * (kMaxPasses + 1);
+    o.K = dv->K.as<uint8_t>() + cb_base[ui];
+    o.Z = dv->Z.as<uint8_t>() + cb_base[ui];
+    o.L = dv->L.as<uint32_t>() + cb_base[ui] * kMaxPasses;
+    o.S = dv->S.as<uint16_t>() + cb_base[ui] * (kMaxPasses + 1);
     o.slopes = dv->slopes.as<uint32_t>();
-    o.flags = dv->flags.as<uint32_t>() + cb_base[p];
+    o.flags = dv->flags.as<uint32_t>() + cb_base[ui];
     o.planes = dv->scratch.as<uint8_t>();
-    o.snaps = dv->snaps.as<uint64_t>() + cb_base[p] * kMaxPasses * 2;
-    o.dmse = dv->dmse.as<int64_t>() + cb_base[p] * kMaxPasses;
-    o.pass_count = dv->pcount.as<uint32_t>() + cb_base[p] * kMaxPasses;
-    o.pass_off = dv->poff.as<uint64_t>() + cb_base[p] * kMaxPasses;
+    o.snaps = dv->snaps.as<uint64_t>() + cb_base[ui] * kMaxPasses * 2;
+    o.dmse = dv->dmse.as<int64_t>() + cb_base[ui] * kMaxPasses;
+    o.pass_count = dv->pcount.as<uint32_t>() + cb_base[ui] * kMaxPasses;
+    o.pass_off = dv->poff.as<uint64_t>() + cb_base[ui] * kMaxPasses;
     o.sym_used = dv->symused.as<unsigned long long>();
     for (int attempt = 0;; ++attempt) {
       if (!dv->symbols.ensure(arena + 256)) return 0;
       o.symbols = dv->symbols.as<uint8_t>();
       o.sym_cap = dv->symbols.cap - 256;   // slack for the MQ kernel's read-ahead
       cudaMemsetAsync(dv->symused.p, 0, 16, s);
-      cudaMemsetAsync(o.flags, 0, cbs[p].size() * 4, s);
-      launch_t1_encode(dv->work.as<bwc_float>(), dv->cbtab.as<CbDev>() + cb_base[p],
-                       (uint32_t)cbs[p].size(), dv->sbtab.as<SbDev>(), o, max_cols, s,
-                       dv->order.as<uint32_t>() + cb_base[p], dv->queue.as<uint32_t>(), m2);
+      cudaMemsetAsync(o.flags, 0, cbs[ui].size() * 4, s);
+      launch_t1_encode(dv->work.as<bwc_float>(), dv->cbtab.as<CbDev>() + cb_base[ui],
+                       (uint32_t)cbs[ui].size(), dv->sbtab.as<SbDev>(), o, max_cols, s,
+                       dv->order.as<uint32_t>() + cb_base[ui], dv->queue.as<uint32_t>(), m2);
       unsigned long long cnt[2] = {0, 0};
       cudaMemcpyAsync(cnt, dv->symused.p, 16, cudaMemcpyDeviceToHost, s);
       if (!cuda_ok(cudaStreamSynchronize(s), "tier-1 encoding")) return 0;
       const unsigned long long used = cnt[0];
-      if (p == 0) dv->timings[8] = 0;
       if (used <= o.sym_cap) {
         dv->timings[8] += (double)cnt[1] * 1e-6;
         break;
@@ -592,17 +642,16 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
   // tier-1 summary to the host
   cudaEventRecord(dv->ev[2], s);
   std::vector<uint8_t> hK(ncb), hZ(ncb);
-  std::vector<uint32_t> hL(ncb * kMaxPasses), hflags(ncb), hslopes(2);
+  std::vector<uint32_t> hL(ncb * kMaxPasses), hflags(ncb), hslopes(2 * ntiles);
   std::vector<uint16_t> hS(ncb * (kMaxPasses + 1));
-  std::vector<bwc_float> hstats(4 * info.nPar);
+  std::vector<bwc_float> hstats(4 * nu);
   cudaMemcpyAsync(hK.data(), dv->K.p, ncb, cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hZ.data(), dv->Z.p, ncb, cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hL.data(), dv->L.p, ncb * kMaxPasses * 4, cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hS.data(), dv->S.p, ncb * (kMaxPasses + 1) * 2, cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hflags.data(), dv->flags.p, ncb * 4, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(hslopes.data(), dv->slopes.p, 8, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(hstats.data(), dv->stats.p, 4 * sizeof(bwc_float) * info.nPar,
-                  cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hslopes.data(), dv->slopes.p, 8 * ntiles, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hstats.data(), dv->stats.p, 4 * sizeof(bwc_float) * nu, cudaMemcpyDeviceToHost, s);
   cudaEventRecord(dv->ev[3], s);
   if (!cuda_ok(cudaStreamSynchronize(s), "tier-1 download")) return 0;
 
@@ -635,14 +684,15 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
       }
     }
   }
-  for (int p = 0; p < info.nPar; ++p) {
-    Parameter &par = tile.params[p];
-    par.pmin = hstats[4 * p + 0];
-    par.pmax = hstats[4 * p + 1];
-    par.alpha = hstats[4 * p + 2];
-    par.beta = hstats[4 * p + 3];
-    for (uint64_t i = 0; i < cbs[p].size(); ++i) {
-      const uint64_t g = cb_base[p] + i;
+  for (size_t ui = 0; ui < nu; ++ui) {
+    const TileUnit &u = units[ui];
+    Parameter &par = eng->tiles[u.tile].params[u.param];
+    par.pmin = hstats[4 * ui + 0];
+    par.pmax = hstats[4 * ui + 1];
+    par.alpha = hstats[4 * ui + 2];
+    par.beta = hstats[4 * ui + 3];
+    for (uint64_t i = 0; i < cbs[ui].size(); ++i) {
+      const uint64_t g = cb_base[ui] + i;
       Codeblock &cb = par.codeblocks[i];
       CodedBlock &e = cb.enc;
       e.K = hK[g];
@@ -650,16 +700,19 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
       e.Kmsbs = e.K ? (uint8_t)(par.subbands[cb.subband].Kmax - e.K) : 0;
       for (int j = 0; j < e.Z; ++j) e.L[j] = hL[g * kMaxPasses + j];
       for (int j = 0; j <= e.Z; ++j) e.S[j] = hS[g * (kMaxPasses + 1) + j];
-      cb.data_off = cbs[p][i].out_off;
-      cb.data_cap = cbs[p][i].out_cap;
+      cb.data_off = cbs[ui][i].out_off;
+      cb.data_cap = cbs[ui][i].out_cap;
     }
   }
-  tile.slope_min = (uint16_t)hslopes[0];
-  tile.slope_max = (uint16_t)hslopes[1];
+  for (size_t t = 0; t < ntiles; ++t) {
+    eng->tiles[t].slope_min = (uint16_t)hslopes[2 * t];
+    eng->tiles[t].slope_max = (uint16_t)hslopes[2 * t + 1];
+  }
 
-  // tier 2 on the host
+  // tier 2 on the host, tile by tile
   const auto h0 = std::chrono::steady_clock::now();
-  if (t2_encode(codec, tile)) return 0;
+  for (Tile &tile : eng->tiles)
+    if (t2_encode(codec, tile)) return 0;
   std::vector<uint8_t> blob;
   std::vector<GatherPiece> pieces;
   const uint64_t total = layout_codestream(codec, stream, blob, pieces);
@@ -715,23 +768,22 @@ static uchar decompress_impl(bwc_codec *codec, bwc_stream *stream) {
     warn(kCsError);
     return 1;
   }
-  if (eng->tiles.size() != 1) {
-    warn("o##########################################################o\n"
-         "| ERROR: this library decodes single-tile codestreams only |\n"
-         "o##########################################################o\n");
-    return 1;
-  }
   DeviceState *dv = device_state(codec);
   if (!dv) return 1;
   cudaStream_t s = dv->stream;
   bwc_gl_ctrl &c = codec->control;
   bwc_gl_inf &info = codec->info;
-  Tile &tile = eng->tiles[0];
-  const uint64_t n = tile.box.size();
   const size_t dsz = (info.data_prec == bwc_precision_double) ? 8 : 4;
   const uint64_t out_bytes = info.nX * info.nY * info.nZ * info.nTS * (uint64_t)info.nPar * dsz;
-  const FieldDims dims{tile.box.nx(), tile.box.ny(), tile.box.nz(), tile.box.nt()};
   const uint64_t cs_len = c.codestreamSize;
+  const std::vector<TileUnit> units = tile_units(codec);
+  uint64_t nmax = 0;
+  // Tiles that start past the first time step are written to time steps 0.. of the field (as
+  // the reference's flush_buffer does): they overwrite earlier tiles there and leave later time
+  // steps as they were in the caller's buffer, so that buffer is brought to the device first.
+  bool keeps_output = false;
+  for (const TileUnit &u : units) nmax = std::max(nmax, u.n);
+  for (const Tile &t : eng->tiles) keeps_output |= t.box.TS0 != 0;
 
   cudaEventRecord(dv->ev[0], s);
   const uint8_t *dcs = (const uint8_t *)stream->inp;
@@ -747,11 +799,18 @@ static uchar decompress_impl(bwc_codec *codec, bwc_stream *stream) {
   if (!out_dev) {
     if (!dv->outbuf.ensure(out_bytes)) return 1;
     dout = dv->outbuf.as<uint8_t>();
+    if (keeps_output &&
+        !cuda_ok(cudaMemcpyAsync(dout, stream->out, out_bytes, cudaMemcpyHostToDevice, s),
+                 "output upload"))
+      return 1;
   }
   cudaEventRecord(dv->ev[1], s);
   float t_t1 = 0, t_dwt = 0, t_norm = 0;
-  for (int p = 0; p < info.nPar; ++p) {
-    Parameter &par = tile.params[p];
+  for (size_t ui = 0; ui < units.size(); ++ui) {
+    const TileUnit &u = units[ui];
+    Parameter &par = eng->tiles[u.tile].params[u.param];
+    const uint64_t n = u.n;
+    const FieldDims &dims = u.dims;
     std::vector<CbDev> cbs;
     std::vector<SbDev> sbs;
     uint64_t bt, st;
@@ -782,7 +841,7 @@ static uchar decompress_impl(bwc_codec *codec, bwc_stream *stream) {
     uint64_t gstate_bytes = 0;
     if (big)
       for (uint64_t i = 0; i < ncb; ++i) gstate_bytes = std::max<uint64_t>(gstate_bytes, cbs[i].scratch_off);
-    if (!dv->work.ensure(n * sizeof(bwc_float)) || !dv->temp.ensure(n * sizeof(bwc_float)) ||
+    if (!dv->work.ensure(nmax * sizeof(bwc_float)) || !dv->temp.ensure(nmax * sizeof(bwc_float)) ||
         !dv->cbtab.ensure(sizeof(CbDev) * ncb) ||
         !dv->sbtab.ensure(sizeof(SbDev) * sbs.size()) || !dv->bytes.ensure(off + 64) ||
         !dv->mags.ensure(st * sizeof(bwc_raw)) || !dv->K.ensure(ncb) || !dv->Z.ensure(ncb) ||
@@ -819,16 +878,20 @@ static uchar decompress_impl(bwc_codec *codec, bwc_stream *stream) {
                         dv->mags.as<bwc_raw>(), dv->flags.as<uint32_t>(), state_cap,
                         big ? dv->scratch.as<uint16_t>() : nullptr, dv->counter.as<uint32_t>(),
                         grid, s, dv->order.as<uint32_t>(), mc);
-    if (p == 0 && dv->ddump_set && dv->ddump.dequantized)
+    if (ui == 0 && dv->ddump_set && dv->ddump.dequantized)
       cudaMemcpyAsync(dv->ddump.dequantized, dv->temp.p, n * sizeof(bwc_float), cudaMemcpyDeviceToHost, s);
     cudaEventRecord(b2, s);
     launch_dwt_inverse(dv->work.as<bwc_float>(), dv->temp.as<bwc_float>(), dims,
                        make_plan(c, par), s);
-    if (p == 0 && dv->ddump_set && dv->ddump.reconstructed)
+    if (ui == 0 && dv->ddump_set && dv->ddump.reconstructed)
       cudaMemcpyAsync(dv->ddump.reconstructed, dv->work.p, n * sizeof(bwc_float), cudaMemcpyDeviceToHost, s);
     cudaEventRecord(c2, s);
-    launch_denormalize(dv->work.as<bwc_float>(), n, par.pmin, par.pmax, c.Qm,
-                       dout + (uint64_t)p * n * dsz, dsz == 8, s);
+    if (u.whole)
+      launch_denormalize(dv->work.as<bwc_float>(), n, par.pmin, par.pmax, c.Qm,
+                         dout + (uint64_t)u.param * n * dsz, dsz == 8, s);
+    else
+      launch_denormalize_box(dv->work.as<bwc_float>(), n, par.pmin, par.pmax, c.Qm, dout,
+                             dsz == 8, u.map, s);
     cudaEventRecord(d2, s);
     if (!cuda_ok(cudaStreamSynchronize(s), "decompression kernels")) return 1;
     float x;
@@ -918,8 +981,11 @@ BatchState *batch_state() {
 
 struct BatchUnit {
   uint32_t field;
+  uint32_t tile;       // tile index within the field
   int param;
   uint64_t n;          // values
+  BoxMap map;          // the tile's samples in the field's input
+  bool whole;          // the field is one tile (its parameter is contiguous)
   uint64_t work_off;   // element offset in the batch working buffers
   const uint8_t *src;  // device address of the unit's input values
   bool src_double;
@@ -945,47 +1011,49 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
            "o##########################################################o\n");
       return 1;
     }
-    if (codecs[i]->tile->tiles.size() != 1) {
-      warn(kSingleTileError);
-      return 1;
-    }
   }
   cudaEventRecord(bs->ev[0], s);
   // ---- units, inputs, tables
   std::vector<BatchUnit> units;
   std::vector<uint64_t> in_off(nf, ~0ull), in_bytes(nf, 0);
   uint64_t work_total = 0, in_total = 0;
+  // slope-range slot of every (field, tile): tile t of field i uses slot tile_base[i] + t
+  std::vector<uint32_t> tile_base(nf + 1, 0);
   for (uint32_t i = 0; i < nf; ++i) {
     bwc_codec *codec = codecs[i];
     const bwc_gl_inf &info = codec->info;
-    Tile &tile = codec->tile->tiles[0];
-    const uint64_t n = tile.box.size();
     const size_t dsz = (info.data_prec == bwc_precision_double) ? 8 : 4;
     in_bytes[i] = info.nX * info.nY * info.nZ * info.nTS * (uint64_t)info.nPar * dsz;
     if (!is_device_pointer(streams[i]->inp)) {
       in_off[i] = in_total;
       in_total += (in_bytes[i] + 255) & ~255ull;
     }
-    for (int p = 0; p < info.nPar; ++p) {
+    tile_base[i + 1] = tile_base[i] + (uint32_t)codec->tile->tiles.size();
+    for (const TileUnit &tu : tile_units(codec)) {
+      const Tile &tile = codec->tile->tiles[tu.tile];
       BatchUnit u{};
       u.field = i;
-      u.param = p;
-      u.n = n;
+      u.tile = tu.tile;
+      u.param = (int)tu.param;
+      u.n = tu.n;
+      u.map = tu.map;
+      u.whole = tu.whole;
       u.work_off = work_total;
-      work_total += (n + 31) & ~31ull;
+      work_total += (u.n + 31) & ~31ull;
       u.src_double = dsz == 8;
-      u.dims = FieldDims{tile.box.nx(), tile.box.ny(), tile.box.nz(), tile.box.nt()};
-      u.plan = make_plan(codec->control, tile.params[p]);
+      u.dims = tu.dims;
+      u.plan = make_plan(codec->control, tile.params[tu.param]);
       u.Qm = codec->control.Qm;
       units.push_back(u);
     }
   }
+  const uint32_t nslots = tile_base[nf];
   std::vector<CbDev> allcb;
   std::vector<SbDev> allsb;
   uint64_t bytes_total = 0, scratch_total = 0, total_samples = 0;
   uint32_t max_cols = 0;
   for (BatchUnit &u : units) {
-    Tile &tile = codecs[u.field]->tile->tiles[0];
+    Tile &tile = codecs[u.field]->tile->tiles[u.tile];
     std::vector<CbDev> cbs;
     std::vector<SbDev> sbs;
     uint64_t bt, st;
@@ -1000,7 +1068,7 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
       d.out_off += bytes_total;
       d.scratch_off += scratch_total;
       d.sb += (uint32_t)allsb.size();
-      d.slot = u.field;
+      d.slot = tile_base[u.field] + u.tile;
       total_samples += (uint64_t)d.w * ((d.h + 3) / 4) * 4 * d.d * d.nt;
       allcb.push_back(d);
     }
@@ -1022,7 +1090,7 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
       !bs->scratch.ensure(scratch_total) || !bs->snaps.ensure(ncb * kMaxPasses * 16) ||
       !bs->dmse.ensure(ncb * kMaxPasses * 8) || !bs->K.ensure(ncb) || !bs->Z.ensure(ncb) ||
       !bs->L.ensure(ncb * kMaxPasses * 4) || !bs->S.ensure(ncb * (kMaxPasses + 1) * 2) ||
-      !bs->flags.ensure(ncb * 4) || !bs->slopes.ensure(8 * nf) ||
+      !bs->flags.ensure(ncb * 4) || !bs->slopes.ensure(8 * nslots) ||
       !bs->pcount.ensure(ncb * kMaxPasses * 4) || !bs->poff.ensure(ncb * kMaxPasses * 8) ||
       !bs->symused.ensure(16) || !bs->order.ensure(ncb * 4) || !bs->queue.ensure(4))
     return 1;
@@ -1084,7 +1152,7 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
     const size_t dsz = u.src_double ? 8 : 4;
     const uint8_t *base = (in_off[u.field] != ~0ull) ? bs->in.as<uint8_t>() + in_off[u.field]
                                                      : (const uint8_t *)streams[u.field]->inp;
-    u.src = base + (uint64_t)u.param * u.n * dsz;
+    u.src = u.whole ? base + (uint64_t)u.param * u.n * dsz : base;
     (void)codec;
   }
   cudaMemcpyAsync(bs->cbtab.p, allcb.data(), sizeof(CbDev) * ncb, cudaMemcpyHostToDevice, s);
@@ -1092,12 +1160,12 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
                   s);
   cudaMemcpyAsync(bs->order.p, order.data(), ncb * 4, cudaMemcpyHostToDevice, s);
   {
-    std::vector<uint32_t> init(2 * nf);
-    for (uint32_t i = 0; i < nf; ++i) {
+    std::vector<uint32_t> init(2 * nslots);
+    for (uint32_t i = 0; i < nslots; ++i) {
       init[2 * i] = 0xFFFF;
       init[2 * i + 1] = 0;
     }
-    cudaMemcpyAsync(bs->slopes.p, init.data(), 8 * nf, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(bs->slopes.p, init.data(), 8 * nslots, cudaMemcpyHostToDevice, s);
     std::vector<uint64_t> keys(2 * nu);
     for (uint64_t u = 0; u < nu; ++u) {
       keys[2 * u] = ~0ull;
@@ -1119,7 +1187,11 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
       cudaStream_t ss = bs->side[ui % kBatchStreams];
       bwc_float *temp = bs->temp.as<bwc_float>() + u.work_off;
       bwc_float *work = bs->work.as<bwc_float>() + u.work_off;
-      launch_fill_minmax(u.src, u.src_double, u.n, temp, bs->keys.as<uint64_t>() + 2 * ui, ss);
+      if (u.whole)
+        launch_fill_minmax(u.src, u.src_double, u.n, temp, bs->keys.as<uint64_t>() + 2 * ui, ss);
+      else
+        launch_fill_minmax_box(u.src, u.src_double, u.n, u.map, temp,
+                               bs->keys.as<uint64_t>() + 2 * ui, ss);
       launch_normalize(temp, u.n, bs->keys.as<uint64_t>() + 2 * ui, u.Qm,
                        bs->stats.as<bwc_float>() + 4 * ui, ss);
       launch_dwt_forward(work, temp, u.dims, u.plan, ss);
@@ -1140,7 +1212,15 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
                (unsigned long long)u.dims.width, (unsigned long long)u.dims.height,
                (unsigned long long)(u.dims.depth * 65536 + u.dims.dt), u.plan.levels, u.Qm);
       sig += buf;
-      for (int l = 0; l < u.plan.levels; ++l) sig += std::to_string(u.plan.axis_on[l]);
+      if (!u.whole) {
+        snprintf(buf, sizeof buf, "b%llu %llu %llu %llu|", (unsigned long long)u.map.base,
+                 (unsigned long long)u.map.sy, (unsigned long long)u.map.sz,
+                 (unsigned long long)u.map.st);
+        sig += buf;
+      }
+      for (int k = 0; k < 4; ++k) sig += std::to_string(u.plan.kern[k]);
+      for (int l = 0; l < u.plan.levels; ++l)
+        sig += std::to_string(u.plan.axis_on[l] | (u.plan.odd[l] << 8)) + ",";
     }
   }
   cudaGraphExec_t exec = nullptr;
@@ -1212,7 +1292,7 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
   }
   cudaEventRecord(bs->ev[3], s);
   std::vector<uint8_t> hK(ncb), hZ(ncb);
-  std::vector<uint32_t> hL(ncb * kMaxPasses), hflags(ncb), hslopes(2 * nf);
+  std::vector<uint32_t> hL(ncb * kMaxPasses), hflags(ncb), hslopes(2 * nslots);
   std::vector<uint16_t> hS(ncb * (kMaxPasses + 1));
   std::vector<bwc_float> hstats(4 * nu);
   cudaMemcpyAsync(hK.data(), bs->K.p, ncb, cudaMemcpyDeviceToHost, s);
@@ -1220,7 +1300,7 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
   cudaMemcpyAsync(hL.data(), bs->L.p, ncb * kMaxPasses * 4, cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hS.data(), bs->S.p, ncb * (kMaxPasses + 1) * 2, cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hflags.data(), bs->flags.p, ncb * 4, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(hslopes.data(), bs->slopes.p, 8 * nf, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hslopes.data(), bs->slopes.p, 8 * nslots, cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hstats.data(), bs->stats.p, 4 * sizeof(bwc_float) * nu, cudaMemcpyDeviceToHost,
                   s);
   if (!cuda_ok(cudaStreamSynchronize(s), "batch tier-1 download")) return 1;
@@ -1248,10 +1328,9 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
       const uint32_t i = next.fetch_add(1);
       if (i >= nf) return;
       bwc_codec *codec = codecs[i];
-      Tile &tile = codec->tile->tiles[0];
       for (uint64_t ui = first_unit[i]; ui < first_unit[i + 1]; ++ui) {
         const BatchUnit &u = units[ui];
-        Parameter &par = tile.params[u.param];
+        Parameter &par = codec->tile->tiles[u.tile].params[u.param];
         par.pmin = hstats[4 * ui + 0];
         par.pmax = hstats[4 * ui + 1];
         par.alpha = hstats[4 * ui + 2];
@@ -1269,9 +1348,16 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
           cb.data_cap = allcb[g].out_cap;
         }
       }
-      tile.slope_min = (uint16_t)hslopes[2 * i];
-      tile.slope_max = (uint16_t)hslopes[2 * i + 1];
-      if (t2_encode(codec, tile)) {
+      bool ok = true;
+      for (Tile &tile : codec->tile->tiles) {
+        tile.slope_min = (uint16_t)hslopes[2 * (tile_base[i] + tile.index)];
+        tile.slope_max = (uint16_t)hslopes[2 * (tile_base[i] + tile.index) + 1];
+        if (t2_encode(codec, tile)) {
+          ok = false;
+          break;
+        }
+      }
+      if (!ok) {
         failed = 1;
         continue;
       }

@@ -3,10 +3,10 @@
 // de-/interleave, :1216-2246 level/axis drivers).
 //
 // Fields whose every transformed axis uses the 9/7 kernel take the fused paths below.  A field
-// with a 5/3 axis is transformed axis by axis in place (dwt_axis_kernel): each block holds whole
-// lines in shared memory with an 8-sample reflected extension on both sides and lifts them over
-// the extended range exactly as the reference lifts its extended line buffers, for either
-// kernel.
+// with a 5/3 axis, or a tile whose level regions start at odd coordinates, is transformed axis by
+// axis in place (dwt_axis_kernel): each block holds whole lines in shared memory with an
+// 8-sample reflected extension on both sides and lifts them over the extended range exactly as
+// the reference lifts its extended line buffers, for either kernel and either start parity.
 //
 // Each level's spatial axes are transformed by one fused pass, reading one field-sized buffer
 // and writing the other: the z-streaming kernel (dwt_stream_fwd_kernel) for large forward 3D
@@ -652,7 +652,12 @@ __global__ void __launch_bounds__(256) dwt_axis_kernel(bwc_float *__restrict__ w
   const int tid = threadIdx.x, nth = blockDim.x;
   // B[q] of line x at sm[(q + kExt + 1) * TX + x]; the lifting's w = B + odd
   auto B = [&](int q, int x) -> bwc_float & { return sm[(q + kExt + 1) * TX + x]; };
-  const int half = kFwd ? (odd ? (len >> 1) : ((len + 1) >> 1)) : ((len + 1) >> 1);
+  const int half = odd ? (len >> 1) : ((len + 1) >> 1);
+  if (!kFwd && odd && (len & 1)) {
+    // the inverse's fill leaves this sample unwritten (the line's last high lands past its end,
+    // where the extension overwrites it); it is zero here
+    for (int x = tid; x < TX; x += nth) B(len - 1, x) = (bwc_float)0;
+  }
   for (int q = tid; q < len * TX; q += nth) {
     const int i = q / TX, x = q - i * TX;
     if (x >= tw) continue;
@@ -848,7 +853,7 @@ void axis_pass(bwc_float *work, const FieldDims &d, const uint64_t *e, int a, in
 bool uses_axis_path(const DwtPlan &plan) {
   for (int l = 0; l < plan.levels; ++l)
     for (int a = 0; a < 4; ++a)
-      if ((plan.axis_on[l] >> a & 1) && plan.kern[a] != 0) return true;
+      if ((plan.axis_on[l] >> a & 1) && (plan.kern[a] != 0 || (plan.odd[l] >> a & 1))) return true;
   return false;
 }
 
@@ -871,7 +876,8 @@ void launch_dwt_forward(bwc_float *work, bwc_float *temp, const FieldDims &dims,
     copy_region(temp, work, dims, full, s);
     for (int l = 0; l < plan.levels; ++l)
       for (int a = 0; a < 4; ++a)
-        if (plan.axis_on[l] >> a & 1) axis_pass<true>(work, dims, plan.ext[l], a, plan.kern[a], 0, s);
+        if (plan.axis_on[l] >> a & 1)
+          axis_pass<true>(work, dims, plan.ext[l], a, plan.kern[a], plan.odd[l] >> a & 1, s);
     return;
   }
   for (int l = 0; l < plan.levels; ++l) {
@@ -901,7 +907,8 @@ void launch_dwt_inverse(bwc_float *work, bwc_float *temp, const FieldDims &dims,
     // axis by axis in place (t, z, y, x per level, coarsest level first), then to `work`
     for (int l = plan.levels - 1; l >= 0; --l)
       for (int a = 3; a >= 0; --a)
-        if (plan.axis_on[l] >> a & 1) axis_pass<false>(temp, dims, plan.ext[l], a, plan.kern[a], 0, s);
+        if (plan.axis_on[l] >> a & 1)
+          axis_pass<false>(temp, dims, plan.ext[l], a, plan.kern[a], plan.odd[l] >> a & 1, s);
     copy_region(temp, work, dims, full, s);
     return;
   }

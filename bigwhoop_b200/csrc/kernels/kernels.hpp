@@ -61,6 +61,17 @@ struct FieldDims {
 };
 
 // field.cu
+// A box of w x h x d x t samples of a field: element (x, y, z, t) at base + x + sy*y + sz*z +
+// st*t (the tiles of a multi-tile field).
+struct BoxMap {
+  uint64_t w, h, d;
+  uint64_t base, sy, sz, st;
+};
+void launch_fill_minmax_box(const void *src, bool src_double, uint64_t n, const BoxMap &m,
+                            bwc_float *work, uint64_t *keys, cudaStream_t s);
+void launch_denormalize_box(const bwc_float *work, uint64_t n, bwc_float pmin, bwc_float pmax,
+                            uint8_t Qm, void *dst, bool dst_double, const BoxMap &m,
+                            cudaStream_t s);
 void launch_fill_minmax(const void *src, bool src_double, uint64_t n, bwc_float *work,
                         uint64_t *minmax_keys, cudaStream_t s);
 void launch_normalize(bwc_float *work, uint64_t n, const uint64_t *minmax_keys, uint8_t Qm,
@@ -71,12 +82,14 @@ void launch_denormalize(const bwc_float *work, uint64_t n, bwc_float pmin, bwc_f
 // dwt.cu: the multi-level separable transform (CDF 9/7 or LeGall 5/3 per axis) of one parameter.
 // level_ext[l] = extents (x, y, z, t) of the region transformed at level l; axis_on[l] bit a
 // set when axis a is transformed at level l.
-// kern[a]: the axis's wavelet kernel, 0 CDF 9/7, 1 LeGall 5/3.
+// kern[a]: the axis's wavelet kernel, 0 CDF 9/7, 1 LeGall 5/3; odd[l] bit a: the level's region
+// starts at an odd coordinate along axis a (tiles of a multi-tile field).
 struct DwtPlan {
   int levels;
   uint64_t ext[16][4];
   uint8_t axis_on[16];
   uint8_t kern[4];
+  uint8_t odd[16];
 };
 // Forward: `temp` holds the normalised field on entry, the coefficients end in `work`;
 // inverse: `temp` holds the coefficients, the field ends in `work`.  `temp` is scratch after.

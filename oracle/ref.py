@@ -58,6 +58,8 @@ def load(precision="double"):
     L.rp_stage_assemble.argtypes = [vp]
     L.rp_copy_work.restype = u64
     L.rp_copy_work.argtypes = [vp, vp]
+    L.rp_set_work.restype = C.c_int
+    L.rp_set_work.argtypes = [vp, vp, u64]
     L.rp_param_stats.argtypes = [vp, C.c_int, vp]
     L.rp_num_codeblocks.restype = u64
     L.rp_num_codeblocks.argtypes = [vp, C.c_int]
@@ -266,6 +268,12 @@ class RefDecompressor:
         buf = np.zeros(n, dtype=dt)
         self.L.rp_copy_work(self.h, buf.ctypes.data)
         return buf
+
+    def set_work(self, buf):
+        """replaces the start of the working buffer with ``buf`` (values of the codec's
+        precision), e.g. a transform computed elsewhere, before finish()"""
+        b = np.ascontiguousarray(buf)
+        assert self.L.rp_set_work(self.h, b.ctypes.data, b.size) == 0
 
     def num_tiles(self):
         return int(self.L.rp_num_tiles(self.h))

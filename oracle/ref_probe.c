@@ -253,6 +253,14 @@ uint64 rp_copy_work(rp_handle *h, void *dst)
    return h->work_len;
 }
 
+/* overwrite the first n values of the working buffer (PREC_BYTE per value); 1 if n exceeds it */
+int rp_set_work(rp_handle *h, const void *src, uint64 n)
+{
+   if(rp_ensure_work(h) || n > h->work_len) return 1;
+   memcpy(h->work, src, n * sizeof(bwc_sample));
+   return 0;
+}
+
 /* parameter statistics after fill: min, max, alpha, beta (as double) */
 void rp_param_stats(rp_handle *h, int p, double *out4)
 {

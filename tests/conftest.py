@@ -35,3 +35,10 @@ def need_ref(precision="double"):
     if not ref.available(precision):
         pytest.skip("reference oracle library not built (make -C oracle)")
     return ref
+
+
+def need_restated(precision="double"):
+    from oracle import restated as rs
+    if not rs.available(precision):
+        pytest.skip("restatement not built (make -C oracle restate)")
+    return rs
