@@ -347,9 +347,12 @@ def run_ours(a):
 
     # kernels per compression: fill+min/max, normalise, one fused DWT pass per level and the
     # region copies between the ping-pong buffers (before every even level but the first, and
-    # after an even number of levels), tier-1 context modelling + MQ coding, codestream gather
+    # after an even number of levels), tier-1 context modelling + MQ coding (per phase),
+    # codestream gather
     L = DECOMP[0]
-    launches = 2 + L + len(range(2, L, 2)) + (1 if L % 2 == 0 else 0) + 2 + 1
+    # (tier-1: one modelling and one MQ launch per phase, stage[11] phases)
+    launches = (2 + L + len(range(2, L, 2)) + (1 if L % 2 == 0 else 0)
+                + 2 * max(1, int(stage[11]) if len(stage) > 11 else 1) + 1)
     line = None
     if rank == 0:
         total_bytes = nbytes * ws
@@ -427,13 +430,15 @@ def run_ours(a):
     return 0
 
 
-# Warp instructions issued per coded symbol by each tier-1 kernel, from the ncu capture named
-# beside it (instruction counts of the 256^3 bench field divided by its symbol count; the
-# figures do not depend on the field size).  The live part of the roofline is the symbol count
-# and each kernel's CUDA-event time in this run.
-T1_WARP_INSTR_PER_SYMBOL = {
-    "t1_model_kernel": (10.6, "profiles/t1_kernels_256cube_f64.md"),
-    "t1_mq_kernel": (44.0, "profiles/t1_kernels_256cube_f64.md"),
+# Warp instructions issued by each tier-1 kernel at this workload (512^3 FP64, 8192 codeblocks,
+# the MQ coder at 16 codeblocks per warp), from the ncu capture named beside it: per coded
+# symbol for the encoder's kernels (smsp__inst_executed.sum over the capture's symbol count),
+# and the decoder's total for one decompression of the workload's codestream.  The live part of
+# the roofline is the symbol count and each kernel's CUDA-event time in this run.
+T1_WARP_INSTR = {
+    "t1_model_kernel": (None, "profiles/t1_kernels_512cube_f64.md"),
+    "t1_mq_kernel": (None, "profiles/t1_kernels_512cube_f64.md"),
+    "t1_decode_kernel": (None, "profiles/t1_kernels_512cube_f64.md"),
 }
 SMS = 148
 
@@ -441,38 +446,57 @@ SMS = 148
 def tier1_roofline(stage, dstage, sm_hz, prec):
     """Tier-1 against its bound, integer instruction issue: symbols per second per kernel and the
     fraction of the GPU's warp-instruction issue slots (148 SMs x 4 schedulers x SM clock) the
-    kernel's instructions would fill over its measured time."""
+    kernel's instructions fill over its measured time.  The MQ coder runs as several launches
+    on side streams (one per modelling phase); its figure is per launch: the instructions of
+    all launches over the sum of their device times (CUDA events on their own streams)."""
     sym = float(stage[8]) * 1e6 if len(stage) > 8 else 0.0
     model_ms = float(stage[9]) if len(stage) > 9 else 0.0
+    mq_ms = float(stage[10]) if len(stage) > 10 else 0.0
+    mq_n = int(stage[11]) if len(stage) > 11 else 0
     t1_ms = float(stage[3])
-    kernels = {}
     peak = SMS * 4 * sm_hz
-    for name, ms in (("t1_model_kernel", model_ms), ("t1_mq_kernel", t1_ms - model_ms)):
-        ipsym, src = T1_WARP_INSTR_PER_SYMBOL[name]
+    kernels = {}
+    for name, ms, launches in (("t1_model_kernel", model_ms, None),
+                               ("t1_mq_kernel", mq_ms, mq_n)):
+        ipsym, src = T1_WARP_INSTR[name]
         if ms <= 0 or sym <= 0:
             continue
-        rate = ipsym * sym / (ms * 1e-3)
-        kernels[name] = {"ms": round(ms, 3), "symbols": sym,
-                         "Gsymbols_per_s": sym / (ms * 1e-3) / 1e9,
-                         "warp_instr_per_symbol": ipsym, "instr_source": src,
-                         "issue_frac": rate / peak}
-    kernels["t1_decode_kernel"] = {"ms": round(float(dstage[3]), 3) if len(dstage) > 3 else None}
-    dom = max((k for k in kernels if "issue_frac" in kernels[k]),
-              key=lambda k: kernels[k]["ms"], default=None)
-    if dom is None:
-        roof = {"bound": "int_issue", "achieved": None, "peak": peak / 1e12, "unit": "Twarp-instr/s",
-                "frac": None, "traffic": None}
+        k = {"ms": round(ms, 3), "symbols": sym, "Gsymbols_per_s": sym / (ms * 1e-3) / 1e9,
+             "warp_instr_per_symbol": ipsym, "instr_source": src,
+             "issue_frac": ipsym * sym / (ms * 1e-3) / peak if ipsym else None}
+        if launches:
+            k["launches"] = launches
+            k["ms_per_launch"] = round(ms / launches, 3)
+            k["ms"] = round(ms, 3)
+            k["timing"] = "sum of the launches' device times; the launches overlap in time"
+        else:
+            k["timing"] = ("tier-1 start to the end of the last modelling launch (the MQ "
+                           "launches of earlier phases run beside it)")
+        kernels[name] = k
+    dec_ms = float(dstage[3]) if len(dstage) > 3 else 0.0
+    dinstr, dsrc = T1_WARP_INSTR["t1_decode_kernel"]
+    if dec_ms > 0:
+        kernels["t1_decode_kernel"] = {"ms": round(dec_ms, 3), "warp_instr": dinstr,
+                                       "instr_source": dsrc,
+                                       "issue_frac": dinstr / (dec_ms * 1e-3) / peak
+                                       if dinstr else None}
+    kernels["tier1_stage"] = {"ms": round(t1_ms, 3), "Gsymbols_per_s":
+                              sym / (t1_ms * 1e-3) / 1e9 if t1_ms > 0 else None}
+    if "t1_mq_kernel" not in kernels or not kernels["t1_mq_kernel"]["warp_instr_per_symbol"]:
+        roof = {"bound": "int_issue", "achieved": None, "peak": peak / 1e12,
+                "unit": "Twarp-instr/s", "frac": None, "traffic": None}
     else:
-        k = kernels[dom]
-        ach = k["warp_instr_per_symbol"] * sym / (k["ms"] * 1e-3)
-        roof = {"bound": "int_issue", "kernel": dom, "achieved": ach / 1e12, "peak": peak / 1e12,
-                "unit": "Twarp-instr/s", "frac": ach / peak, "traffic": None,
-                "symbols_per_s": sym / (k["ms"] * 1e-3),
+        k = kernels["t1_mq_kernel"]
+        ach = k["warp_instr_per_symbol"] * sym / (mq_ms * 1e-3)
+        roof = {"bound": "int_issue", "kernel": "t1_mq_kernel", "achieved": ach / 1e12,
+                "peak": peak / 1e12, "unit": "Twarp-instr/s", "frac": ach / peak,
+                "traffic": None, "symbols_per_s_per_launch": sym / (mq_ms * 1e-3),
                 "note": "tier-1 has no HBM or tensor bound: the MQ coder is one dependent chain "
-                        "per codeblock and the context modelling is scalar integer logic; the "
-                        "denominator is the GPU's warp-instruction issue rate at the sampled SM "
-                        "clock, the numerator the kernel's ncu-counted instructions per symbol "
-                        "times the symbols coded per second in this run",
+                        "per codeblock, so its launches last as long as their longest chains and "
+                        "fill few issue slots; the denominator is the GPU's warp-instruction "
+                        "issue rate at the sampled SM clock, the numerator the kernel's "
+                        "ncu-counted instructions per symbol times the symbols coded per second "
+                        "of launch time in this run",
                 "peak_source": "148 SMs x 4 issue slots x sampled SM clock"}
     return {"roofline": roof, "kernels": kernels}
 

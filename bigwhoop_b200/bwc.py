@@ -326,8 +326,8 @@ class Compressor:
         return n
 
     def timings(self):
-        out = np.zeros(10)
-        k = self.L.bwc_b200_last_timings(self.codec, out.ctypes.data, 10)
+        out = np.zeros(12)
+        k = self.L.bwc_b200_last_timings(self.codec, out.ctypes.data, 12)
         return out[:k]
 
     def close(self):
@@ -395,8 +395,8 @@ class Decompressor:
         return self.out
 
     def timings(self):
-        out = np.zeros(10)
-        k = self.L.bwc_b200_last_timings(self.codec, out.ctypes.data, 10)
+        out = np.zeros(12)
+        k = self.L.bwc_b200_last_timings(self.codec, out.ctypes.data, 12)
         return out[:k]
 
     def close(self):

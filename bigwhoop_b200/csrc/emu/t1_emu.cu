@@ -320,6 +320,49 @@ int t1emu_decode(bwc_float *work, const uint64_t *dims, const uint64_t *box, bwc
   return 0;
 }
 
+// MQ coding, truncation lengths and slopes of one codeblock's decisions (back to back, as
+// t1emu_encode returns them, pass_count[Z] per pass) with the coder in two halves: the interval
+// half codes every chunk into (add, shift) pairs first, the register half then applies them, as
+// the split MQ kernel's two warps do chunk by chunk.  Outputs L[Z], S[Z + 1], the bytes
+// (bytes_cap of room) and flags.  Returns 0, or -1 on bad arguments.
+int t1emu_mq_split(const uint8_t *symbols, const uint32_t *pass_count, int K, int Z,
+                   const int64_t *dmse, double gain_step2, uint32_t *L, uint16_t *S,
+                   uint8_t *bytes, uint32_t bytes_cap, uint32_t *flags) {
+  if (Z < 0 || Z > kMaxPasses) return -1;
+  // the arena layout: every pass starts on a 16-byte boundary, readable 32 bytes past the end
+  std::vector<uint64_t> start(Z + 1, 0);
+  uint64_t pos = 0, src = 0;
+  for (int p = 0; p < Z; ++p) {
+    start[p] = pos;
+    pos += ((uint64_t)pass_count[p] + 15) & ~15ull;
+  }
+  std::vector<uint8_t> arena(pos + 64, 0);
+  for (int p = 0; p < Z; ++p) {
+    if (pass_count[p]) std::memcpy(arena.data() + start[p], symbols + src, pass_count[p]);
+    src += pass_count[p];
+  }
+  const uint32_t nchunks = stream_chunks(pass_count, Z);
+  std::vector<uint32_t> pairs((size_t)nchunks * 16 + 16, 0);
+  std::vector<uint16_t> snapA(kMaxPasses, 0);
+  std::vector<uint64_t> snaps(2 * kMaxPasses + 16, 0);
+  uint32_t slot[dev::kCtxTotal];
+  MqProducer P;
+  mq_producer_init(P, arena.data(), pass_count, Z, dev::h_mq_states, slot, 1);
+  for (uint32_t k = 0; k < nchunks; ++k)
+    if (!mq_produce_chunk(P, pairs.data() + (size_t)k * 16, 1, snapA.data(), 1)) return -1;
+  mq_producer_passes(P, snapA.data(), 1);
+  MqConsumer Q;
+  mq_consumer_init(Q, pass_count, Z, bytes, bytes_cap);
+  for (uint32_t k = 0; k < nchunks; ++k)
+    if (!mq_consume_chunk(Q, pairs.data() + (size_t)k * 16, 1, snaps.data())) return -1;
+  mq_consumer_passes(Q, snaps.data());
+  for (int p = 0; p < Z; ++p) snaps[2 * p] |= (uint64_t)snapA[p] << 48;
+  uint32_t smin, smax;
+  t1_finish(Q.e, Q.bo, K, Z, snaps.data(), dmse, gain_step2, L, S, &smin, &smax);
+  *flags = Q.bo.flags;
+  return 0;
+}
+
 // 8x8 bit transpose as the kernels use it (for its unit test)
 unsigned long long t1emu_transpose8(unsigned long long x) { return transpose8(x); }
 

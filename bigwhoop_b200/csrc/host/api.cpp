@@ -110,6 +110,63 @@ struct DevBuf {
   }
 };
 
+// Page-locked host memory, grown as needed and kept (copies from the device into it run at
+// full DMA speed; the driver stages copies into pageable memory through small chunks).
+struct PinnedBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  bool ensure(size_t bytes) {
+    if (cap >= bytes) return true;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+      return false;
+    }
+    cap = bytes;
+    return true;
+  }
+  ~PinnedBuf() {
+    if (p) cudaFreeHost(p);
+  }
+};
+
+// Host copy of the tier-1 results of one call: per codeblock K, Z, truncation lengths, slopes
+// and flags, per slope slot the slope range, per unit the field statistics.  Lives in the
+// caller's page-locked buffer, or in `fallback` when no page-locked memory can be had.
+struct T1Host {
+  uint8_t *K = nullptr, *Z = nullptr;
+  uint32_t *L = nullptr, *flags = nullptr, *slopes = nullptr;
+  uint16_t *S = nullptr;
+  bwc_float *stats = nullptr;
+  std::vector<uint8_t> fallback;
+  bool layout(PinnedBuf &pb, uint64_t ncb, uint64_t nslots, uint64_t nu) {
+    auto al = [](uint64_t x) { return (x + 15) & ~15ull; };
+    const uint64_t oZ = al(ncb), oL = oZ + al(ncb), oF = oL + al(ncb * kMaxPasses * 4),
+                   oSl = oF + al(ncb * 4), oS = oSl + al(8 * nslots),
+                   oSt = oS + al(ncb * (kMaxPasses + 1) * 2),
+                   end = oSt + al(4 * sizeof(bwc_float) * nu);
+    uint8_t *base = nullptr;
+    if (pb.ensure(end)) {
+      base = static_cast<uint8_t *>(pb.p);
+    } else {
+      fallback.assign(end + 16, 0);
+      base = reinterpret_cast<uint8_t *>(
+          (reinterpret_cast<uintptr_t>(fallback.data()) + 15) & ~uintptr_t(15));
+    }
+    K = base;
+    Z = base + oZ;
+    L = reinterpret_cast<uint32_t *>(base + oL);
+    flags = reinterpret_cast<uint32_t *>(base + oF);
+    slopes = reinterpret_cast<uint32_t *>(base + oSl);
+    S = reinterpret_cast<uint16_t *>(base + oS);
+    stats = reinterpret_cast<bwc_float *>(base + oSt);
+    return true;
+  }
+};
+
 uint8_t sig_class(uint8_t hb) {
   // context table by subband orientation (tier1.c:2416-2446)
   switch (hb) {
@@ -132,8 +189,10 @@ struct DeviceState {
   bool dump_set = false, ddump_set = false;
   bwc_b200_stage_dump dump{};
   bwc_b200_decode_dump ddump{};
-  double timings[10] = {};   // stage times (ms); [8] tier-1 symbols coded (millions),
-                             // [9] tier-1 context modelling kernel (ms, part of [3])
+  PinnedBuf t1host;          // page-locked home of the tier-1 results on the host
+  double timings[12] = {};   // stage times (ms); [8] tier-1 symbols coded (millions),
+                             // [9] tier-1 context modelling (ms, part of [3]), [10] the MQ
+                             // launches' device time summed (ms), [11] MQ launches
 
   ~DeviceState() {
     DevBuf *all[] = {&order, &queue, &temp, &in, &work, &keys, &stats, &cbtab, &sbtab, &bytes, &scratch, &snaps, &dmse,
@@ -172,6 +231,34 @@ void free_engine(bwc_codec *codec) {
 }
 
 // timing events of one stage sequence, released however the scope is left
+// MQ launch timing events of one tier-1 launch
+struct ScopedMqTimes {
+  T1LaunchTimes t;
+  ScopedMqTimes() {
+    for (int i = 0; i < 8; ++i) {
+      cudaEventCreate(&t.start[i]);
+      cudaEventCreate(&t.end[i]);
+    }
+  }
+  ~ScopedMqTimes() {
+    for (int i = 0; i < 8; ++i) {
+      cudaEventDestroy(t.start[i]);
+      cudaEventDestroy(t.end[i]);
+    }
+  }
+  double total_ms() const {
+    double sum = 0;
+    for (int i = 0; i < t.n; ++i) {
+      float x = 0;
+      if (cudaEventElapsedTime(&x, t.start[i], t.end[i]) == cudaSuccess) sum += x;
+    }
+    cudaGetLastError();
+    return sum;
+  }
+  ScopedMqTimes(const ScopedMqTimes &) = delete;
+  ScopedMqTimes &operator=(const ScopedMqTimes &) = delete;
+};
+
 struct ScopedEvents {
   cudaEvent_t e[5];
   ScopedEvents() {
@@ -556,7 +643,7 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
     total_samples += (uint64_t)allcb[i].w * ((allcb[i].h + 3) / 4) * 4 * allcb[i].d * allcb[i].nt;
   uint64_t arena = std::max<uint64_t>(1 << 20, total_samples * (kPrecBit + 1) * 9 / 8);
   if (!dv->pcount.ensure(ncb * kMaxPasses * 4) || !dv->poff.ensure(ncb * kMaxPasses * 8) ||
-      !dv->symused.ensure(16) || !dv->order.ensure(ncb * 4) || !dv->queue.ensure(4))
+      !dv->symused.ensure(16) || !dv->order.ensure(ncb * 4) || !dv->queue.ensure(16))
     return 0;
   {
     std::vector<uint32_t> order;
@@ -568,6 +655,8 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
     if (!cuda_ok(cudaStreamSynchronize(s), "tier-1 order")) return 0;
   }
   float t_norm = 0, t_dwt = 0, t_t1 = 0, t_model = 0;
+  double t_mq = 0;
+  int mq_launches = 0;
   dv->timings[8] = 0;
   for (size_t ui = 0; ui < nu; ++ui) {
     const TileUnit &u = units[ui];
@@ -605,6 +694,7 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
     o.pass_count = dv->pcount.as<uint32_t>() + cb_base[ui] * kMaxPasses;
     o.pass_off = dv->poff.as<uint64_t>() + cb_base[ui] * kMaxPasses;
     o.sym_used = dv->symused.as<unsigned long long>();
+    ScopedMqTimes mqt;
     for (int attempt = 0;; ++attempt) {
       if (!dv->symbols.ensure(arena + 256)) return 0;
       o.symbols = dv->symbols.as<uint8_t>();
@@ -613,13 +703,16 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
       cudaMemsetAsync(o.flags, 0, cbs[ui].size() * 4, s);
       launch_t1_encode(dv->work.as<bwc_float>(), dv->cbtab.as<CbDev>() + cb_base[ui],
                        (uint32_t)cbs[ui].size(), dv->sbtab.as<SbDev>(), o, max_cols, s,
-                       dv->order.as<uint32_t>() + cb_base[ui], dv->queue.as<uint32_t>(), m2);
+                       dv->order.as<uint32_t>() + cb_base[ui], dv->queue.as<uint32_t>(), m2,
+                       &mqt.t);
       unsigned long long cnt[2] = {0, 0};
       cudaMemcpyAsync(cnt, dv->symused.p, 16, cudaMemcpyDeviceToHost, s);
       if (!cuda_ok(cudaStreamSynchronize(s), "tier-1 encoding")) return 0;
       const unsigned long long used = cnt[0];
       if (used <= o.sym_cap) {
         dv->timings[8] += (double)cnt[1] * 1e-6;
+        t_mq += mqt.total_ms();
+        mq_launches += mqt.t.n;
         break;
       }
       if (attempt >= 3) {
@@ -641,17 +734,19 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
 
   // tier-1 summary to the host
   cudaEventRecord(dv->ev[2], s);
-  std::vector<uint8_t> hK(ncb), hZ(ncb);
-  std::vector<uint32_t> hL(ncb * kMaxPasses), hflags(ncb), hslopes(2 * ntiles);
-  std::vector<uint16_t> hS(ncb * (kMaxPasses + 1));
-  std::vector<bwc_float> hstats(4 * nu);
-  cudaMemcpyAsync(hK.data(), dv->K.p, ncb, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(hZ.data(), dv->Z.p, ncb, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(hL.data(), dv->L.p, ncb * kMaxPasses * 4, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(hS.data(), dv->S.p, ncb * (kMaxPasses + 1) * 2, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(hflags.data(), dv->flags.p, ncb * 4, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(hslopes.data(), dv->slopes.p, 8 * ntiles, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(hstats.data(), dv->stats.p, 4 * sizeof(bwc_float) * nu, cudaMemcpyDeviceToHost, s);
+  T1Host h;
+  h.layout(dv->t1host, ncb, ntiles, nu);
+  uint8_t *const hK = h.K, *const hZ = h.Z;
+  uint32_t *const hL = h.L, *const hflags = h.flags, *const hslopes = h.slopes;
+  uint16_t *const hS = h.S;
+  bwc_float *const hstats = h.stats;
+  cudaMemcpyAsync(hK, dv->K.p, ncb, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hZ, dv->Z.p, ncb, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hL, dv->L.p, ncb * kMaxPasses * 4, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hS, dv->S.p, ncb * (kMaxPasses + 1) * 2, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hflags, dv->flags.p, ncb * 4, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hslopes, dv->slopes.p, 8 * ntiles, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hstats, dv->stats.p, 4 * sizeof(bwc_float) * nu, cudaMemcpyDeviceToHost, s);
   cudaEventRecord(dv->ev[3], s);
   if (!cuda_ok(cudaStreamSynchronize(s), "tier-1 download")) return 0;
 
@@ -666,12 +761,12 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
   if (dv->dump_set) {
     const bwc_b200_stage_dump &d = dv->dump;
     const uint64_t n0 = cbs[0].size();
-    if (d.K) std::memcpy(d.K, hK.data(), n0);
-    if (d.Z) std::memcpy(d.Z, hZ.data(), n0);
-    if (d.L) std::memcpy(d.L, hL.data(), n0 * kMaxPasses * 4);
-    if (d.S) std::memcpy(d.S, hS.data(), n0 * (kMaxPasses + 1) * 2);
-    if (d.flags) std::memcpy(d.flags, hflags.data(), n0 * 4);
-    if (d.stats) std::memcpy(d.stats, hstats.data(), 4 * sizeof(bwc_float));
+    if (d.K) std::memcpy(d.K, hK, n0);
+    if (d.Z) std::memcpy(d.Z, hZ, n0);
+    if (d.L) std::memcpy(d.L, hL, n0 * kMaxPasses * 4);
+    if (d.S) std::memcpy(d.S, hS, n0 * (kMaxPasses + 1) * 2);
+    if (d.flags) std::memcpy(d.flags, hflags, n0 * 4);
+    if (d.stats) std::memcpy(d.stats, hstats, 4 * sizeof(bwc_float));
     if (d.bytes && d.byte_offsets) {
       uint64_t pos = 0;
       for (uint64_t i = 0; i < n0; ++i) {
@@ -757,6 +852,8 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
   dv->timings[6] = as;
   dv->timings[7] = up + t_norm + t_dwt + t_t1 + dl + dv->timings[5] + as;
   dv->timings[9] = t_model;
+  dv->timings[10] = t_mq;
+  dv->timings[11] = mq_launches;
   dv->dump_set = false;
   return total;
 }
@@ -945,6 +1042,7 @@ struct BatchState {
   DevBuf in, work, temp, keys, stats, cbtab, sbtab, bytes, scratch, snaps, dmse, K, Z, L, S,
       flags, slopes, pcount, poff, symbols, symused, blob, pieces, cs, order, queue;
   double timings[8] = {};
+  PinnedBuf t1host;   // page-locked home of the tier-1 results on the host
   // instantiated graphs of the fill/normalise/transform phase, by batch signature (geometry,
   // sources and buffer addresses); the few most recent are kept
   std::vector<std::pair<std::string, cudaGraphExec_t>> graphs;
@@ -1092,7 +1190,7 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
       !bs->L.ensure(ncb * kMaxPasses * 4) || !bs->S.ensure(ncb * (kMaxPasses + 1) * 2) ||
       !bs->flags.ensure(ncb * 4) || !bs->slopes.ensure(8 * nslots) ||
       !bs->pcount.ensure(ncb * kMaxPasses * 4) || !bs->poff.ensure(ncb * kMaxPasses * 8) ||
-      !bs->symused.ensure(16) || !bs->order.ensure(ncb * 4) || !bs->queue.ensure(4))
+      !bs->symused.ensure(16) || !bs->order.ensure(ncb * 4) || !bs->queue.ensure(16))
     return 1;
   const std::vector<uint32_t> order = work_order(allcb, allsb, 0, ncb);
   // Inputs in pageable host memory go through a page-locked staging area: several host threads
@@ -1291,18 +1389,19 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
     arena = used + (used >> 3) + (1 << 20);
   }
   cudaEventRecord(bs->ev[3], s);
-  std::vector<uint8_t> hK(ncb), hZ(ncb);
-  std::vector<uint32_t> hL(ncb * kMaxPasses), hflags(ncb), hslopes(2 * nslots);
-  std::vector<uint16_t> hS(ncb * (kMaxPasses + 1));
-  std::vector<bwc_float> hstats(4 * nu);
-  cudaMemcpyAsync(hK.data(), bs->K.p, ncb, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(hZ.data(), bs->Z.p, ncb, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(hL.data(), bs->L.p, ncb * kMaxPasses * 4, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(hS.data(), bs->S.p, ncb * (kMaxPasses + 1) * 2, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(hflags.data(), bs->flags.p, ncb * 4, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(hslopes.data(), bs->slopes.p, 8 * nslots, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(hstats.data(), bs->stats.p, 4 * sizeof(bwc_float) * nu, cudaMemcpyDeviceToHost,
-                  s);
+  T1Host h;
+  h.layout(bs->t1host, ncb, nslots, nu);
+  uint8_t *const hK = h.K, *const hZ = h.Z;
+  uint32_t *const hL = h.L, *const hflags = h.flags, *const hslopes = h.slopes;
+  uint16_t *const hS = h.S;
+  bwc_float *const hstats = h.stats;
+  cudaMemcpyAsync(hK, bs->K.p, ncb, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hZ, bs->Z.p, ncb, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hL, bs->L.p, ncb * kMaxPasses * 4, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hS, bs->S.p, ncb * (kMaxPasses + 1) * 2, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hflags, bs->flags.p, ncb * 4, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hslopes, bs->slopes.p, 8 * nslots, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(hstats, bs->stats.p, 4 * sizeof(bwc_float) * nu, cudaMemcpyDeviceToHost, s);
   if (!cuda_ok(cudaStreamSynchronize(s), "batch tier-1 download")) return 1;
   for (uint64_t c = 0; c < ncb; ++c)
     if (hflags[c] & (1u | 16u)) {
@@ -1467,7 +1566,7 @@ extern "C" void bwc_b200_set_decode_dump(bwc_codec *const codec, bwc_b200_decode
 
 extern "C" int bwc_b200_last_timings(bwc_codec *const codec, double *out_ms, int n) {
   if (!codec || !codec->tile || !codec->tile->dev) return 0;
-  const int k = std::min(n, 10);
+  const int k = std::min(n, 12);
   for (int i = 0; i < k; ++i) out_ms[i] = codec->tile->dev->timings[i];
   return k;
 }

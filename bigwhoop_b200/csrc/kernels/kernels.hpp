@@ -105,13 +105,22 @@ size_t t1_model_smem(uint32_t max_cols);
 uint64_t t1_scratch_bytes(uint64_t ncols);
 // Each codeblock addresses its samples as work[base + x + y*sy + z*sz + t*st].  `order`
 // (optional, device) lists the codeblocks largest first: the MQ kernel's lanes take them in
-// that order, and with `queue` (a device counter, zeroed here) the modelling kernel runs
-// persistent and takes codeblocks from that work queue.  `after_model` (optional) is recorded
-// on `s` between the modelling and the MQ kernel.
+// that order, and with `queue` (four device counters, zeroed here) the modelling kernel runs
+// persistent and takes codeblocks from that work queue.  With an order, a queue and at least
+// 2048 codeblocks, the order is modelled in four phases on `s` and each phase's MQ kernel runs
+// on a side stream once its phase is modelled; `s` waits for them before it goes on.
+// `after_model` (optional) is recorded on `s` after the (last) modelling launch; `mq_times`
+// (optional) receives the MQ launches' start and end events.
+// Timing events (created by the caller, timing enabled) that launch_t1_encode records around
+// each MQ launch, on the stream that launch runs on; `n` is set to the number of launches.
+struct T1LaunchTimes {
+  cudaEvent_t start[8] = {}, end[8] = {};
+  int n = 0;
+};
 void launch_t1_encode(const bwc_float *work, const CbDev *cbs, uint32_t ncb, const SbDev *sbs,
                       const T1EncOut &out, uint32_t max_cols, cudaStream_t s,
                       const uint32_t *order = nullptr, uint32_t *queue = nullptr,
-                      cudaEvent_t after_model = nullptr);
+                      cudaEvent_t after_model = nullptr, T1LaunchTimes *mq_times = nullptr);
 
 // t1_decode.cu: decodes Z[c] passes of codeblock c from data + out_off (Lmax[c] bytes) and
 // writes the dequantised samples into the (zeroed) working buffer.

@@ -749,8 +749,9 @@ __global__ void __launch_bounds__(t1::kModelBlock)
 
 // ---- MQ coding, truncation lengths, convex hull ----------------------------------------------
 
+// Codes the codeblocks of queue positions [0, nslots): order[slot], or slot without an order.
 __global__ void __launch_bounds__(kMqThreads) t1_mq_kernel(const CbDev *__restrict__ cbs,
-                                                           uint32_t ncb,
+                                                           uint32_t nslots,
                                                            const SbDev *__restrict__ sbs,
                                                            T1EncOut out, uint32_t lanes,
                                                            const uint32_t *__restrict__ order) {
@@ -763,8 +764,8 @@ __global__ void __launch_bounds__(kMqThreads) t1_mq_kernel(const CbDev *__restri
   // (the host retries those with a larger one) have nothing to code.
   const bool lane_used = threadIdx.x < lanes;
   const uint32_t slot = blockIdx.x * lanes + (lane_used ? threadIdx.x : 0u);
-  const uint32_t c = (slot < ncb) ? (order ? order[slot] : slot) : ncb;
-  if (!lane_used || c >= ncb) return;
+  if (!lane_used || slot >= nslots) return;
+  const uint32_t c = order ? order[slot] : slot;
   const int K = out.K[c];
   if (K == 0 || (out.flags[c] & 8u)) return;
   const CbDev cb = cbs[c];
@@ -784,6 +785,110 @@ __global__ void __launch_bounds__(kMqThreads) t1_mq_kernel(const CbDev *__restri
     atomicMax(&out.slopes[2 * cb.slot + 1], smax);
   }
   out.flags[c] |= bo.flags;
+}
+
+// ---- MQ coding in two halves: one producer and one consumer warp per CTA ---------------------
+// Warp 0 runs the coder's interval half for `lanes` codeblocks, warp 1 its register half for
+// the same codeblocks (t1_mq.cuh).  They meet in a shared-memory ring of kMqRing chunks per
+// lane: the producer fills slot k % kMqRing with chunk k's (add, shift) pairs and arrives on the
+// slot's FULL barrier; the consumer waits on FULL, applies the pairs and arrives on the slot's
+// EMPTY barrier, which the producer waits on before refilling the slot.  Both warps take the
+// same number of steps (the longest lane's chunk count), so every barrier completes; nothing
+// waits on anything outside the CTA.  At the end the consumer adds the producer's A to each
+// pass-end snapshot and computes truncation lengths, hull and slopes.
+constexpr int kMqRing = 4;   // chunks in flight per lane; barrier ids 1..2*kMqRing and 15
+
+// named barriers of the two warps (64 threads); the calling warp is converged first, as the
+// aligned barrier instructions require
+__device__ __forceinline__ void named_sync(int id) {
+  __syncwarp();
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(64) : "memory");
+}
+__device__ __forceinline__ void named_arrive(int id) {
+  __syncwarp();
+  asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(64) : "memory");
+}
+
+__global__ void __launch_bounds__(64) t1_mq_split_kernel(const CbDev *__restrict__ cbs,
+                                                         uint32_t nslots,
+                                                         const SbDev *__restrict__ sbs,
+                                                         T1EncOut out, uint32_t lanes,
+                                                         const uint32_t *__restrict__ order) {
+  __shared__ uint32_t tbl[94];
+  __shared__ uint32_t slots[dev::kCtxTotal][32];
+  __shared__ uint32_t ring[kMqRing][16][32];
+  __shared__ uint16_t snapA[kMaxPasses][32];
+  for (int i = threadIdx.x; i < 94; i += blockDim.x) tbl[i] = dev::c_mq_states[i];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t slot = blockIdx.x * lanes + (uint32_t)lane;
+  const bool have = (uint32_t)lane < lanes && slot < nslots;
+  const uint32_t c = have ? (order ? order[slot] : slot) : 0u;
+  const int K = have ? out.K[c] : 0;
+  // codeblocks with nothing to code, or whose symbol stream did not fit the arena (the host
+  // retries those with a larger one), take part in the barriers only
+  const bool active = have && K != 0 && !(out.flags[c] & 8u);
+  const int Z = active ? out.Z[c] : 0;
+  const uint64_t pbase = (uint64_t)c * kMaxPasses;
+  const uint32_t *pcount = out.pass_count + pbase;
+  const uint32_t nchunks = active ? t1::stream_chunks(pcount, Z) : 0u;
+  const uint32_t nsteps = __reduce_max_sync(0xffffffffu, nchunks);
+  if (warp == 0) {
+    t1::MqProducer P;
+    if (active)
+      t1::mq_producer_init(P, out.symbols + out.pass_off[pbase], pcount, Z, tbl,
+                           &slots[0][lane], 32);
+    for (uint32_t k = 0; k < nsteps; ++k) {
+      const int r = (int)(k % kMqRing);
+      if (k >= (uint32_t)kMqRing) named_sync(1 + kMqRing + r);
+      if (active) t1::mq_produce_chunk(P, &ring[r][0][lane], 32, &snapA[0][lane], 32);
+      __threadfence_block();
+      named_arrive(1 + r);
+    }
+    for (uint32_t k = nsteps; k < nsteps + kMqRing; ++k)
+      if (k >= (uint32_t)kMqRing) named_sync(1 + kMqRing + (int)(k % kMqRing));
+    if (active) t1::mq_producer_passes(P, &snapA[0][lane], 32);
+    __threadfence_block();
+    named_sync(15);
+    return;
+  }
+  const CbDev cb = cbs[c];
+  uint64_t *snaps = out.snaps + pbase * 2;
+  t1::MqConsumer Q;
+  if (active) t1::mq_consumer_init(Q, pcount, Z, out.bytes + cb.out_off, cb.out_cap);
+  for (uint32_t k = 0; k < nsteps; ++k) {
+    const int r = (int)(k % kMqRing);
+    named_sync(1 + r);
+    if (active) t1::mq_consume_chunk(Q, &ring[r][0][lane], 32, snaps);
+    named_arrive(1 + kMqRing + r);
+  }
+  if (active) t1::mq_consumer_passes(Q, snaps);
+  named_sync(15);
+  if (!active) return;
+  for (int p = 0; p < Z; ++p) snaps[2 * p] |= (uint64_t)snapA[p][lane] << 48;
+  const SbDev sb = sbs[cb.sb];
+  uint32_t smin, smax;
+  t1::t1_finish(Q.e, Q.bo, K, Z, snaps, out.dmse + pbase, sb.gain_step2, out.L + pbase,
+                out.S + (uint64_t)c * (kMaxPasses + 1), &smin, &smax);
+  if (smax) {
+    atomicMin(&out.slopes[2 * cb.slot], smin);
+    atomicMax(&out.slopes[2 * cb.slot + 1], smax);
+  }
+  out.flags[c] |= Q.bo.flags;
+}
+
+// MQ launch over queue positions [0, n) of `order`: the split kernel (default) or the
+// one-warp lane coder (BWC_B200_MQ_SPLIT=0)
+void launch_mq(const CbDev *cbs, uint32_t n, const SbDev *sbs, const T1EncOut &out,
+               uint32_t lanes, const uint32_t *order, cudaStream_t s) {
+  static const bool split = [] {
+    const char *v = getenv("BWC_B200_MQ_SPLIT");
+    return !(v && v[0] == '0');
+  }();
+  if (split)
+    t1_mq_split_kernel<<<(n + lanes - 1) / lanes, 64, 0, s>>>(cbs, n, sbs, out, lanes, order);
+  else
+    t1_mq_kernel<<<(n + lanes - 1) / lanes, kMqThreads, 0, s>>>(cbs, n, sbs, out, lanes, order);
 }
 
 }  // namespace
@@ -869,14 +974,34 @@ void load_tune_file_locked() {
   fclose(f);
 }
 
+// Side streams of the phased tier-1 launch, one set per device, created on first use and kept.
+constexpr int kT1Phases = 4;   // at most 8 (T1LaunchTimes)
+std::mutex g_phase_mutex;
+cudaStream_t g_phase_streams[64][kT1Phases] = {};
+
+bool phase_streams(cudaStream_t *out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
+  std::lock_guard<std::mutex> lock(g_phase_mutex);
+  for (int i = 0; i < kT1Phases; ++i) {
+    if (!g_phase_streams[dev][i] &&
+        cudaStreamCreateWithFlags(&g_phase_streams[dev][i], cudaStreamNonBlocking) != cudaSuccess) {
+      g_phase_streams[dev][i] = nullptr;
+      cudaGetLastError();
+      return false;
+    }
+    out[i] = g_phase_streams[dev][i];
+  }
+  return true;
+}
+
 }  // namespace
 
-// Context modelling, then MQ coding, on `s`.  (Running the modelling of later codeblocks
-// concurrently with the MQ coding of earlier ones was measured slower: the issue-bound modelling
-// warps lengthen the latency-bound MQ chains, and the longest chain sets the time.)
+// Context modelling, then MQ coding, on `s` (phased across side streams for large counts).
 void launch_t1_encode(const bwc_float *work, const CbDev *cbs, uint32_t ncb, const SbDev *sbs,
                       const T1EncOut &out, uint32_t max_cols, cudaStream_t s,
-                      const uint32_t *order, uint32_t *queue, cudaEvent_t after_model) {
+                      const uint32_t *order, uint32_t *queue, cudaEvent_t after_model,
+                      T1LaunchTimes *mq_times) {
   if (!ncb) return;
   const size_t smem = t1_model_smem(max_cols);
   const bool narrow = max_cols <= t1::kModelMaxCols;
@@ -884,7 +1009,7 @@ void launch_t1_encode(const bwc_float *work, const CbDev *cbs, uint32_t ncb, con
     cudaFuncSetAttribute(t1_model_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   else
     cudaFuncSetAttribute(t1_model_wide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  unsigned grid = ncb;
+  unsigned resident = ncb;
   if (queue) {
     // persistent: as many CTAs as fit on the GPU at once
     int dev = 0, sms = dev::kNumSMs, per_sm = 1;
@@ -894,15 +1019,17 @@ void launch_t1_encode(const bwc_float *work, const CbDev *cbs, uint32_t ncb, con
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, t1_model_kernel, t1::kModelBlock, smem);
     else
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, t1_model_wide_kernel, kModelThreads, smem);
-    grid = std::min<unsigned>(ncb, (unsigned)std::max(1, sms * std::max(1, per_sm)));
-    cudaMemsetAsync(queue, 0, sizeof(uint32_t), s);
+    resident = (unsigned)std::max(1, sms * std::max(1, per_sm));
   }
-  if (narrow)
-    t1_model_kernel<<<grid, t1::kModelBlock, smem, s>>>(work, cbs, ncb, sbs, out, order, queue);
-  else
-    t1_model_wide_kernel<<<grid, kModelThreads, smem, s>>>(work, cbs, ncb, sbs, out, order, queue,
-                                                           t1_model_stage_cap(max_cols));
-  if (after_model) cudaEventRecord(after_model, s);
+  auto model = [&](const uint32_t *ord, uint32_t n, uint32_t *q) {
+    const unsigned grid = q ? std::min<unsigned>(n, resident) : n;
+    if (q) cudaMemsetAsync(q, 0, sizeof(uint32_t), s);
+    if (narrow)
+      t1_model_kernel<<<grid, t1::kModelBlock, smem, s>>>(work, cbs, n, sbs, out, ord, q);
+    else
+      t1_model_wide_kernel<<<grid, kModelThreads, smem, s>>>(work, cbs, n, sbs, out, ord, q,
+                                                             t1_model_stage_cap(max_cols));
+  };
   const uint32_t rule = mq_lanes_per_warp(ncb);
   uint32_t lanes = rule;
   bool tune = false;
@@ -918,7 +1045,47 @@ void launch_t1_encode(const bwc_float *work, const CbDev *cbs, uint32_t ncb, con
     else
       tune = true;
   }
-  t1_mq_kernel<<<(ncb + lanes - 1) / lanes, kMqThreads, 0, s>>>(cbs, ncb, sbs, out, lanes, order);
+  // Phased: the work order is largest first, and a codeblock's MQ chain is long, so the
+  // codeblocks are modelled in phases (the first 1/64 of the order, then 3/64, 3/16, 3/4), and
+  // each phase's MQ kernel runs on a side stream as soon as that phase is modelled, beside the
+  // modelling of the later phases.  No kernel waits on another: each side stream waits, by a
+  // stream event, for the modelling launch it depends on; the main stream then waits for all.
+  cudaStream_t side[kT1Phases];
+  const bool phased = order && queue && ncb >= 2048 && phase_streams(side);
+  if (!phased) {
+    model(order, ncb, queue);
+    if (after_model) cudaEventRecord(after_model, s);
+    if (mq_times) cudaEventRecord(mq_times->start[0], s);
+    launch_mq(cbs, ncb, sbs, out, lanes, order, s);
+    if (mq_times) {
+      cudaEventRecord(mq_times->end[0], s);
+      mq_times->n = 1;
+    }
+  } else {
+    const uint32_t bound[kT1Phases + 1] = {0, ncb / 64, ncb / 16, ncb / 4, ncb};
+    cudaEvent_t modelled[kT1Phases], coded[kT1Phases];
+    for (int i = 0; i < kT1Phases; ++i) {
+      cudaEventCreateWithFlags(&modelled[i], cudaEventDisableTiming);
+      cudaEventCreateWithFlags(&coded[i], cudaEventDisableTiming);
+    }
+    for (int i = 0; i < kT1Phases; ++i) {
+      const uint32_t n = bound[i + 1] - bound[i];
+      model(order + bound[i], n, queue + i);
+      cudaEventRecord(modelled[i], s);
+      cudaStreamWaitEvent(side[i], modelled[i], 0);
+      if (mq_times) cudaEventRecord(mq_times->start[i], side[i]);
+      launch_mq(cbs, n, sbs, out, lanes, order + bound[i], side[i]);
+      if (mq_times) cudaEventRecord(mq_times->end[i], side[i]);
+      cudaEventRecord(coded[i], side[i]);
+    }
+    if (mq_times) mq_times->n = kT1Phases;
+    if (after_model) cudaEventRecord(after_model, s);
+    for (int i = 0; i < kT1Phases; ++i) {
+      cudaStreamWaitEvent(s, coded[i], 0);
+      cudaEventDestroy(modelled[i]);   // released once the work that uses it has completed
+      cudaEventDestroy(coded[i]);
+    }
+  }
   if (!tune) return;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
@@ -927,7 +1094,7 @@ void launch_t1_encode(const bwc_float *work, const CbDev *cbs, uint32_t ncb, con
   uint32_t best_lanes = rule;
   for (uint32_t cand = std::max(1u, rule / 4); cand <= std::min(32u, rule * 4); cand *= 2) {
     cudaEventRecord(e0, s);
-    t1_mq_kernel<<<(ncb + cand - 1) / cand, kMqThreads, 0, s>>>(cbs, ncb, sbs, out, cand, order);
+    launch_mq(cbs, ncb, sbs, out, cand, order, s);
     cudaEventRecord(e1, s);
     if (cudaEventSynchronize(e1) != cudaSuccess) break;
     float ms = 0;

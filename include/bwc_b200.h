@@ -97,9 +97,9 @@ size_t bwc_b200_assemble_from_tier1(bwc_codec *const codec, bwc_stream *const st
                                     uint16 const slope_min, uint16 const slope_max);
 /* The same for a codec of one or more tiles (bwc_set_tiles): codeblocks of every tile in tile
  * order, within a tile parameter by parameter; minmax = min, max per tile and parameter;
- * slopes = slope minimum, maximum per tile.  bwc_compress codes single-tile fields only; this
- * runs the host half of multi-tile coding (per-tile rate control, packets, the multi-tile
- * codestream).  No counterpart in the reference. */
+ * slopes = slope minimum, maximum per tile.  This runs the host half of multi-tile coding
+ * alone (per-tile rate control, packets, the multi-tile codestream), on tier-1 results made
+ * elsewhere.  No counterpart in the reference. */
 size_t bwc_b200_assemble_tiles_from_tier1(bwc_codec *const codec, bwc_stream *const stream,
                                           uint8 const *K, uint8 const *Z, uint64 const *L,
                                           uint16 const *S, uint8 const *bytes,
@@ -109,9 +109,11 @@ size_t bwc_b200_assemble_tiles_from_tier1(bwc_codec *const codec, bwc_stream *co
 /* Device time of the stages of the last bwc_compress / bwc_decompress on this codec, in
  * milliseconds (CUDA events on the codec's stream): [0] upload, [1] fill+normalise, [2] wavelet,
  * [3] tier-1, [4] download of tier-1 results, [5] tier-2 (host), [6] codestream gather and
- * download, [7] total, [8] tier-1 symbols coded (millions, compression), [9] the tier-1 context
- * modelling kernel alone (compression; the rest of [3] is the MQ coder).  Returns the number of
- * entries written (at most n). */
+ * download, [7] total, [8] tier-1 symbols coded (millions, compression), [9] tier-1 context
+ * modelling (compression: from the start of tier-1 to the end of its last modelling launch),
+ * [10] the MQ coder launches' device time, summed over launches (compression; the launches run
+ * on side streams and overlap the modelling of later codeblocks, so [9] + [10] can exceed [3]),
+ * [11] the number of those launches.  Returns the number of entries written (at most n). */
 int    bwc_b200_last_timings(bwc_codec *const codec, double *out_ms, int n);
 
 /* Batched compression of n independently configured codecs (each set up with

@@ -1,7 +1,8 @@
 """The tier-1 encoder's kernel logic on the CPU (no GPU needed).
 
-The CUDA kernels' bodies -- the block-wide context modelling (t1_model.cuh) and the MQ lane
-coder with its finish (t1_mq.cuh, t1_common.cuh) -- are also built for the host
+The CUDA kernels' bodies -- the block-wide context modelling (t1_model.cuh), the MQ lane
+coder, whole and in its two halves, with its finish (t1_mq.cuh, t1_common.cuh) -- are also
+built for the host
 (lib/emu/<precision>/libt1emu.so, 256 host threads standing in for the CUDA block).  Their
 output is compared, codeblock by codeblock, with the C restatement of the reference encoder:
 
@@ -69,7 +70,32 @@ def run_emu(L, work, dims, box, qt_eff, gain_step2, cls, erres, precision):
     assert total >= 0
     z = int(Z[0])
     return dict(K=int(K[0]), Z=z, counts=pc[:z].astype(np.uint64), symbols=sym[:total].copy(),
-                L=Ls[:z].astype(np.uint64), S=Ss[:z + 1].copy(), data=data, flags=int(flags[0]))
+                L=Ls[:z].astype(np.uint64), S=Ss[:z + 1].copy(), data=data, flags=int(flags[0]),
+                dmse=dm[:z].copy(), bcap=bcap)
+
+
+def run_split(L, m, gain_step2, precision):
+    """the same decisions through the coder in two halves (t1emu_mq_split)"""
+    mp = MAX_PASSES[precision]
+    vp = C.c_void_p
+    L.t1emu_mq_split.restype = C.c_int
+    L.t1emu_mq_split.argtypes = [vp, vp, C.c_int, C.c_int, vp, C.c_double, vp, vp, vp,
+                                 C.c_uint32, vp]
+    z = m["Z"]
+    pc = np.zeros(mp, np.uint32)
+    pc[:z] = m["counts"]
+    dm = np.zeros(mp, np.int64)
+    dm[:z] = m["dmse"]
+    sym = np.concatenate([m["symbols"], np.zeros(16, np.uint8)])
+    Ls = np.zeros(mp, np.uint32)
+    Ss = np.zeros(mp + 1, np.uint16)
+    data = np.zeros(m["bcap"], np.uint8)
+    flags = np.zeros(1, np.uint32)
+    rc = L.t1emu_mq_split(sym.ctypes.data, pc.ctypes.data, m["K"], z, dm.ctypes.data, gain_step2,
+                          Ls.ctypes.data, Ss.ctypes.data, data.ctypes.data, m["bcap"],
+                          flags.ctypes.data)
+    assert rc == 0
+    return dict(L=Ls[:z].astype(np.uint64), S=Ss[:z + 1].copy(), data=data, flags=int(flags[0]))
 
 
 def test_transpose8_moves_bit_8k_plus_j_to_8j_plus_k():
@@ -100,6 +126,13 @@ def _compare(L, rs, work, dims, box, qt_eff, gain_step2, hb, erres, precision, g
     assert np.array_equal(m["S"], Sr)
     n = int(Lr[-1]) if Z else 0
     assert bytes(m["data"][:n]) == data_r[:n]
+    if K:
+        # the coder in two halves gives the same truncation lengths, slopes and bytes
+        sp = run_split(L, m, gain_step2, precision)
+        assert sp["flags"] == m["flags"]
+        assert np.array_equal(sp["L"], m["L"])
+        assert np.array_equal(sp["S"], m["S"])
+        assert bytes(sp["data"][:n + 16]) == bytes(m["data"][:n + 16])
     if golden is not None:
         gK, gZ, gL, gS, gdata = golden
         assert (m["K"], m["Z"]) == (gK, gZ)
