@@ -345,7 +345,7 @@ int t1emu_mq_split(const uint8_t *symbols, const uint32_t *pass_count, int K, in
   std::vector<uint32_t> pairs((size_t)nchunks * 16 + 16, 0);
   std::vector<uint16_t> snapA(kMaxPasses, 0);
   std::vector<uint64_t> snaps(2 * kMaxPasses + 16, 0);
-  uint32_t slot[dev::kCtxTotal];
+  MqSlot slot[dev::kCtxTotal];
   MqProducer P;
   mq_producer_init(P, arena.data(), pass_count, Z, dev::h_mq_states, slot, 1);
   for (uint32_t k = 0; k < nchunks; ++k)
@@ -356,6 +356,7 @@ int t1emu_mq_split(const uint8_t *symbols, const uint32_t *pass_count, int K, in
   for (uint32_t k = 0; k < nchunks; ++k)
     if (!mq_consume_chunk(Q, pairs.data() + (size_t)k * 16, 1, snaps.data())) return -1;
   mq_consumer_passes(Q, snaps.data());
+  mq_consumer_overflow(Q);
   for (int p = 0; p < Z; ++p) snaps[2 * p] |= (uint64_t)snapA[p] << 48;
   uint32_t smin, smax;
   t1_finish(Q.e, Q.bo, K, Z, snaps.data(), dmse, gain_step2, L, S, &smin, &smax);

@@ -133,6 +133,17 @@ struct PinnedBuf {
   }
 };
 
+// Page-locked tier-1 result buffer of each device, shared by the process's codecs (a codec's
+// own would be allocated, slowly, by every new codec); held under its mutex while a call copies
+// its results in and reads them out.  Kept until the process ends.
+std::mutex g_t1host_mutex[64];
+PinnedBuf *g_t1host[64] = {};
+
+PinnedBuf &t1host_of(int dev) {
+  if (!g_t1host[dev]) g_t1host[dev] = new PinnedBuf();   // under g_t1host_mutex[dev]
+  return *g_t1host[dev];
+}
+
 // Host copy of the tier-1 results of one call: per codeblock K, Z, truncation lengths, slopes
 // and flags, per slope slot the slope range, per unit the field statistics.  Lives in the
 // caller's page-locked buffer, or in `fallback` when no page-locked memory can be had.
@@ -189,7 +200,6 @@ struct DeviceState {
   bool dump_set = false, ddump_set = false;
   bwc_b200_stage_dump dump{};
   bwc_b200_decode_dump ddump{};
-  PinnedBuf t1host;          // page-locked home of the tier-1 results on the host
   double timings[12] = {};   // stage times (ms); [8] tier-1 symbols coded (millions),
                              // [9] tier-1 context modelling (ms, part of [3]), [10] the MQ
                              // launches' device time summed (ms), [11] MQ launches
@@ -734,8 +744,10 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
 
   // tier-1 summary to the host
   cudaEventRecord(dv->ev[2], s);
+  if (dv->device < 0 || dv->device >= 64) return 0;
+  std::unique_lock<std::mutex> t1lock(g_t1host_mutex[dv->device]);
   T1Host h;
-  h.layout(dv->t1host, ncb, ntiles, nu);
+  h.layout(t1host_of(dv->device), ncb, ntiles, nu);
   uint8_t *const hK = h.K, *const hZ = h.Z;
   uint32_t *const hL = h.L, *const hflags = h.flags, *const hslopes = h.slopes;
   uint16_t *const hS = h.S;
@@ -803,6 +815,7 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
     eng->tiles[t].slope_min = (uint16_t)hslopes[2 * t];
     eng->tiles[t].slope_max = (uint16_t)hslopes[2 * t + 1];
   }
+  t1lock.unlock();   // the tier-1 results are in the codec's own structures now
 
   // tier 2 on the host, tile by tile
   const auto h0 = std::chrono::steady_clock::now();

@@ -815,7 +815,7 @@ __global__ void __launch_bounds__(64) t1_mq_split_kernel(const CbDev *__restrict
                                                          T1EncOut out, uint32_t lanes,
                                                          const uint32_t *__restrict__ order) {
   __shared__ uint32_t tbl[94];
-  __shared__ uint32_t slots[dev::kCtxTotal][32];
+  __shared__ t1::MqSlot slots[dev::kCtxTotal][32];
   __shared__ uint32_t ring[kMqRing][16][32];
   __shared__ uint16_t snapA[kMaxPasses][32];
   for (int i = threadIdx.x; i < 94; i += blockDim.x) tbl[i] = dev::c_mq_states[i];
@@ -862,7 +862,10 @@ __global__ void __launch_bounds__(64) t1_mq_split_kernel(const CbDev *__restrict
     if (active) t1::mq_consume_chunk(Q, &ring[r][0][lane], 32, snaps);
     named_arrive(1 + kMqRing + r);
   }
-  if (active) t1::mq_consumer_passes(Q, snaps);
+  if (active) {
+    t1::mq_consumer_passes(Q, snaps);
+    t1::mq_consumer_overflow(Q);
+  }
   named_sync(15);
   if (!active) return;
   for (int p = 0; p < Z; ++p) snaps[2 * p] |= (uint64_t)snapA[p][lane] << 48;

@@ -197,26 +197,45 @@ T1_HD uint32_t stream_chunks(const uint32_t *pcount, int Z) {
   return n;
 }
 
+// A context slot of the interval half: the context's state entry and the entries of its two
+// successor states (after a more and a less probable symbol), so that a decision's next state
+// is a select, not a table read; the successors of a new state are read from the table once,
+// when the state is stored, a decision before they can be needed.
+struct MqSlot {
+  uint32_t cur, mps, lps, pad;
+};
+
+T1_HD MqSlot mq_slot_of(uint32_t ent, const uint32_t *tbl) {
+  return MqSlot{ent, tbl[(ent >> 17) & 0x7F], tbl[(ent >> 24) & 0x7F], 0u};
+}
+
 // The interval half of mq_code_one: A and the context states; returns the decision's pair.
-T1_HD uint32_t mq_interval_one(uint32_t &A, uint32_t sym, uint32_t &ent, uint32_t nk,
-                               uint32_t nent, uint32_t *slot, int stride, const uint32_t *tbl) {
+//   ent: the slot of the decision's context; on return the slot of the next decision's context
+//   (nk == k and the state moved ? the new slot : nent, read before this decision)
+T1_HD uint32_t mq_interval_one(uint32_t &A, uint32_t sym, MqSlot &ent, uint32_t nk,
+                               const MqSlot &nent, MqSlot *slot, int stride,
+                               const uint32_t *tbl) {
   const uint32_t k = sym >> 1;
-  const uint32_t em = tbl[(ent >> 17) & 0x7F], el = tbl[(ent >> 24) & 0x7F];
-  const uint32_t qe = ent & 0xFFFFu;
+  const uint32_t qe = ent.cur & 0xFFFFu;
   const uint32_t A1 = A - qe;
-  const bool is_mps = ((sym ^ (ent >> 16)) & 1u) == 0u;
+  const bool is_mps = ((sym ^ (ent.cur >> 16)) & 1u) == 0u;
   const bool keep = is_mps != (A1 < qe);
   const uint32_t An = keep ? A1 : qe;
   const bool ren = An < 0x8000u;
-  const uint32_t ne = is_mps ? em : el;
-  if (ren) slot[k * stride] = ne;
-  ent = (ren && nk == k) ? ne : nent;
+  const MqSlot ns = mq_slot_of(is_mps ? ent.mps : ent.lps, tbl);
+  if (ren) slot[k * stride] = ns;
+  const bool fwd = ren && nk == k;
+  ent.cur = fwd ? ns.cur : nent.cur;
+  ent.mps = fwd ? ns.mps : nent.mps;
+  ent.lps = fwd ? ns.lps : nent.lps;
   const int sh = clz32(An) - 16;
   A = An << sh;
   return (keep ? qe : 0u) | ((uint32_t)sh << 16);
 }
 
-// The register half of mq_code_one: C, the shift counter and the byte transfers.
+// The register half of mq_code_one: C, the shift counter and the byte transfers.  A transfer
+// whose byte falls at or beyond the capacity is not stored; mq_consumer_passes' caller raises
+// the overflow flag from the final byte count instead of per decision (the count only grows).
 T1_HD void mq_register_one(MqState &e, ByteSink &bo, uint32_t pair) {
   const int sh = (int)(pair >> 16);
   e.C += pair & 0xFFFFu;
@@ -229,7 +248,6 @@ T1_HD void mq_register_one(MqState &e, ByteSink &bo, uint32_t pair) {
   const uint32_t T1 = e.T + carry;
   const uint32_t C1 = carry ? (e.C & 0x7FFFFFFu) : e.C;
   if (tr && (uint32_t)e.L < bo.cap) bo.out[e.L] = (uint8_t)T1;
-  if (tr && e.L >= 0 && (uint32_t)e.L >= bo.cap) bo.flags |= 1u;
   const bool ff = T1 == 0xFFu;
   const uint32_t T2 = (C1 >> (ff ? 20 : 19)) & 0xFFu;
   const uint32_t C2 = C1 & (ff ? 0xFFFFFu : 0x7FFFFu);
@@ -257,14 +275,15 @@ struct MqProducer {
   uint32_t A;
   const uint8_t *fetch;
   Chunk cur, nxt;
-  uint32_t *slot;   // 19 context slots at `stride` words
+  MqSlot *slot;   // 19 context slots at `stride` slots
   int stride;
   const uint32_t *tbl;
 };
 
 T1_HD void mq_producer_init(MqProducer &P, const uint8_t *src, const uint32_t *pcount, int Z,
-                            const uint32_t *tbl, uint32_t *slot, int stride) {
-  for (int k = 0; k < dev::kCtxTotal; ++k) slot[k * stride] = tbl[dev::mq_initial_state(k)];
+                            const uint32_t *tbl, MqSlot *slot, int stride) {
+  for (int k = 0; k < dev::kCtxTotal; ++k)
+    slot[k * stride] = mq_slot_of(tbl[dev::mq_initial_state(k)], tbl);
   walk_init(P.w, pcount, Z);
   P.A = 0x8000u;
   P.cur = load_chunk(src);
@@ -292,15 +311,15 @@ T1_HD uint32_t mq_produce_chunk(MqProducer &P, uint32_t *pairs, int pstride, uin
   P.cur = P.nxt;
   P.nxt = load_chunk(P.fetch);
   P.fetch += 16;
-  uint32_t *slot = P.slot;
+  MqSlot *slot = P.slot;
   const int stride = P.stride;
-  uint32_t ent = slot[(chunk_sym(c, 0) >> 1) * stride];
+  MqSlot ent = slot[(chunk_sym(c, 0) >> 1) * stride];
   if (P.w.left >= 16u) {
 #pragma unroll
     for (int jj = 0; jj < 16; ++jj) {
       const uint32_t sym = chunk_sym(c, jj);
       const uint32_t nk = (jj < 15) ? (chunk_sym(c, jj + 1) >> 1) : 0xFFu;
-      const uint32_t nent = (jj < 15) ? slot[nk * stride] : 0u;
+      const MqSlot nent = (jj < 15) ? slot[nk * stride] : MqSlot{0u, 0u, 0u, 0u};
       pairs[jj * pstride] = mq_interval_one(P.A, sym, ent, nk, nent, slot, stride, P.tbl);
     }
     P.w.left -= 16u;
@@ -309,7 +328,8 @@ T1_HD uint32_t mq_produce_chunk(MqProducer &P, uint32_t *pairs, int pstride, uin
   const uint32_t n = P.w.left;
   for (uint32_t jj = 0; jj < n; ++jj) {
     const uint32_t sym = (c.w[jj >> 2] >> (8 * (jj & 3))) & 0xFFu;
-    uint32_t nk = 0xFFu, nent = 0u;
+    uint32_t nk = 0xFFu;
+    MqSlot nent{0u, 0u, 0u, 0u};
     if (jj + 1 < n) {
       nk = ((c.w[(jj + 1) >> 2] >> (8 * ((jj + 1) & 3))) & 0xFFu) >> 1;
       nent = slot[nk * stride];
@@ -331,6 +351,12 @@ T1_HD void mq_consumer_init(MqConsumer &Q, const uint32_t *pcount, int Z, uint8_
   walk_init(Q.w, pcount, Z);
   Q.e = MqState{0x8000u, 0u, 0u, 12, -1};
   Q.bo = ByteSink{out, cap, 0u};
+}
+
+// The overflow flag of the transfers so far: some byte fell at or beyond the capacity exactly
+// when the byte count passed it (a transfer that finds L >= 0 counts one byte).
+T1_HD void mq_consumer_overflow(MqConsumer &Q) {
+  if (Q.e.L > 0 && (uint32_t)Q.e.L > Q.bo.cap) Q.bo.flags |= 1u;
 }
 
 // Passes that end before the next chunk: the register part of the coder state into snaps (A
