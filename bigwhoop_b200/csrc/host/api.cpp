@@ -653,7 +653,7 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
     total_samples += (uint64_t)allcb[i].w * ((allcb[i].h + 3) / 4) * 4 * allcb[i].d * allcb[i].nt;
   uint64_t arena = std::max<uint64_t>(1 << 20, total_samples * (kPrecBit + 1) * 9 / 8);
   if (!dv->pcount.ensure(ncb * kMaxPasses * 4) || !dv->poff.ensure(ncb * kMaxPasses * 8) ||
-      !dv->symused.ensure(16) || !dv->order.ensure(ncb * 4) || !dv->queue.ensure(16))
+      !dv->symused.ensure(16) || !dv->order.ensure(ncb * 4) || !dv->queue.ensure(32))
     return 0;
   {
     std::vector<uint32_t> order;
@@ -1203,7 +1203,7 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
       !bs->L.ensure(ncb * kMaxPasses * 4) || !bs->S.ensure(ncb * (kMaxPasses + 1) * 2) ||
       !bs->flags.ensure(ncb * 4) || !bs->slopes.ensure(8 * nslots) ||
       !bs->pcount.ensure(ncb * kMaxPasses * 4) || !bs->poff.ensure(ncb * kMaxPasses * 8) ||
-      !bs->symused.ensure(16) || !bs->order.ensure(ncb * 4) || !bs->queue.ensure(16))
+      !bs->symused.ensure(16) || !bs->order.ensure(ncb * 4) || !bs->queue.ensure(32))
     return 1;
   const std::vector<uint32_t> order = work_order(allcb, allsb, 0, ncb);
   // Inputs in pageable host memory go through a page-locked staging area: several host threads
