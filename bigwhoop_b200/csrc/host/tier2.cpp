@@ -649,14 +649,18 @@ void build_layer(Tile &tile, int q, Probe &pr) {
   });
 }
 
-// index (in the tables) of the codeblock's first record with S >= threshold, or ~0u
+// index (in the tables) of the codeblock's first record with S >= threshold, or ~0u: a
+// branch-free binary search (the records' S increase strictly; the outcome of each step is
+// data, not a predictable branch)
 inline uint32_t truncation_record(const Probe &pr, const ProbeCb &e, uint16_t threshold) {
-  uint32_t lo = 0, hi = e.rec_n;
   const uint16_t *s = pr.rec_s.data() + e.rec_off;
-  while (lo < hi) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (s[mid] >= threshold) hi = mid; else lo = mid + 1;
+  uint32_t n = e.rec_n, lo = 0;   // the answer lies in [lo, lo + n]
+  while (n > 1) {
+    const uint32_t half = n >> 1;
+    lo = (s[lo + half - 1] < threshold) ? lo + half : lo;
+    n -= half;
   }
+  if (n == 1 && s[lo] < threshold) ++lo;
   return (lo < e.rec_n) ? e.rec_off + lo : ~0u;
 }
 
