@@ -436,9 +436,9 @@ def run_ours(a):
 # and the decoder's total for one decompression of the workload's codestream.  The live part of
 # the roofline is the symbol count and each kernel's CUDA-event time in this run.
 T1_WARP_INSTR = {
-    "t1_model_kernel": (2.672, "profiles/t1_kernels_512cube_f64.md"),
-    "t1_mq_kernel": (6.170, "profiles/t1_kernels_512cube_f64.md"),
-    "t1_decode_kernel": (112.73e9, "profiles/t1_kernels_512cube_f64.md"),
+    "t1_model_kernel": (2.673, "profiles/t1_kernels_512cube_f64.md"),
+    "t1_mq_kernel": (6.010, "profiles/t1_kernels_512cube_f64.md"),
+    "t1_decode_kernel": (122.55e9, "profiles/t1_kernels_512cube_f64.md"),
 }
 SMS = 148
 
