@@ -85,7 +85,7 @@ int    bwc_b200_subband_steps(bwc_codec *const codec, uint8 const param, uint64 
 int    bwc_b200_parsed_codeblock(bwc_codec *const codec, uint8 const param, uint64 const c,
                                  int64 *meta3, uint64 *L);
 /* the same for codeblock c of parameter `param` in tile `tile` of a multi-tile codestream
- * (bwc_create_decompression parses those; bwc_decompress decodes single-tile ones only).  No
+ * (bwc_create_decompression parses those).  No
  * counterpart in the reference. */
 int    bwc_b200_parsed_codeblock_of_tile(bwc_codec *const codec, uint32 const tile,
                                          uint8 const param, uint64 const c, int64 *meta3,
