@@ -235,8 +235,11 @@ def decompress(codec, stream, precision="double"):
 
 def set_transform_tuning(mode=1, ctas=0, precision="double"):
     """Forward transform path for levels that transform x, y and z: 0 = 3D tile kernel only,
-    1 = z-streaming kernel where it pays (default), 2 = z-streaming kernel wherever x, y, z >= 8;
-    ``ctas`` > 0 fixes the streaming kernel's grid.  Coefficients are identical."""
+    1 = the bulk-copy z-streaming kernel wherever rows start on 16-byte boundaries, else the
+    register z-streaming kernel where it pays (default), 2 = as 1 with the register kernel
+    wherever x, y, z >= 8, 3 = the register z-streaming kernel wherever x, y, z >= 8 (never the
+    bulk-copy one); ``ctas`` > 0 fixes the streaming kernels' grids.  Coefficients are
+    identical."""
     load(precision).bwc_b200_set_transform_tuning(int(mode), int(ctas))
 
 

@@ -152,13 +152,14 @@ struct T1Host {
   uint32_t *L = nullptr, *flags = nullptr, *slopes = nullptr;
   uint16_t *S = nullptr;
   bwc_float *stats = nullptr;
+  uint32_t *fault = nullptr;   // the transform's fault word
   std::vector<uint8_t> fallback;
   bool layout(PinnedBuf &pb, uint64_t ncb, uint64_t nslots, uint64_t nu) {
     auto al = [](uint64_t x) { return (x + 15) & ~15ull; };
     const uint64_t oZ = al(ncb), oL = oZ + al(ncb), oF = oL + al(ncb * kMaxPasses * 4),
                    oSl = oF + al(ncb * 4), oS = oSl + al(8 * nslots),
                    oSt = oS + al(ncb * (kMaxPasses + 1) * 2),
-                   end = oSt + al(4 * sizeof(bwc_float) * nu);
+                   oFa = oSt + al(4 * sizeof(bwc_float) * nu), end = oFa + 16;
     uint8_t *base = nullptr;
     if (pb.ensure(end)) {
       base = static_cast<uint8_t *>(pb.p);
@@ -174,6 +175,7 @@ struct T1Host {
     slopes = reinterpret_cast<uint32_t *>(base + oSl);
     S = reinterpret_cast<uint16_t *>(base + oS);
     stats = reinterpret_cast<bwc_float *>(base + oSt);
+    fault = reinterpret_cast<uint32_t *>(base + oFa);
     return true;
   }
 };
@@ -759,8 +761,15 @@ static size_t compress_impl(bwc_codec *codec, bwc_stream *stream) {
   cudaMemcpyAsync(hflags, dv->flags.p, ncb * 4, cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hslopes, dv->slopes.p, 8 * ntiles, cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hstats, dv->stats.p, 4 * sizeof(bwc_float) * nu, cudaMemcpyDeviceToHost, s);
+  dwt_fault_download(h.fault, s);
   cudaEventRecord(dv->ev[3], s);
   if (!cuda_ok(cudaStreamSynchronize(s), "tier-1 download")) return 0;
+  if (*h.fault) {
+    warn("o##########################################################o\n"
+         "| ERROR: the wavelet transform's input copies timed out    |\n"
+         "o##########################################################o\n");
+    return 0;
+  }
 
   for (uint64_t i = 0; i < ncb; ++i) {
     if (hflags[i] & (1u | 16u)) {
@@ -1339,6 +1348,7 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
     if (g.first == sig) exec = g.second;
   if (!exec) {
     cudaGraph_t graph = nullptr;
+    dwt_setup();
     if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
       enqueue_transforms();
       if (cudaStreamEndCapture(s, &graph) == cudaSuccess && graph &&
@@ -1415,7 +1425,14 @@ static uchar compress_batch_impl(bwc_codec *const *codecs, bwc_stream *const *st
   cudaMemcpyAsync(hflags, bs->flags.p, ncb * 4, cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hslopes, bs->slopes.p, 8 * nslots, cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hstats, bs->stats.p, 4 * sizeof(bwc_float) * nu, cudaMemcpyDeviceToHost, s);
+  dwt_fault_download(h.fault, s);
   if (!cuda_ok(cudaStreamSynchronize(s), "batch tier-1 download")) return 1;
+  if (*h.fault) {
+    warn("o##########################################################o\n"
+         "| ERROR: the wavelet transform's input copies timed out    |\n"
+         "o##########################################################o\n");
+    return 1;
+  }
   for (uint64_t c = 0; c < ncb; ++c)
     if (hflags[c] & (1u | 16u)) {
       warn("o##########################################################o\n"

@@ -21,6 +21,9 @@
 #include <algorithm>
 #include <cstdio>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "device_common.cuh"
 
 namespace bwcb {
@@ -624,6 +627,421 @@ __global__ void __launch_bounds__(kZThreads, 1)
   }
 }
 
+// ---- z-streaming forward levels staged by TMA tensor copies ---------------------------------
+//
+// dwt_tma_fwd_kernel: 40 x 40 (x, y) tiles -- a 32 x 32 interior with a 4-sample reflected halo
+// -- streamed along z in batches of 8 planes, one CTA of 16 warps per SM.  A batch arrives in
+// shared memory by TMA tensor copies completing on the batch slot's mbarrier: the interior
+// columns as 128-byte-wide boxes with the 128-byte swizzle (16-byte chunk c of tile row y at
+// chunk c ^ (y & 7), so row-wise and column-wise accesses are both conflict-free), and the two
+// 4-column halos as narrow boxes.  A batch inside the region's z extent is one 3D box per column
+// group (4 copies in FP64); a batch that reaches past either z end is loaded plane by plane with
+// the reflected plane index.  Rows and columns outside the region (filled with zeros by TMA) are
+// read from their reflected places: the thread that lifts a row reads the reflected source row,
+// and the x-halo samples past the region's ends from the reflected place in that row.  Two batch
+// slots: while a batch is lifted, the next one is in flight.  Per batch, one thread per tile row
+// lifts the whole row along x in registers, one thread per interior column lifts the column
+// along y, and each thread advances the z window of two interior points through the batch's
+// planes and stores the finished coefficients in their de-interleaved places.  No shuffles:
+// every line sits in one thread's registers.  The arithmetic of every sample is the tile
+// kernel's line lifting (x, then y, then z), so the coefficients are bit-identical.  TMA wants
+// 16-byte aligned rows (even widths in FP64, multiples of 4 in FP32); other fields take the
+// kernels above.
+constexpr int kBT = 40, kBH = 4, kBI = kBT - 2 * kBH;   // tile extent (x and y), halo, interior
+constexpr int kBPl = 8;                                  // planes per batch
+constexpr int kBThreads = 512;                           // 16 warps
+constexpr int kES = (int)sizeof(bwc_float);
+constexpr int kIB = 128 / kES;                   // samples per interior box row (128 bytes)
+constexpr int kNIB = kBI / kIB;                  // interior boxes (FP64 2, FP32 1)
+constexpr int kPerChunk = 16 / kES;              // samples per 16-byte chunk
+constexpr int kHW = kBH;                         // halo box width
+constexpr uint32_t kIBPlane = kBT * 128;                     // bytes of an interior box plane
+constexpr uint32_t kIBBytes = kBPl * kIBPlane;               // ... of an interior box
+constexpr uint32_t kHPlane = kBT * kHW * kES;                // ... of a halo box plane
+constexpr uint32_t kHBytes = kBPl * kHPlane;                 // ... of a halo box
+constexpr uint32_t kHaloL = kNIB * kIBBytes, kHaloR = kHaloL + kHBytes;
+constexpr uint32_t kSlotBytes = kHaloR + kHBytes;            // one batch slot
+constexpr size_t kBSmem = 1024 + 2 * (size_t)kSlotBytes + 128;   // + alignment, barriers
+constexpr uint32_t kBSpin = 1u << 22;   // mbarrier polls before a batch is given up
+static_assert(kSlotBytes % 1024 == 0 && kIBBytes % 1024 == 0 && kIBPlane % 1024 == 0,
+              "swizzled boxes start on 1024-byte boundaries");
+static_assert(kHaloL % 128 == 0 && kHPlane % 128 == 0, "halo boxes start on 128-byte boundaries");
+static_assert(kBThreads >= kBPl * kBT, "one thread per row of a batch");
+static_assert(kBThreads / 32 >= kBPl && kBI == 32, "one warp per plane in the y pass");
+static_assert(kBPl * (kNIB + 2) <= 32, "one warp issues a batch's per-plane copies");
+
+struct BulkGeom {
+  uint32_t ex, ey, ez;      // region extents
+  uint32_t lx, ly, lz;      // low-band sizes, (e + 1) / 2
+  uint32_t ntx, nty, nbat;  // tiles along x and y, 8-plane output batches along z
+  uint32_t sy, sz;          // buffer strides within a time slice (< 2^31 samples)
+  uint64_t st;              // time-slice stride
+  uint32_t units;           // ntx * nty * time slices * nbat (< 2^31)
+};
+
+// tensor maps over the level region (x, y, z, t): interior and halo boxes, 8 planes deep and
+// one plane deep
+struct TmaMaps {
+  CUtensorMap in8, halo8, in1, halo1;
+};
+
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<double> {
+  using type = double2;
+};
+template <>
+struct Vec16<float> {
+  using type = float4;
+};
+using v16_t = Vec16<bwc_float>::type;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// bounded wait for the phase of the given parity; false when it did not complete
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (uint32_t it = 0; it < kBSpin; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+// TMA tensor copy of the box at (x, y, z, t) into shared memory, completing on `bar`
+__device__ __forceinline__ void tma_load(uint32_t dst, const CUtensorMap *map, int x, int y, int z,
+                                         int t, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];\n" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(t), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// byte offset in a slot of tile sample i (0..39) of row y of plane p
+__device__ __forceinline__ uint32_t tma_off(int p, int y, int i) {
+  const uint32_t r = (uint32_t)(p * kBT + y);
+  if (i < kBH) return kHaloL + (r * kHW + (uint32_t)i) * kES;
+  if (i >= kBH + kBI) return kHaloR + (r * kHW + (uint32_t)(i - kBH - kBI)) * kES;
+  const int xi = i - kBH, bx = xi / kIB, e = xi % kIB;
+  const uint32_t c = (uint32_t)(e / kPerChunk) ^ (uint32_t)(y & 7);
+  return (uint32_t)bx * kIBBytes + r * 128 + c * 16 + (uint32_t)(e % kPerChunk) * kES;
+}
+
+// A CTA's units form runs (consecutive output batches of one tile column); a run's fed planes
+// are zc0 - 5 (odd) .. (zc1 + 3) & ~1 (even): four context planes on either side of its output
+// planes [zc0, zc1), and (odd, even) plane pairs inside every batch of 8.
+struct BulkRun {
+  uint32_t u, n;   // first unit, units
+  int nb;          // batches fed
+};
+__device__ __forceinline__ BulkRun bulk_run(const BulkGeom &g, uint32_t u, uint32_t uend) {
+  BulkRun r;
+  r.u = u;
+  if (u >= uend) {
+    r.n = 0;
+    r.nb = 0;
+    return r;
+  }
+  const uint32_t b0 = u % g.nbat;
+  r.n = min(uend - u, g.nbat - b0);
+  const int zc0 = kBPl * (int)b0, zc1 = min(kBPl * (int)(b0 + r.n), (int)g.ez);
+  r.nb = ((((zc1 + 3) & ~1) - (zc0 - 5) + 1) + kBPl - 1) / kBPl;
+  return r;
+}
+
+// batch k of a run, as every thread of the CTA reads it from shared memory
+struct BulkBatch {
+  uint32_t bx, by, t;
+  int zc0, zc1;   // output planes of the run
+  int jb, np;     // first fed plane, planes (even, <= 8); np = 0: no batch
+  int whole;      // planes jb .. jb + np - 1 lie inside the region: one 3D box per column group
+};
+__device__ __forceinline__ BulkBatch bulk_batch(const BulkGeom &g, const BulkRun &r, int k) {
+  BulkBatch b;
+  b.np = 0;
+  if (r.n == 0) return b;
+  const uint32_t tile = r.u / g.nbat, b0 = r.u % g.nbat;
+  b.bx = tile % g.ntx;
+  const uint32_t rest = tile / g.ntx;
+  b.by = rest % g.nty;
+  b.t = rest / g.nty;
+  b.zc0 = kBPl * (int)b0;
+  b.zc1 = min(kBPl * (int)(b0 + r.n), (int)g.ez);
+  b.jb = b.zc0 - 5 + kBPl * k;
+  b.np = min(kBPl, ((b.zc1 + 3) & ~1) + 1 - b.jb);
+  b.whole = b.jb >= 0 && b.jb + b.np <= (int)g.ez;
+  return b;
+}
+// bytes one batch brings into its slot (boxes count whole, zero-filled parts included)
+__device__ __forceinline__ uint32_t bulk_bytes(const BulkBatch &b) {
+  return b.whole ? kSlotBytes : (uint32_t)b.np * (kNIB * kIBPlane + 2 * kHPlane);
+}
+
+__global__ void __launch_bounds__(kBThreads, 1)
+    dwt_tma_fwd_kernel(bwc_float *__restrict__ dst, BulkGeom g, const __grid_constant__ TmaMaps maps,
+                       uint32_t *fault) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // swizzled boxes want 1024-byte aligned destinations
+  unsigned char *sm = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sm + 2 * (size_t)kSlotBytes);
+  BulkBatch *desc = reinterpret_cast<BulkBatch *>(bar + 2);   // the batch in each slot
+  volatile int &s_abort = *reinterpret_cast<int *>(desc + 2);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  const uint32_t ubeg = (uint32_t)((uint64_t)blockIdx.x * g.units / gridDim.x);
+  const uint32_t uend = (uint32_t)((uint64_t)(blockIdx.x + 1) * g.units / gridDim.x);
+  // the posting thread (the first of the last warp, idle in the x and y passes) walks the
+  // batch sequence one batch ahead of the issue: (arun, ak) is the next batch to post
+  BulkRun arun = bulk_run(g, ubeg, uend);
+  int ak = 0;
+  auto advance = [&]() {
+    if (++ak >= arun.nb) {
+      arun = bulk_run(g, arun.u + arun.n, uend);
+      ak = 0;
+    }
+  };
+  // the posting thread writes a slot's batch and arrives on the slot's barrier with the batch's
+  // bytes (the one arrival of each phase) before any copy of it is issued
+  auto post = [&](uint32_t q) {
+    const BulkBatch b = bulk_batch(g, arun, ak);
+    desc[q & 1] = b;
+    if (b.np) {
+      advance();
+      mbar_arrive_tx(&bar[q & 1], bulk_bytes(b));
+    }
+  };
+  if (tid == kBThreads - 32) {
+    asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&maps.in8))
+                 : "memory");
+    asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&maps.halo8))
+                 : "memory");
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    post(0);
+    post(1);
+  }
+  __syncthreads();
+
+  // warp 0 issues the copies of the batch described in slot q & 1
+  auto issue = [&](uint32_t q) {
+    const BulkBatch b = desc[q & 1];
+    if (warp != 0 || b.np == 0) return;
+    const uint32_t base = smem_u32(sm) + (q & 1) * kSlotBytes;
+    const int xb = (int)(b.bx * kBI), yb = (int)(b.by * kBI) - kBH;
+    // copy `lane`: box kind k (0 .. kNIB-1 interior, kNIB left halo, kNIB+1 right halo), plane p
+    const int k = lane % (kNIB + 2), p = lane / (kNIB + 2);
+    const int x = (k < kNIB) ? xb + k * kIB : (k == kNIB ? xb - kBH : xb + kBI);
+    const uint32_t kb = (k < kNIB) ? (uint32_t)k * kIBBytes : (k == kNIB ? kHaloL : kHaloR);
+    if (b.whole) {
+      if (p == 0)
+        tma_load(base + kb, (k < kNIB) ? &maps.in8 : &maps.halo8, x, yb, b.jb, (int)b.t, &bar[q & 1]);
+    } else if (p < b.np) {
+      const uint32_t pb = (k < kNIB) ? kIBPlane : kHPlane;
+      tma_load(base + kb + (uint32_t)p * pb, (k < kNIB) ? &maps.in1 : &maps.halo1, x, yb,
+               reflect(b.jb + p, (int)g.ez), (int)b.t, &bar[q & 1]);
+    }
+  };
+  issue(0);
+  issue(1);
+
+  // y- and z-pass column of this lane (column 4 + lane): sample of row y at
+  // cb + (c16 ^ 16 (y & 7)) + 128 y of its plane
+  const uint32_t cb = (uint32_t)(lane / kIB) * kIBBytes + (uint32_t)(lane % kPerChunk) * kES;
+  const uint32_t c16 = (uint32_t)((lane % kIB) / kPerChunk) * 16;
+
+  // z windows of this thread's two interior points (column 4 + lane, rows 4 + warp and
+  // 20 + warp): w5 = plane j-5 after step 3, w4 = j-4 after step 2, w3 = j-3 after step 1,
+  // w2 = j-2 as lifted along x and y
+  bwc_float w5[2], w4[2], w3[2], w2[2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i) w5[i] = w4[i] = w3[i] = w2[i] = (bwc_float)0;
+
+  uint32_t q = 0;
+  for (;; ++q) {
+    const BulkBatch b = desc[q & 1];
+    if (b.np == 0) break;
+    unsigned char *slot = sm + (q & 1) * kSlotBytes;
+    const bool arrived = mbar_wait(&bar[q & 1], (q >> 1) & 1);
+    if (!arrived) s_abort = 1;
+    const int x0 = (int)(b.bx * kBI) - kBH, y0 = (int)(b.by * kBI) - kBH;
+    const bool yedge = y0 < 0 || y0 + kBT > (int)g.ey;
+
+    // rows just outside the region (4 on either side) first take their reflected source row;
+    // rows further out feed no stored sample and keep the zeros TMA wrote
+    const int p = tid / kBT, y = tid % kBT;
+    const bool xrow = tid < kBT * b.np && arrived;
+    if (yedge) {
+      const int yy = y0 + y;
+      if (xrow && ((yy < 0 && yy >= -kBH) || (yy >= (int)g.ey && yy < (int)g.ey + kBH))) {
+        const int ys = reflect(yy, (int)g.ey) - y0;
+        const uint32_t rd = (uint32_t)(p * kBT + y), rs = (uint32_t)(p * kBT + ys);
+#pragma unroll
+        for (int i = 0; i < kHW; i += kPerChunk) {
+          *reinterpret_cast<v16_t *>(slot + kHaloL + (rd * kHW + i) * kES) =
+              *reinterpret_cast<const v16_t *>(slot + kHaloL + (rs * kHW + i) * kES);
+          *reinterpret_cast<v16_t *>(slot + kHaloR + (rd * kHW + i) * kES) =
+              *reinterpret_cast<const v16_t *>(slot + kHaloR + (rs * kHW + i) * kES);
+        }
+#pragma unroll
+        for (int c = 0; c < kBI / kPerChunk; ++c) {
+          const uint32_t bo = (uint32_t)(c / (kIB / kPerChunk)) * kIBBytes;
+          const uint32_t cc = (uint32_t)(c % (kIB / kPerChunk));
+          *reinterpret_cast<v16_t *>(slot + bo + rd * 128 + ((cc ^ (uint32_t)(y & 7)) * 16)) =
+              *reinterpret_cast<const v16_t *>(slot + bo + rs * 128 + ((cc ^ (uint32_t)(ys & 7)) * 16));
+        }
+      }
+      __syncthreads();
+    }
+
+    // x pass: one row per thread; x-halo samples just past the region's ends come from their
+    // reflected place in the row (further out: zeros, feeding no stored sample)
+    if (xrow) {
+      bwc_float v[kBT];
+      const uint32_t r = (uint32_t)(p * kBT + y);
+#pragma unroll
+      for (int i = 0; i < kHW; i += kPerChunk) {
+        const v16_t a = *reinterpret_cast<const v16_t *>(slot + kHaloL + (r * kHW + i) * kES);
+        const v16_t c = *reinterpret_cast<const v16_t *>(slot + kHaloR + (r * kHW + i) * kES);
+#pragma unroll
+        for (int e = 0; e < kPerChunk; ++e) {
+          v[i + e] = reinterpret_cast<const bwc_float *>(&a)[e];
+          v[kBH + kBI + i + e] = reinterpret_cast<const bwc_float *>(&c)[e];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < kBI / kPerChunk; ++c) {
+        const uint32_t o = (uint32_t)(c / (kIB / kPerChunk)) * kIBBytes + r * 128 +
+                           ((uint32_t)(c % (kIB / kPerChunk)) ^ (uint32_t)(y & 7)) * 16;
+        const v16_t a = *reinterpret_cast<const v16_t *>(slot + o);
+#pragma unroll
+        for (int e = 0; e < kPerChunk; ++e)
+          v[kBH + c * kPerChunk + e] = reinterpret_cast<const bwc_float *>(&a)[e];
+      }
+      if (x0 < 0) {   // x = -4 .. -1 reflect to 4 .. 1
+#pragma unroll
+        for (int i = 0; i < kBH; ++i) v[i] = v[2 * kBH - i];
+      }
+      if (x0 + kBT > (int)g.ex) {
+#pragma unroll
+        for (int i = kBH + 1; i < kBT; ++i) {
+          const int xx = x0 + i;
+          if (xx >= (int)g.ex && xx < (int)g.ex + kBH)
+            v[i] = *reinterpret_cast<const bwc_float *>(
+                slot + tma_off(p, y, reflect(xx, (int)g.ex) - x0));
+        }
+      }
+      lift_line<true, kBT>(v);
+#pragma unroll
+      for (int c = 0; c < kBI / kPerChunk; ++c) {
+        const uint32_t o = (uint32_t)(c / (kIB / kPerChunk)) * kIBBytes + r * 128 +
+                           ((uint32_t)(c % (kIB / kPerChunk)) ^ (uint32_t)(y & 7)) * 16;
+        v16_t a;
+#pragma unroll
+        for (int e = 0; e < kPerChunk; ++e)
+          reinterpret_cast<bwc_float *>(&a)[e] = v[kBH + c * kPerChunk + e];
+        *reinterpret_cast<v16_t *>(slot + o) = a;
+      }
+    }
+    __syncthreads();
+    if (s_abort) break;
+    // the batch after next goes into this slot's record now (every thread holds this batch's
+    // record and has passed this slot's wait); a warp the y pass leaves idle writes it
+    if (tid == kBThreads - 32) post(q + 2);
+
+    // y pass: one interior column per thread, one warp per plane
+    if (warp < b.np) {
+      unsigned char *col = slot + cb + (uint32_t)warp * kIBPlane;
+      bwc_float v[kBT];
+#pragma unroll
+      for (int i = 0; i < kBT; ++i)
+        v[i] = *reinterpret_cast<const bwc_float *>(col + (c16 ^ (16u * (i & 7))) + (uint32_t)i * 128);
+      lift_line<true, kBT>(v);
+#pragma unroll
+      for (int i = kBH; i < kBH + kBI; ++i)
+        *reinterpret_cast<bwc_float *>(col + (c16 ^ (16u * (i & 7))) + (uint32_t)i * 128) = v[i];
+    }
+    __syncthreads();
+
+    // z pass: (odd, even) plane pairs (jb + p, jb + p + 1); at even plane j the finished planes
+    // are j - 4 (low band) and j - 3 (high band)
+    {
+      bwc_float *dbase = dst + (uint64_t)b.t * g.st;
+      const uint32_t gx = b.bx * kBI + (uint32_t)lane;
+      const uint32_t mx = (gx & 1) ? g.lx + (gx >> 1) : (gx >> 1);
+      uint32_t off[2];
+      bool in[2];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const uint32_t gy = b.by * kBI + (uint32_t)(warp + 16 * i);
+        const uint32_t my = (gy & 1) ? g.ly + (gy >> 1) : (gy >> 1);
+        off[i] = mx + my * g.sy;
+        in[i] = gx < g.ex && gy < g.ey;
+      }
+      // rows 4 + warp and 20 + warp share y & 7; all four plane pairs are lifted (past np, in a
+      // run's last batch, they read earlier planes and change only the window, which the next
+      // run's context planes refill before any of its stored samples)
+      const unsigned char *pt =
+          slot + cb + (c16 ^ (16u * ((kBH + warp) & 7))) + (uint32_t)(kBH + warp) * 128;
+#pragma unroll
+      for (int pp = 0; pp < kBPl; pp += 2) {
+        const int j = b.jb + pp + 1;
+        const int ze = j - 4, zo = j - 3;
+        const bool st_e = ze >= b.zc0 && ze < b.zc1, st_o = zo >= b.zc0 && zo < b.zc1;
+        const uint32_t de = (uint32_t)(ze >> 1) * g.sz;
+        const uint32_t dz = (g.lz + (uint32_t)(zo >> 1)) * g.sz;
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const bwc_float v1 =
+              *reinterpret_cast<const bwc_float *>(pt + (uint32_t)pp * kIBPlane + 16u * 128u * i);
+          const bwc_float v0 = *reinterpret_cast<const bwc_float *>(
+              pt + (uint32_t)(pp + 1) * kIBPlane + 16u * 128u * i);
+          const bwc_float a = dev::fadd(v1, dev::fmul(kAlpha, dev::fadd(w2[i], v0)));
+          const bwc_float c = dev::fadd(w2[i], dev::fmul(kBeta, dev::fadd(w3[i], a)));
+          const bwc_float o = dev::fmul(
+              kKappaH, dev::fadd(w3[i], dev::fmul(kGamma, dev::fadd(w4[i], c))));
+          const bwc_float e = dev::fmul(
+              kKappaL, dev::fadd(w4[i], dev::fmul(kDelta, dev::fadd(w5[i], o))));
+          if (in[i]) {
+            if (st_e) dbase[de + off[i]] = e;
+            if (st_o) dbase[dz + off[i]] = o;
+          }
+          w5[i] = o;
+          w4[i] = c;
+          w3[i] = a;
+          w2[i] = v0;
+        }
+      }
+    }
+    __syncthreads();   // the slot is consumed
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    issue(q + 2);
+  }
+  if (s_abort) {
+    if (tid == 0) atomicOr(fault, 1u);
+    // the other slot's copies may still be in flight: wait for them (bounded) before leaving
+    if (desc[(q + 1) & 1].np) mbar_wait(&bar[(q + 1) & 1], ((q + 1) >> 1) & 1);
+  }
+}
+
 // ---- one axis in place, any kernel ---------------------------------------------------------
 constexpr int kExt = 8;   // reflected samples on each side of a line (the liftings read at most 6)
 // LeGall 5/3 lifting constants of the reference (dwt.c:478-558): halving and (sum + 2) / 4
@@ -754,12 +1172,18 @@ void copy_region(const bwc_float *src, bwc_float *dst, const FieldDims &d, const
                                           d.width * d.height * d.depth);
 }
 
-// Transform path selection (bwc_b200_set_transform_tuning): 0 = tile kernel only, 1 = the
-// z-streaming kernel where x and y span at least 48 samples and the level gives every SM at
-// least 8 plane pairs, 2 = the z-streaming kernel wherever x, y and z are transformed and span
-// at least 8.  `ctas` > 0 fixes the streaming kernel's grid, 0 = one CTA per SM.
+// Transform path selection (bwc_b200_set_transform_tuning): 0 = tile kernel only; 1 = the
+// TMA streaming kernel wherever x, y and z are transformed, span at least 8 and rows start on
+// 16-byte boundaries, else the register streaming kernel where x and y span at least
+// 48 samples and the level gives every SM at least 8 plane pairs; 2 = as 1, with the register
+// streaming kernel wherever x, y and z are transformed and span at least 8; 3 = the register
+// streaming kernel wherever possible, never the TMA one.  `ctas` > 0 fixes the streaming
+// kernels' grids, 0 = one CTA per SM.
 int g_transform_mode = 1;
 int g_transform_ctas = 0;
+
+// set by a TMA streaming kernel whose batch did not arrive within its wait limit (never expected)
+__device__ uint32_t g_dwt_fault;
 
 int sm_count() {
   int dev = 0, n = 0;
@@ -769,8 +1193,96 @@ int sm_count() {
   return n;
 }
 
+uint32_t *fault_word() {
+  static uint32_t *addr[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return nullptr;
+  if (!addr[dev]) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_dwt_fault) != cudaSuccess) return nullptr;
+    addr[dev] = static_cast<uint32_t *>(p);
+  }
+  return addr[dev];
+}
+
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// a 4D tensor map over the level region of `src` with boxes of bw x 40 x bz x 1
+bool region_map(CUtensorMap *m, const bwc_float *src, const FieldDims &d, const uint64_t *e,
+                uint32_t bw, uint32_t bz, bool swizzle) {
+  auto enc = tensor_map_encoder();
+  if (!enc) return false;
+  const cuuint64_t dims[4] = {e[0], e[1], e[2], e[3]};
+  const cuuint64_t strides[3] = {d.width * sizeof(bwc_float), d.width * d.height * sizeof(bwc_float),
+                                 d.width * d.height * d.depth * sizeof(bwc_float)};
+  const cuuint32_t box[4] = {bw, (cuuint32_t)kBT, bz, 1};
+  const cuuint32_t unit[4] = {1, 1, 1, 1};
+  const CUresult r =
+      enc(m, sizeof(bwc_float) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+          4, const_cast<bwc_float *>(src), dims, strides, box, unit, CU_TENSOR_MAP_INTERLEAVE_NONE,
+          swizzle ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+bool tma_pass(const bwc_float *src, bwc_float *dst, const FieldDims &d, const uint64_t *e,
+              uint8_t on, cudaStream_t s) {
+  if (g_transform_mode == 0 || g_transform_mode == 3 || (on & 7) != 7) return false;
+  if (e[0] < 8 || e[1] < 8 || e[2] < 8) return false;
+  if (d.width * d.height * d.depth >= (1ull << 31)) return false;   // 32-bit slice offsets
+  const uint64_t es = sizeof(bwc_float);
+  if ((reinterpret_cast<uintptr_t>(src) % 16) || (d.width * es) % 16) return false;
+  uint32_t *fault = fault_word();
+  if (!fault) return false;
+  TmaMaps maps;
+  if (!region_map(&maps.in8, src, d, e, kIB, kBPl, true) ||
+      !region_map(&maps.halo8, src, d, e, kHW, kBPl, false) ||
+      !region_map(&maps.in1, src, d, e, kIB, 1, true) ||
+      !region_map(&maps.halo1, src, d, e, kHW, 1, false))
+    return false;
+  BulkGeom g;
+  g.ex = (uint32_t)e[0];
+  g.ey = (uint32_t)e[1];
+  g.ez = (uint32_t)e[2];
+  g.lx = (g.ex + 1) >> 1;
+  g.ly = (g.ey + 1) >> 1;
+  g.lz = (g.ez + 1) >> 1;
+  g.ntx = (g.ex + kBI - 1) / kBI;
+  g.nty = (g.ey + kBI - 1) / kBI;
+  g.nbat = (g.ez + kBPl - 1) / kBPl;
+  const uint64_t units = (uint64_t)g.ntx * g.nty * e[3] * g.nbat;
+  if (units >= (1ull << 31)) return false;
+  g.units = (uint32_t)units;
+  g.sy = (uint32_t)d.width;
+  g.sz = (uint32_t)(d.width * d.height);
+  g.st = d.width * d.height * d.depth;
+  static const int sms = sm_count();
+  const uint64_t grid =
+      std::min<uint64_t>(g.units, g_transform_ctas > 0 ? (uint64_t)g_transform_ctas : (uint64_t)sms);
+  cudaFuncSetAttribute(dwt_tma_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)kBSmem);
+  dwt_tma_fwd_kernel<<<(unsigned)grid, kBThreads, kBSmem, s>>>(dst, g, maps, fault);
+  return true;
+}
+
 bool stream_pass(const bwc_float *src, bwc_float *dst, const FieldDims &d, const uint64_t *e,
                  uint8_t on, cudaStream_t s) {
+  if (tma_pass(src, dst, d, e, on, s)) return true;
   if (g_transform_mode == 0 || (on & 7) != 7) return false;
   if (e[0] < 8 || e[1] < 8 || e[2] < 8) return false;
   if (d.width * d.height * d.depth >= (1ull << 31)) return false;   // 32-bit slice offsets
@@ -859,6 +1371,18 @@ bool uses_axis_path(const DwtPlan &plan) {
 
 }  // namespace
 
+void dwt_setup() { fault_word(); }
+
+void dwt_fault_download(uint32_t *host, cudaStream_t s) {
+  uint32_t *f = fault_word();
+  if (!f) {
+    *host = 0;
+    return;
+  }
+  cudaMemcpyAsync(host, f, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+  cudaMemsetAsync(f, 0, sizeof(uint32_t), s);
+}
+
 // Forward: `temp` holds the normalised field on entry; the coefficients end in `work`.  Even
 // levels go temp -> work and odd levels work -> temp, each level reading one buffer and writing
 // the other.  The high bands a level leaves in temp (odd levels) are copied back to work before
@@ -926,6 +1450,6 @@ void launch_dwt_inverse(bwc_float *work, bwc_float *temp, const FieldDims &dims,
 }  // namespace bwcb
 
 extern "C" void bwc_b200_set_transform_tuning(int mode, int ctas) {
-  bwcb::g_transform_mode = (mode < 0 || mode > 2) ? 1 : mode;
+  bwcb::g_transform_mode = (mode < 0 || mode > 3) ? 1 : mode;
   bwcb::g_transform_ctas = ctas > 0 ? ctas : 0;
 }

@@ -97,6 +97,11 @@ void launch_dwt_forward(bwc_float *work, bwc_float *temp, const FieldDims &dims,
                         const DwtPlan &plan, cudaStream_t s);
 void launch_dwt_inverse(bwc_float *work, bwc_float *temp, const FieldDims &dims,
                         const DwtPlan &plan, cudaStream_t s);
+// copies the transform's fault word (non-zero: a bulk-copy batch never arrived and the
+// coefficients are incomplete) to `host` (page-locked) on `s` and clears it
+void dwt_fault_download(uint32_t *host, cudaStream_t s);
+// looks up the fault word of the current device (call before capturing transforms in a graph)
+void dwt_setup();
 
 // t1_encode.cu: context modelling (one CTA per codeblock, max_cols = largest number of stripe
 // columns of a codeblock) followed by MQ coding (one thread per codeblock).
