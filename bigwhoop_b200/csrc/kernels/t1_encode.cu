@@ -1008,6 +1008,20 @@ void launch_t1_encode(const bwc_float *work, const CbDev *cbs, uint32_t ncb, con
   if (!ncb) return;
   const size_t smem = t1_model_smem(max_cols);
   const bool narrow = max_cols <= t1::kModelMaxCols;
+  // The modelling kernel is persistent and finishes only when its last CTA has run; the MQ
+  // launches of earlier phases run beside it for tens of milliseconds.  With the largest
+  // shared-memory carveout for all tier-1 kernels, an SM holding MQ CTAs still has room for its
+  // share of modelling CTAs, which otherwise waited for those MQ CTAs to end (tier-1 stage at
+  // 512^3 between 91 and 241 ms from call to call, by how the CTAs happened to be placed).
+  // (function attributes are per device: set on every call, like the dynamic smem size)
+  cudaFuncSetAttribute(t1_model_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       cudaSharedmemCarveoutMaxShared);
+  cudaFuncSetAttribute(t1_model_wide_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       cudaSharedmemCarveoutMaxShared);
+  cudaFuncSetAttribute(t1_mq_split_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       cudaSharedmemCarveoutMaxShared);
+  cudaFuncSetAttribute(t1_mq_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       cudaSharedmemCarveoutMaxShared);
   if (narrow)
     cudaFuncSetAttribute(t1_model_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   else
