@@ -1236,7 +1236,10 @@ bool region_map(CUtensorMap *m, const bwc_float *src, const FieldDims &d, const 
       enc(m, sizeof(bwc_float) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
           4, const_cast<bwc_float *>(src), dims, strides, box, unit, CU_TENSOR_MAP_INTERLEAVE_NONE,
           swizzle ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
-          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+          // interior rows are 128 bytes; a halo row is 32 (FP64) or 16 bytes, and a larger L2
+          // fetch for it read several times the field from DRAM (ncu at 256^3: 347 MB for 134)
+          swizzle ? CU_TENSOR_MAP_L2_PROMOTION_L2_128B : CU_TENSOR_MAP_L2_PROMOTION_NONE,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
 
