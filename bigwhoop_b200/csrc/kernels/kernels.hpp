@@ -110,10 +110,11 @@ size_t t1_model_smem(uint32_t max_cols);
 uint64_t t1_scratch_bytes(uint64_t ncols);
 // Each codeblock addresses its samples as work[base + x + y*sy + z*sz + t*st].  `order`
 // (optional, device) lists the codeblocks largest first: the MQ kernel's lanes take them in
-// that order, and with `queue` (one device counter per phase, room for eight, zeroed here) the modelling kernel runs
-// persistent and takes codeblocks from that work queue.  With an order, a queue and at least
-// 2048 codeblocks, the order is modelled in four phases on `s` and each phase's MQ kernel runs
-// on a side stream once its phase is modelled; `s` waits for them before it goes on.
+// that order, and with `queue` (one device counter per phase, room for eight, zeroed here) the
+// modelling kernel runs persistent and takes codeblocks from that work queue.  With an order, a
+// queue and at least 2048 codeblocks, the order is modelled in four phases on `s` (one CTA per
+// codeblock, in order) and each phase's MQ kernel runs on a side stream once its phase is
+// modelled; `s` waits for them before it goes on.
 // `after_model` (optional) is recorded on `s` after the (last) modelling launch; `mq_times`
 // (optional) receives the MQ launches' start and end events.
 // Timing events (created by the caller, timing enabled) that launch_t1_encode records around

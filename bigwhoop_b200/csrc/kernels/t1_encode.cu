@@ -1008,11 +1008,11 @@ void launch_t1_encode(const bwc_float *work, const CbDev *cbs, uint32_t ncb, con
   if (!ncb) return;
   const size_t smem = t1_model_smem(max_cols);
   const bool narrow = max_cols <= t1::kModelMaxCols;
-  // The modelling kernel is persistent and finishes only when its last CTA has run; the MQ
-  // launches of earlier phases run beside it for tens of milliseconds.  With the largest
-  // shared-memory carveout for all tier-1 kernels, an SM holding MQ CTAs still has room for its
-  // share of modelling CTAs, which otherwise waited for those MQ CTAs to end (tier-1 stage at
-  // 512^3 between 91 and 241 ms from call to call, by how the CTAs happened to be placed).
+  // The MQ launches of earlier phases run beside the later phases' modelling for tens of
+  // milliseconds.  With the largest shared-memory carveout for all tier-1 kernels, an SM holding
+  // MQ CTAs still has room for modelling CTAs, which otherwise waited for those MQ CTAs to end
+  // (tier-1 stage at 512^3 between 91 and 241 ms from call to call, by how the CTAs happened to
+  // be placed).
   // (function attributes are per device: set on every call, like the dynamic smem size)
   cudaFuncSetAttribute(t1_model_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                        cudaSharedmemCarveoutMaxShared);
@@ -1085,9 +1085,14 @@ void launch_t1_encode(const bwc_float *work, const CbDev *cbs, uint32_t ncb, con
       cudaEventCreateWithFlags(&modelled[i], cudaEventDisableTiming);
       cudaEventCreateWithFlags(&coded[i], cudaEventDisableTiming);
     }
+    // The phases' modelling launches take one CTA per codeblock (the order's slice, largest
+    // first) rather than a persistent grid on the work queue: a persistent kernel ends only when
+    // its last CTA has been scheduled, and beside the earlier phases' long MQ launches that CTA
+    // sometimes waited for them (512^3: modelling end 28 ms in most calls, up to 112 ms in some;
+    // one CTA per codeblock: 28-44 ms, tier-1 93-105 ms against 92-178 ms).
     for (int i = 0; i < kT1Phases; ++i) {
       const uint32_t n = bound[i + 1] - bound[i];
-      model(order + bound[i], n, queue + i);
+      model(order + bound[i], n, nullptr);
       cudaEventRecord(modelled[i], s);
       cudaStreamWaitEvent(side[i], modelled[i], 0);
       if (mq_times) cudaEventRecord(mq_times->start[i], side[i]);
