@@ -140,10 +140,13 @@ int    bwc_b200_last_batch_timings(double *out_ms, int n);
 int    bwc_b200_mq_lanes(uint32 ncb);
 
 /* Forward transform path for the levels that transform x, y and z: mode 0 = the 3D tile kernel
- * only, 1 (default) = the z-streaming kernel where x and y span at least 48 samples and the
- * level gives every SM at least 8 plane pairs, 2 = the z-streaming kernel wherever x, y and z
- * span at least 8.  ctas > 0 fixes the streaming kernel's grid (its CTAs split the level's
- * (tile, plane pair) units evenly), 0 = one CTA per SM.  Process-wide; set it between calls.
+ * only; 1 (default) = the TMA z-streaming kernel wherever x, y and z span at least 8 and rows
+ * start on 16-byte boundaries (even widths in FP64, multiples of 4 in FP32), else the register
+ * z-streaming kernel where x and y span at least 48 samples and the level gives every SM at
+ * least 8 plane pairs, else the tile kernel; 2 = as 1, with the register z-streaming kernel
+ * wherever x, y and z span at least 8; 3 = the register z-streaming kernel wherever x, y and z
+ * span at least 8, never the TMA one.  ctas > 0 fixes the streaming kernels' grids (their CTAs
+ * split the level's units evenly), 0 = one CTA per SM.  Process-wide; set it between calls.
  * All settings give bit-identical coefficients.  No counterpart in the reference API. */
 void   bwc_b200_set_transform_tuning(int mode, int ctas);
 
