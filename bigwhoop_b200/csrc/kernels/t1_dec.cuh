@@ -167,6 +167,9 @@ T1_HD uint32_t nib_any(u64 m) {
   return (uint32_t)m;
 }
 
+// bit i set when nibble i of m is all ones
+T1_HD uint32_t nib_all(u64 m) { return ~nib_any(~m) & 0xFFFFu; }
+
 struct DecOut {
   int bitplane;   // first plane not decoded completely (the reference's `bitplane`)
   int cpass;      // pass reached in it (0 when it was not started)
@@ -263,9 +266,27 @@ T1_HD DecOut decode_seq(const uint8_t *bytes, uint32_t Lmax, int K, int Z, bool 
         } else {
           work = nib_any(~S & ~P & VALID);
         }
+        // cleanup: a column of a full stripe with no significant or visited sample and nothing
+        // significant around it (a superset of its neighbourhood: the columns before and after it
+        // in scan order and the stripes above and below) starts with its run decision, and a 0
+        // ends the column with its state unchanged, before any neighbourhood is cut out.  A
+        // column that becomes significant takes the run start from the column after it.
+        uint32_t runcols = 0;
+        if (kind == 2 && wide) {
+          const uint32_t sigcols = nib_any(S);
+          const uint32_t busy = nib_any(S | P) | (sigcols << 1) | (sigcols >> 1) | (Lb ? 1u : 0u) |
+                                (Rb ? 0x8000u : 0u) |
+                                nib_any(((Uw | ULw | URw) & kRow3) | ((Dw | DLw | DRw) & kRow0));
+          runcols = nib_all(VALID) & ~busy & work;
+        }
         while (work) {
           const int ci = ctz64(work);
           work &= work - 1u;
+          bool run_one = false;   // the column's run decision was decoded here, as a 1
+          if ((runcols >> ci) & 1u) {
+            if (!dec_bit(d, &slot[dev::kCtxRun], tbl)) continue;
+            run_one = true;
+          }
           const int col = c0 + ci;
           uint32_t x, js;
           if (wide) {
@@ -404,8 +425,8 @@ T1_HD DecOut decode_seq(const uint8_t *bytes, uint32_t Lmax, int K, int Z, bool 
               uint32_t r = 0;
               bool skip_first = false;
               if (full && own == 0 && opi == 0 && !(Lx | Rx | u | dd)) {
-                // run mode
-                if (!dec_bit(d, &slot[dev::kCtxRun], tbl)) {
+                // run mode (the run decision already decoded when run_one)
+                if (!run_one && !dec_bit(d, &slot[dev::kCtxRun], tbl)) {
                   r = 4;
                 } else {
                   r = dec_bit(d, &slot[dev::kCtxUni], tbl) << 1;
@@ -428,6 +449,8 @@ T1_HD DecOut decode_seq(const uint8_t *bytes, uint32_t Lmax, int K, int Z, bool 
           }
           if (kind == 0 && ci < 15 && (((uint32_t)(S >> (4 * ci)) & 0xFu) != own0))
             work |= candcols & (2u << ci);   // the right neighbour may now be visited
+          if (kind == 2 && (((uint32_t)(S >> (4 * ci)) & 0xFu) != own0))
+            runcols &= ~(2u << ci);   // its right neighbour has a significant neighbour now
         }
         // cursor of the next group
         gx += 16;
