@@ -224,6 +224,20 @@ T1_HD DecOut decode_seq(const uint8_t *bytes, uint32_t Lmax, int K, int Z, bool 
       for (int g = 0; g < ngroups; ++g) {
         u64 S = sig[g], G = sgn[g], P = pi[g], D = del[g], Bt = bits[g];
         const int c0 = 16 * g;
+        // valid samples of the group (rows below a partial last stripe do not exist)
+        const uint32_t ncg = ((int)ncols - c0 < 16) ? (uint32_t)((int)ncols - c0) : 16u;
+        u64 VALID = (ncg == 16) ? ~0ull : ((1ull << (4 * ncg)) - 1ull);
+        if (rem) VALID = col_masks(g, W, nstripes, nfull, rem, ncols).valid;
+        // the columns that can need a decision in this pass: significance propagation visits
+        // insignificant samples next to significant ones (a column that becomes significant
+        // adds its right neighbour below); refinement the significant, unvisited samples;
+        // cleanup the insignificant, unvisited ones.  A group with none skips the neighbourhood.
+        uint32_t work;
+        uint32_t candcols = 0;
+        if (kind == 0) work = candcols = nib_any(~S & VALID);
+        else if (kind == 1) work = nib_any(S & ~P & VALID);
+        else work = nib_any(~S & ~P & VALID);
+        if (work) {
         // neighbours in other groups: left / right boundary columns, stripes above and below
         const uint32_t Lb = (g > 0) ? (uint32_t)(sig[g - 1] >> 60) : 0u;
         const uint32_t LbS = (g > 0) ? (uint32_t)(sgn[g - 1] >> 60) : 0u;
@@ -240,31 +254,12 @@ T1_HD DecOut decode_seq(const uint8_t *bytes, uint32_t Lmax, int K, int Z, bool 
           UsW = window(sgn, c0 - Wi, ngroups);
           DsW = window(sgn, c0 + Wi, ngroups);
         }
-        // valid samples of the group (rows below a partial last stripe do not exist)
-        const uint32_t ncg = ((int)ncols - c0 < 16) ? (uint32_t)((int)ncols - c0) : 16u;
-        u64 VALID = (ncg == 16) ? ~0ull : ((1ull << (4 * ncg)) - 1ull);
-        if (rem) VALID = col_masks(g, W, nstripes, nfull, rem, ncols).valid;
-        // the columns that can need a decision in this pass: significance propagation visits
-        // insignificant samples next to significant ones (a column that becomes significant
-        // adds its right neighbour below); refinement the significant, unvisited samples;
-        // cleanup the insignificant, unvisited ones
-        uint32_t work;
-        uint32_t candcols = 0;
-        if (kind == 0) {
-          candcols = nib_any(~S & VALID);
-          if (wide) {
-            const uint32_t sigcols = nib_any(S);
-            const uint32_t ud = nib_any(((Uw | ULw | URw) & kRow3) | ((Dw | DLw | DRw) & kRow0));
-            const uint32_t nbc = sigcols | (sigcols << 1) | (sigcols >> 1) | (Lb ? 1u : 0u) |
-                                 (Rb ? 0x8000u : 0u) | ud;
-            work = candcols & nbc & 0xFFFFu;
-          } else {
-            work = candcols;
-          }
-        } else if (kind == 1) {
-          work = nib_any(S & ~P & VALID);
-        } else {
-          work = nib_any(~S & ~P & VALID);
+        if (kind == 0 && wide) {
+          const uint32_t sigcols = nib_any(S);
+          const uint32_t ud = nib_any(((Uw | ULw | URw) & kRow3) | ((Dw | DLw | DRw) & kRow0));
+          const uint32_t nbc = sigcols | (sigcols << 1) | (sigcols >> 1) | (Lb ? 1u : 0u) |
+                               (Rb ? 0x8000u : 0u) | ud;
+          work = candcols & nbc & 0xFFFFu;
         }
         // cleanup: a column of a full stripe with no significant or visited sample and nothing
         // significant around it (a superset of its neighbourhood: the columns before and after it
@@ -452,6 +447,7 @@ T1_HD DecOut decode_seq(const uint8_t *bytes, uint32_t Lmax, int K, int Z, bool 
           if (kind == 2 && (((uint32_t)(S >> (4 * ci)) & 0xFu) != own0))
             runcols &= ~(2u << ci);   // its right neighbour has a significant neighbour now
         }
+        }   // work
         // cursor of the next group
         gx += 16;
         while (gx >= W) {
