@@ -444,7 +444,7 @@ def run_ours(a):
 T1_WARP_INSTR = {
     "t1_model_kernel": (2.673, "profiles/t1_kernels_512cube_f64.md"),
     "t1_mq_kernel": (6.010, "profiles/t1_kernels_512cube_f64.md"),
-    "t1_decode_kernel": (122.55e9, "profiles/t1_kernels_512cube_f64.md"),
+    "t1_decode_kernel": (104.38e9, "profiles/t1_kernels_512cube_f64.md"),
 }
 SMS = 148
 
