@@ -20,6 +20,7 @@
 // like the reference lifts its extended lines.
 #include <algorithm>
 #include <cstdio>
+#include <mutex>
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -1194,10 +1195,12 @@ int sm_count() {
 }
 
 uint32_t *fault_word() {
+  static std::mutex m;
   static uint32_t *addr[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lock(m);
   if (!addr[dev]) {
     void *p = nullptr;
     if (cudaGetSymbolAddress(&p, g_dwt_fault) != cudaSuccess) return nullptr;
@@ -1208,17 +1211,16 @@ uint32_t *fault_word() {
 
 // cuTensorMapEncodeTiled from the driver, looked up once through the runtime
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static bool tried = false;
-  if (!tried) {
-    tried = true;
+  // initialised once, thread-safely (a function-local static)
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
     void *p = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
             cudaSuccess &&
         q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-  }
+      return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+  }();
   return fn;
 }
 
