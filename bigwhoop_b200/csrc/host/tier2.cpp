@@ -460,6 +460,75 @@ struct StuffCounter {
       n -= m;
     }
   }
+  // The first n bits of rb, given `lead` (their leading one bits, at most 8) and `runs` (the
+  // ascending starts p of every 8-bit all-ones run in them): the bytes are counted from one
+  // possible 0xFF to the next instead of bit by bit.  A byte is w bits (8, or 7 after an 0xFF
+  // byte); from a byte start S (negative while bits before rb are pending), the next 0xFF can
+  // only be a run starting at S + 8k, so the bytes up to it are counted at once.
+  void put_run(const RawBits &rb, uint8_t lead, const std::vector<uint32_t> &runs) {
+    const int64_t n = (int64_t)rb.n;
+    if (!n) return;
+    int64_t S = -(int64_t)nacc;                       // start of the byte being filled
+    const uint64_t pend = acc & ((1ull << nacc) - 1);   // its bits from before rb
+    size_t ri = 0;
+    for (;;) {
+      if (w == 7) {
+        if (S + 7 > n) break;   // the 7-bit byte is not complete within rb
+        bytes++;
+        S += 7;
+        w = 8;
+        continue;
+      }
+      // w == 8: the first 0xFF byte at or after S, if any
+      int64_t ff = 0;
+      bool has_ff = false;
+      if (S < 0) {
+        // the byte mixing pending bits and rb's first bits
+        if (S + 8 <= n && pend == (1ull << (-S)) - 1 && (int64_t)lead >= 8 + S) {
+          ff = S;
+          has_ff = true;
+        }
+        else if (S + 8 > n) break;   // not complete within rb
+        else {
+          bytes++;
+          S += 8;
+          continue;
+        }
+      } else {
+        // runs before S are passed for good; a run at S + 8k + r (r != 0) may start a byte
+        // once a 7-bit byte has shifted the boundaries, so it is only skipped here
+        while (ri < runs.size() && (int64_t)runs[ri] < S) ++ri;
+        for (size_t j = ri; j < runs.size(); ++j)
+          if ((((int64_t)runs[j] - S) & 7) == 0) {
+            ff = runs[j];
+            has_ff = true;
+            break;
+          }
+      }
+      if (!has_ff) {   // no 0xFF byte: every whole byte left counts at once
+        const int64_t k = (n - S) >> 3;
+        bytes += (uint64_t)k;
+        S += 8 * k;
+        break;
+      }
+      bytes += (uint64_t)((ff - S) >> 3) + 1;   // the bytes before it, and the 0xFF byte
+      S = ff + 8;
+      w = 7;
+    }
+    // the bits of the byte being filled, [S, n)
+    const int rest = (int)(n - S);
+    acc = (S >= 0) ? read_bits(rb, (uint64_t)S, rest)
+                   : ((pend << n) | read_bits(rb, 0, (int)n));
+    nacc = rest;
+  }
+  // k (< 64) bits of rb from bit `off`, most significant first
+  static uint64_t read_bits(const RawBits &rb, uint64_t off, int k) {
+    if (k <= 0) return 0;
+    const uint64_t i = off >> 6, b = off & 63;
+    uint64_t v = rb.words[i] << b;
+    if (b + (uint64_t)k > 64) v |= rb.words[i + 1] >> (64 - b);
+    return v >> (64 - k);
+  }
   uint64_t finish() const { return bytes + ((nacc > 0 || w == 7) ? 1 : 0); }
 };
 
@@ -670,7 +739,32 @@ struct PieceResult {
   int64_t body = 0;
   bool e = false;
   RawBits hdr;
+  uint8_t lead = 0;             // leading one bits of hdr, at most 8
+  std::vector<uint32_t> runs;   // starts of the 8-bit all-ones runs in hdr, ascending
 };
+
+// lead and runs of a piece's header bits (bits past hdr.n are zero, so no run reaches them)
+static void scan_runs(PieceResult &r) {
+  r.runs.clear();
+  r.lead = 0;
+  const uint64_t n = r.hdr.n;
+  if (!n) return;
+  const uint64_t *w = r.hdr.words.data();
+  const size_t nw = r.hdr.words.size();
+  const uint64_t inv = ~w[0];
+  const uint64_t lead = inv ? (uint64_t)__builtin_clzll(inv) : 64;
+  r.lead = (uint8_t)std::min<uint64_t>(std::min<uint64_t>(lead, 8), n);
+  for (size_t i = 0; i < nw; ++i) {
+    const uint64_t x = w[i], y = (i + 1 < nw) ? w[i + 1] : 0;
+    uint64_t v = x;   // bit 63 - j set: stream bits 64 i + j .. 64 i + j + 7 are all ones
+    for (int t = 1; t < 8; ++t) v &= (x << t) | (y >> (64 - t));
+    while (v) {
+      const int j = __builtin_clzll(v);
+      r.runs.push_back((uint32_t)(64ull * i + (uint64_t)j));
+      v &= ~(1ull << (63 - j));
+    }
+  }
+}
 
 void probe_piece(const Probe &pr, uint16_t threshold, const ProbePiece &pc, PieceResult &out) {
   out.body = 0;
@@ -725,6 +819,7 @@ void probe_piece(const Probe &pr, uint16_t threshold, const ProbePiece &pc, Piec
     if (sh >= 0 && sh < 31) hb.put(L & (uint32_t)((2ull << sh) - 1), sh + 1);
   }
   hb.finish();
+  scan_runs(out);
 }
 
 // create_quality_layer(codec, tile, threshold, q, 1) for the tables of layer q, for several
@@ -753,7 +848,7 @@ void probe_thresholds(const Probe &pr, const std::vector<uint16_t> &thr, std::ve
         const PieceResult &r = part[k * np + j];
         size += r.body;
         e = e || r.e;
-        sc.put_bits(r.hdr, 0, r.hdr.n);
+        sc.put_run(r.hdr, r.lead, r.runs);
       }
       size += e ? (int64_t)sc.finish() : 1;
     }
