@@ -743,24 +743,25 @@ struct PieceResult {
   std::vector<uint32_t> runs;   // starts of the 8-bit all-ones runs in hdr, ascending
 };
 
-// lead and runs of a piece's header bits (bits past hdr.n are zero, so no run reaches them)
-static void scan_runs(PieceResult &r) {
-  r.runs.clear();
-  r.lead = 0;
-  const uint64_t n = r.hdr.n;
+// leading one bits (at most 8) and the starts of the runs of eight 1 bits of a bit string (its
+// bits past n are zero, so no run reaches them)
+static void scan_runs(const RawBits &rb, uint8_t &lead_out, std::vector<uint32_t> &runs) {
+  runs.clear();
+  lead_out = 0;
+  const uint64_t n = rb.n;
   if (!n) return;
-  const uint64_t *w = r.hdr.words.data();
-  const size_t nw = r.hdr.words.size();
+  const uint64_t *w = rb.words.data();
+  const size_t nw = rb.words.size();
   const uint64_t inv = ~w[0];
   const uint64_t lead = inv ? (uint64_t)__builtin_clzll(inv) : 64;
-  r.lead = (uint8_t)std::min<uint64_t>(std::min<uint64_t>(lead, 8), n);
+  lead_out = (uint8_t)std::min<uint64_t>(std::min<uint64_t>(lead, 8), n);
   for (size_t i = 0; i < nw; ++i) {
     const uint64_t x = w[i], y = (i + 1 < nw) ? w[i + 1] : 0;
     uint64_t v = x;   // bit 63 - j set: stream bits 64 i + j .. 64 i + j + 7 are all ones
     for (int t = 1; t < 8; ++t) v &= (x << t) | (y >> (64 - t));
     while (v) {
       const int j = __builtin_clzll(v);
-      r.runs.push_back((uint32_t)(64ull * i + (uint64_t)j));
+      runs.push_back((uint32_t)(64ull * i + (uint64_t)j));
       v &= ~(1ull << (63 - j));
     }
   }
@@ -819,7 +820,7 @@ void probe_piece(const Probe &pr, uint16_t threshold, const ProbePiece &pc, Piec
     if (sh >= 0 && sh < 31) hb.put(L & (uint32_t)((2ull << sh) - 1), sh + 1);
   }
   hb.finish();
-  scan_runs(out);
+  scan_runs(out.hdr, out.lead, out.runs);
 }
 
 // create_quality_layer(codec, tile, threshold, q, 1) for the tables of layer q, for several
@@ -884,12 +885,15 @@ int64_t final_quality_layer(bwc_codec *codec, Tile &tile, uint16_t threshold, in
   }
   std::vector<RawBits> bits(ns);
   std::vector<uint64_t> body(ns, 0);
+  std::vector<uint8_t> lead(ns, 0);
+  std::vector<std::vector<uint32_t>> runs(ns);
   WorkPool::instance().run(ns, [&](size_t j) {
     const uint32_t s = order[j];
     if (!e[segs[s].packet]) return;
     const PacketRef &r = pks[segs[s].packet];
     BodyPieces unused;
     segment_bits(*r.par, *r.res, r.p, segs[s].m, q, 1, bits[s], body[s], unused);
+    scan_runs(bits[s], lead[s], runs[s]);
   });
   int64_t total = 0;
   for (size_t i = 0; i < pks.size(); ++i) {
@@ -902,7 +906,7 @@ int64_t final_quality_layer(bwc_codec *codec, Tile &tile, uint16_t threshold, in
     StuffCounter sc;
     sc.put(1, 1);
     for (uint32_t s = first[i]; s < first[i + 1]; ++s) {
-      sc.put_bits(bits[s], 0, bits[s].n);
+      sc.put_run(bits[s], lead[s], runs[s]);
       pk.body_size += body[s];
     }
     total += (int64_t)sc.finish();
